@@ -1,0 +1,759 @@
+// C ABI of the sm_100a MBIR hot path (declared in include/mbir_b200.h).
+//
+// Host-side responsibilities: argument validation (before any launch),
+// launch-shape selection, workspace carving and the per-subset launch chain.
+// Nothing here allocates device memory.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "vcd.cuh"
+
+using namespace mbir;
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<unsigned long long> g_launches{0};
+
+// Optional per-kernel timing: when enabled, every launch is bracketed by a
+// pair of CUDA events recorded on its own stream; mbir_timing_collect sums
+// the elapsed times per kernel name.  Off by default (no events recorded).
+struct TimedLaunch {
+  const char *name;
+  cudaEvent_t a, b;
+};
+std::atomic<int> g_timing{0};
+std::mutex g_timing_mu;
+std::vector<TimedLaunch> g_timed;
+thread_local cudaEvent_t t_pending = nullptr;
+thread_local cudaStream_t t_stream = nullptr;
+
+void tpre(cudaStream_t st) {
+  t_stream = st;
+  if (!g_timing.load(std::memory_order_relaxed)) return;
+  cudaEventCreate(&t_pending);
+  cudaEventRecord(t_pending, st);
+}
+
+void tpost(const char *name) {
+  if (!t_pending) return;
+  cudaEvent_t b;
+  cudaEventCreate(&b);
+  cudaEventRecord(b, t_stream);
+  std::lock_guard<std::mutex> lk(g_timing_mu);
+  g_timed.push_back({name, t_pending, b});
+  t_pending = nullptr;
+}
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define MBIR_CHECK_LAUNCH(what)                                                     \
+  do {                                                                              \
+    g_launches.fetch_add(1, std::memory_order_relaxed);                             \
+    tpost(what);                                                                    \
+    cudaError_t _e = cudaGetLastError();                                            \
+    if (_e != cudaSuccess)                                                          \
+      return fail(MBIR_ERR_CUDA, "%s: launch failed: %s", what, cudaGetErrorString(_e)); \
+  } while (0)
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int next_pow2(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+// Sequential carving of a workspace buffer.
+struct Carver {
+  char *base;
+  size_t used = 0;
+  explicit Carver(void *b) : base(static_cast<char *>(b)) {}
+  template <typename T> T *take(size_t count) {
+    T *p = reinterpret_cast<T *>(base ? base + used : nullptr);
+    used += align_up(count * sizeof(T));
+    return p;
+  }
+};
+
+int validate_geometry(const mbir_geometry *g) {
+  if (!g) return fail(MBIR_ERR_INVALID, "geometry is NULL");
+  if (g->geometry != MBIR_PARALLEL && g->geometry != MBIR_CONE)
+    return fail(MBIR_ERR_INVALID, "geometry must be MBIR_PARALLEL or MBIR_CONE, got %d", g->geometry);
+  if (g->num_views <= 0 || g->num_det_rows <= 0 || g->num_det_channels <= 0 ||
+      g->num_recon_rows <= 0 || g->num_recon_cols <= 0 || g->num_slices <= 0)
+    return fail(MBIR_ERR_INVALID, "geometry sizes must be positive");
+  if ((long long)g->num_recon_rows * g->num_recon_cols >= (1LL << 31))
+    return fail(MBIR_ERR_INVALID, "recon grid too large for 32-bit pixel indices");
+  if (g->psf_radius < 0 || g->psf_radius > MBIR_MAX_TAP_RADIUS || g->bp_psf_radius < 0 ||
+      g->bp_psf_radius > MBIR_MAX_TAP_RADIUS)
+    return fail(MBIR_ERR_INVALID, "tap radii must lie in [0, %d] (psf %d, bp %d)",
+                MBIR_MAX_TAP_RADIUS, g->psf_radius, g->bp_psf_radius);
+  if (!(g->delta_det_channel > 0.f) || !(g->delta_voxel > 0.f) || !(g->delta_voxel_row > 0.f))
+    return fail(MBIR_ERR_INVALID, "detector and voxel pitches must be positive");
+  if (g->geometry == MBIR_PARALLEL && g->num_det_rows != g->num_slices)
+    return fail(MBIR_ERR_INVALID, "parallel beam needs num_det_rows == num_slices (%d vs %d)",
+                g->num_det_rows, g->num_slices);
+  if (g->geometry == MBIR_CONE) {
+    if (!(g->delta_det_row > 0.f) || !(g->delta_voxel_slice > 0.f) || !(g->magnification > 0.f))
+      return fail(MBIR_ERR_INVALID, "cone pitches and magnification must be positive");
+    if (!(g->source_detector_dist > 0.f))
+      return fail(MBIR_ERR_INVALID, "source_detector_dist must be positive");
+    if (g->num_det_rows > 4096)
+      return fail(MBIR_ERR_INVALID, "cone beam supports at most 4096 detector rows");
+  }
+  return MBIR_OK;
+}
+
+// ── back projection launch shape ───────────────────────────────────────────
+struct BackShape {
+  int T, SPL, slice_chunks, blocks_x, nchunks, vpc;
+  size_t smem;
+};
+
+BackShape back_shape(const mbir_geometry *g, int view_count, long long P, int band,
+                     size_t partial_budget_bytes) {
+  BackShape s;
+  if (g->geometry == MBIR_CONE) {
+    s.T = 32;
+    s.SPL = band <= 32 ? 1 : (band <= 64 ? 2 : 4);
+    s.smem = (size_t)(kThreads / 32) * g->num_det_rows * sizeof(float);
+  } else {
+    if (band <= 8) { s.T = 8; s.SPL = 1; }
+    else if (band <= 16) { s.T = 4; s.SPL = 4; }
+    else if (band <= 32) { s.T = 8; s.SPL = 4; }
+    else if (band <= 64) { s.T = 16; s.SPL = 4; }
+    else { s.T = 32; s.SPL = 4; }
+    s.smem = 0;
+  }
+  s.slice_chunks = (band + s.T * s.SPL - 1) / (s.T * s.SPL);
+  const long long teams = P * s.slice_chunks;
+  const int teams_per_block = kThreads / s.T;
+  s.blocks_x = (int)((teams + teams_per_block - 1) / teams_per_block);
+  // Enough warps for ~2 full waves of the 148 SMs; split views otherwise.
+  const long long warps = (teams * s.T + 31) / 32;
+  const long long target = 148LL * 64;
+  long long nch = warps >= target ? 1 : (target + warps - 1) / warps;
+  nch = std::min<long long>(nch, std::max(1, view_count / 4));
+  nch = std::min<long long>(nch, 64);
+  const size_t per_chunk = (size_t)P * band * sizeof(float);
+  if (nch > 1 && per_chunk > 0) {
+    long long fit = (long long)(partial_budget_bytes / per_chunk);
+    if (fit < nch) nch = std::max(1LL, fit);
+  }
+  s.nchunks = (int)std::max(1LL, nch);
+  s.vpc = (view_count + s.nchunks - 1) / s.nchunks;
+  s.nchunks = (view_count + s.vpc - 1) / s.vpc;
+  return s;
+}
+
+size_t back_partial_bytes(const BackShape &s, long long P, int band) {
+  return s.nchunks > 1 ? align_up((size_t)s.nchunks * P * band * sizeof(float)) : 0;
+}
+
+template <int CP, int SPL, typename RD>
+int launch_back_t(const Geo &geo, const mbir_geometry *g, const float *vp, int v_start,
+                  int v_count, const BackShape &s, const RD &rd, const int64_t *pix, long long P,
+                  int slice_start, int band, float *dst, cudaStream_t st, const char *what) {
+  dim3 grid(s.blocks_x, s.nchunks);
+  if (g->geometry == MBIR_CONE) {
+    auto k = back_cone_kernel<CP, SPL, RD>;
+    if (s.smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    tpre(st);
+    k<<<grid, kThreads, s.smem, st>>>(geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P,
+                                      slice_start, band, s.slice_chunks, dst);
+  } else {
+    tpre(st);
+    back_parallel_kernel<CP, SPL, RD><<<grid, kThreads, 0, st>>>(
+        geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P, band, s.T, s.slice_chunks, dst);
+  }
+  MBIR_CHECK_LAUNCH(what);
+  return MBIR_OK;
+}
+
+template <int CP, typename RD>
+int launch_back_spl(const Geo &geo, const mbir_geometry *g, const float *vp, int v_start,
+                    int v_count, const BackShape &s, const RD &rd, const int64_t *pix,
+                    long long P, int slice_start, int band, float *dst, cudaStream_t st,
+                    const char *what) {
+  switch (s.SPL) {
+    case 1: return launch_back_t<CP, 1>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
+    case 2: return launch_back_t<CP, 2>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
+    default: return launch_back_t<CP, 4>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
+  }
+}
+
+// Back projection with a given reader into `out` (or chunk partials in
+// `partials` followed by the fixed-order reduction).
+template <typename RD>
+int run_back(const mbir_geometry *g, const float *vp, int v_start, int v_count, const RD &rd,
+             const int64_t *pix, long long P, int cp, int slice_start, int band, float *out,
+             const BackShape &s, float *partials, cudaStream_t st, bool reduce_into_out,
+             const char *what = "back projection") {
+  const Geo geo = make_geo(*g);
+  float *dst = s.nchunks > 1 ? partials : out;
+  int rc = cp == 2 ? launch_back_spl<2>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what)
+                   : launch_back_spl<1>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
+  if (rc) return rc;
+  if (s.nchunks > 1 && reduce_into_out) {
+    const size_t n = (size_t)P * band;
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    tpre(st);
+    reduce_chunks_kernel<<<blocks, 256, 0, st>>>(partials, s.nchunks, n, out);
+    MBIR_CHECK_LAUNCH("chunk reduction");
+  }
+  return MBIR_OK;
+}
+
+// ── forward projection launch shape ────────────────────────────────────────
+FwdShape fwd_shape(const mbir_geometry *g, int band) {
+  FwdShape fs;
+  fs.rows = g->geometry == MBIR_CONE ? g->num_det_rows : band;
+  fs.TG = std::min(kThreads, next_pow2(std::max(fs.rows, 1)));
+  fs.RPT = (fs.rows + fs.TG - 1) / fs.TG;
+  const int G = kThreads / fs.TG;
+  const int RS = fs.TG * fs.RPT + 1;
+  int cb = (int)(48 * 1024 / (sizeof(float) * (size_t)G * RS));
+  cb = std::max(8, std::min(cb, 128));
+  fs.CB = std::min(cb, g->num_det_channels);
+  return fs;
+}
+
+template <bool CONE, typename EPI>
+int launch_forward(const mbir_geometry *g, const float *vp, int v_start, int v_count,
+                   const float *values, long long P, int band, int slice_start, const int64_t *pix,
+                   const FwdShape &fs, const EPI &epi, cudaStream_t st, const char *what) {
+  const Geo geo = make_geo(*g);
+  const size_t smem = fs.smem_bytes();
+  auto k = forward_kernel<CONE, EPI>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+      return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s", smem,
+                  cudaGetErrorString(e));
+  }
+  dim3 grid((g->num_det_channels + fs.CB - 1) / fs.CB, v_count);
+  tpre(st);
+  k<<<grid, kThreads, smem, st>>>(geo, vp, v_start, values, (int)P, band, slice_start, pix, fs, epi);
+  MBIR_CHECK_LAUNCH(what);
+  return MBIR_OK;
+}
+
+template <typename EPI>
+int run_forward(const mbir_geometry *g, const float *vp, int v_start, int v_count,
+                const float *values, long long P, int band, int slice_start, const int64_t *pix,
+                const EPI &epi, cudaStream_t st, const char *what = "forward projection") {
+  const FwdShape fs = fwd_shape(g, band);
+  if (g->geometry == MBIR_CONE)
+    return launch_forward<true>(g, vp, v_start, v_count, values, P, band, slice_start, pix, fs, epi, st, what);
+  return launch_forward<false>(g, vp, v_start, v_count, values, P, band, slice_start, pix, fs, epi, st, what);
+}
+
+int fwd_blocks(const mbir_geometry *g, int band, int v_count) {
+  const FwdShape fs = fwd_shape(g, band);
+  return ((g->num_det_channels + fs.CB - 1) / fs.CB) * v_count;
+}
+
+// ── VCD workspace ─────────────────────────────────────────────────────────
+struct VcdWs {
+  float *grad_part, *delta, *gbuf, *hinv, *gpbuf, *hpbuf, *alpha;
+  double *dc_sums, *prior_part, *fwd_part, *sq_part, *l1_part;
+  void *ad;
+  BackShape bs;
+  int dc_chunks, prior_blocks, fwd_blocks, upd_chunks, upd_yblocks;
+  size_t bytes;
+};
+
+constexpr int kUpdChunk = 32;   // pixels per update tile
+constexpr int kDcChunk = 256;   // pixels per DC-sum chunk
+
+size_t storage_size(int storage) { return storage == MBIR_F32 ? 4 : 2; }
+
+VcdWs vcd_layout(const mbir_geometry *g, long long Ps, const mbir_vcd_params *prm, void *base) {
+  VcdWs w;
+  const int S = g->num_slices, V = g->num_views;
+  const size_t PS = (size_t)Ps * S;
+  w.bs = back_shape(g, V, Ps, S, (size_t)64 * PS * sizeof(float));
+  Carver c(base);
+  w.grad_part = c.take<float>((size_t)std::max(1, w.bs.nchunks) * PS);
+  w.delta = c.take<float>(PS);
+  w.gbuf = c.take<float>(PS);
+  w.hinv = c.take<float>(PS);
+  w.gpbuf = c.take<float>(PS);
+  w.hpbuf = c.take<float>(PS);
+  w.dc_chunks = (int)((Ps + kDcChunk - 1) / kDcChunk);
+  w.dc_sums = c.take<double>((size_t)w.dc_chunks * S * 2);
+  w.prior_blocks = (int)((PS + kThreads - 1) / kThreads);
+  w.prior_part = c.take<double>((size_t)w.prior_blocks * 2);
+  w.fwd_blocks = fwd_blocks(g, S, V);
+  w.fwd_part = c.take<double>((size_t)w.fwd_blocks * 2);
+  w.upd_chunks = (int)((Ps + kUpdChunk - 1) / kUpdChunk);
+  w.upd_yblocks = (S + kThreads - 1) / kThreads;
+  w.sq_part = c.take<double>((size_t)w.upd_chunks * S);
+  w.l1_part = c.take<double>((size_t)w.upd_chunks * w.upd_yblocks);
+  w.alpha = c.take<float>(4);
+  w.ad = c.take<char>((size_t)V * g->num_det_channels * g->num_det_rows * storage_size(prm->storage));
+  w.bytes = c.used;
+  return w;
+}
+
+template <typename T>
+int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params *prm,
+                 float *flat, T *err, const float *es, const T *wts, const float *wsc,
+                 const float *H, const float *dc, const int64_t *pix, long long Ps,
+                 double *accum, float *alpha_user, VcdWs &w, cudaStream_t st) {
+  const int S = g->num_slices, V = g->num_views, C = g->num_det_channels, R = g->num_det_rows;
+  const size_t PS = (size_t)Ps * S;
+  const VcdScalars sc = make_scalars(*prm);
+  const bool DCon = dc != nullptr;
+  int rc;
+  // 1. gradient partials of A^T (w e), one slab per view chunk
+  if (wts) {
+    ReadWeighted<T> rd{err, es, wts, wsc, C, R};
+    rc = run_back(g, vp, 0, V, rd, pix, Ps, 1, 0, S, w.grad_part, w.bs, w.grad_part, st, false,
+                  "vcd gradient (back projection)");
+  } else {
+    ReadScaled<T> rd{err, es, C, R};
+    rc = run_back(g, vp, 0, V, rd, pix, Ps, 1, 0, S, w.grad_part, w.bs, w.grad_part, st, false,
+                  "vcd gradient (back projection)");
+  }
+  if (rc) return rc;
+  // 2. direction (reduces the chunk slabs in order)
+  const int nb = w.prior_blocks;
+  if (!DCon) {
+    tpre(st);
+    vcd_direction_kernel<false><<<nb, kThreads, 0, st>>>(
+        (int)Ps, S, pix, g->num_recon_rows, g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H,
+        sc, w.delta, nullptr, nullptr, nullptr, nullptr, w.prior_part);
+    MBIR_CHECK_LAUNCH("vcd direction");
+  } else {
+    tpre(st);
+    vcd_direction_kernel<true><<<nb, kThreads, 0, st>>>(
+        (int)Ps, S, pix, g->num_recon_rows, g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H,
+        sc, nullptr, w.gbuf, w.hinv, w.gpbuf, w.hpbuf, nullptr);
+    MBIR_CHECK_LAUNCH("vcd direction (damped)");
+    dim3 gs((S + 127) / 128, w.dc_chunks);
+    tpre(st);
+    vcd_dc_sums_kernel<<<gs, 128, 0, st>>>((int)Ps, S, kDcChunk, w.gbuf, w.hinv, w.dc_sums);
+    MBIR_CHECK_LAUNCH("vcd DC sums");
+    tpre(st);
+    vcd_dc_direction_kernel<<<nb, kThreads, 0, st>>>((int)Ps, S, w.dc_chunks, w.dc_sums, dc,
+                                                     w.gbuf, w.hinv, w.gpbuf, w.hpbuf, w.delta,
+                                                     w.prior_part);
+    MBIR_CHECK_LAUNCH("vcd DC direction");
+  }
+  // 3. forward A delta + line-search partials
+  LineSearchEpi<T> epi{err, es, wts, wsc, static_cast<T *>(w.ad), C, R, w.fwd_part, 1, 0.0, 0.0};
+  rc = run_forward(g, vp, 0, V, w.delta, Ps, S, 0, pix, epi, st,
+                   "vcd forward + line search");
+  if (rc) return rc;
+  // 4. alpha
+  tpre(st);
+  vcd_alpha_kernel<<<1, kThreads, 0, st>>>(w.prior_part, nb, w.fwd_part, w.fwd_blocks, sc.fmc,
+                                           sc.max_alpha, w.alpha, alpha_user);
+  MBIR_CHECK_LAUNCH("vcd alpha");
+  if (prm->positivity) {
+    tpre(st);
+    vcd_positivity_kernel<<<(unsigned)((PS + 255) / 256), 256, 0, st>>>((int)Ps, S, pix, flat,
+                                                                        w.alpha, w.delta);
+    MBIR_CHECK_LAUNCH("vcd positivity");
+    LineSearchEpi<T> epi2{err, es, wts, wsc, static_cast<T *>(w.ad), C, R, nullptr, 0, 0.0, 0.0};
+    rc = run_forward(g, vp, 0, V, w.delta, Ps, S, 0, pix, epi2, st, "vcd forward (positivity)");
+    if (rc) return rc;
+  }
+  // 5. update
+  dim3 gu(w.upd_chunks, w.upd_yblocks);
+  tpre(st);
+  vcd_pixel_update_kernel<<<gu, kThreads, 0, st>>>((int)Ps, S, kUpdChunk, pix, w.delta, w.alpha,
+                                                   flat, w.sq_part, w.l1_part);
+  MBIR_CHECK_LAUNCH("vcd pixel update");
+  tpre(st);
+  vcd_finish_kernel<<<1, kThreads, 0, st>>>(S, w.upd_chunks, w.upd_chunks * w.upd_yblocks,
+                                            w.sq_part, w.l1_part, w.alpha, accum);
+  MBIR_CHECK_LAUNCH("vcd finish");
+  const size_t n = (size_t)V * C * R;
+  const int blocks = (int)std::min<size_t>((n / 4 + 255) / 256 + 1, 148 * 32);
+  tpre(st);
+  vcd_sino_update_kernel<T><<<blocks, 256, 0, st>>>(n, w.alpha, err, static_cast<const T *>(w.ad));
+  MBIR_CHECK_LAUNCH("vcd sinogram update");
+  return MBIR_OK;
+}
+
+int validate_vcd(const mbir_geometry *g, const mbir_vcd_params *prm, const void *flat,
+                 const void *err, const float *es, const void *wts, const float *wsc,
+                 const float *H, long long Ps) {
+  int rc = validate_geometry(g);
+  if (rc) return rc;
+  if (!prm) return fail(MBIR_ERR_INVALID, "params is NULL");
+  if (prm->storage != MBIR_F32 && prm->storage != MBIR_BF16 && prm->storage != MBIR_F16)
+    return fail(MBIR_ERR_INVALID, "unknown storage dtype %d", prm->storage);
+  if (!flat || !err || !es || !H) return fail(MBIR_ERR_INVALID, "NULL state pointer");
+  if (wts && !wsc) return fail(MBIR_ERR_INVALID, "weights given without their scale");
+  if (Ps <= 0) return fail(MBIR_ERR_INVALID, "subset must have at least one pixel");
+  if (!(prm->sigma_x > 0.f) || !(prm->fm_constant > 0.f) || !(prm->T > 0.f))
+    return fail(MBIR_ERR_INVALID, "sigma_x, T and fm_constant must be positive");
+  return MBIR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t mbir_abi_version(void) { return 10000; }
+
+const char *mbir_last_error(void) { return g_last_error.c_str(); }
+
+unsigned long long mbir_launch_count(void) { return g_launches.load(); }
+
+int32_t mbir_timing_enable(int32_t on) {
+  const int prev = g_timing.exchange(on ? 1 : 0);
+  return prev;
+}
+
+int32_t mbir_timing_collect(char *names, int32_t names_bytes, double *total_ms,
+                            int64_t *counts, int32_t max_entries) {
+  std::vector<TimedLaunch> timed;
+  {
+    std::lock_guard<std::mutex> lk(g_timing_mu);
+    timed.swap(g_timed);
+  }
+  std::vector<std::string> keys;
+  std::vector<double> ms;
+  std::vector<int64_t> cnt;
+  for (auto &t : timed) {
+    float e = 0.f;
+    cudaEventSynchronize(t.b);
+    if (cudaEventElapsedTime(&e, t.a, t.b) != cudaSuccess) e = 0.f;
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+    size_t k = 0;
+    while (k < keys.size() && keys[k] != t.name) ++k;
+    if (k == keys.size()) {
+      keys.push_back(t.name);
+      ms.push_back(0.0);
+      cnt.push_back(0);
+    }
+    ms[k] += e;
+    cnt[k] += 1;
+  }
+  std::string joined;
+  const int n = (int)std::min<size_t>(keys.size(), (size_t)std::max(0, max_entries));
+  for (int k = 0; k < n; ++k) {
+    if (total_ms) total_ms[k] = ms[k];
+    if (counts) counts[k] = cnt[k];
+    joined += keys[k];
+    joined += '\n';
+  }
+  if (names && names_bytes > 0) {
+    const size_t m = std::min<size_t>(joined.size(), (size_t)names_bytes - 1);
+    memcpy(names, joined.data(), m);
+    names[m] = 0;
+  }
+  cudaGetLastError();
+  return n;
+}
+
+int32_t mbir_forward_project(const mbir_geometry *geom, const float *view_params,
+                             int32_t view_start, int32_t view_count, const float *values,
+                             int64_t num_pixels, int32_t band_len, int32_t slice_start,
+                             const int64_t *pixel_indices, float *sino_out, int32_t out_layout,
+                             void *stream) {
+  int rc = validate_geometry(geom);
+  if (rc) return rc;
+  if (view_start < 0 || view_count < 0 || view_start + view_count > geom->num_views)
+    return fail(MBIR_ERR_INVALID, "view range [%d, %d) outside [0, %d)", view_start,
+                view_start + view_count, geom->num_views);
+  if (num_pixels < 0 || num_pixels >= (1LL << 31)) return fail(MBIR_ERR_INVALID, "bad num_pixels");
+  if (band_len <= 0 || slice_start < 0 || slice_start + band_len > geom->num_slices)
+    return fail(MBIR_ERR_INVALID, "slice band [%d, %d) outside [0, %d)", slice_start,
+                slice_start + band_len, geom->num_slices);
+  if (geom->geometry == MBIR_PARALLEL && (slice_start != 0 || band_len != geom->num_det_rows))
+    return fail(MBIR_ERR_INVALID, "parallel beam projects whole cylinders (band == rows)");
+  if (out_layout != MBIR_LAYOUT_VRC && out_layout != MBIR_LAYOUT_VCR)
+    return fail(MBIR_ERR_INVALID, "unknown layout %d", out_layout);
+  if (!view_params || !sino_out || (num_pixels > 0 && (!values || !pixel_indices)))
+    return fail(MBIR_ERR_INVALID, "NULL array argument");
+  if (view_count == 0) return MBIR_OK;
+  cudaStream_t st = as_stream(stream);
+  if (num_pixels == 0) {
+    cudaError_t e = cudaMemsetAsync(sino_out, 0,
+        (size_t)view_count * geom->num_det_rows * geom->num_det_channels * sizeof(float), st);
+    if (e != cudaSuccess) return fail(MBIR_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
+    return MBIR_OK;
+  }
+  StoreSino epi{sino_out, out_layout, geom->num_det_channels, geom->num_det_rows};
+  return run_forward(geom, view_params, view_start, view_count, values, num_pixels, band_len,
+                     slice_start, pixel_indices, epi, st);
+}
+
+size_t mbir_back_project_workspace_size(const mbir_geometry *geom, int32_t view_count,
+                                        int64_t num_pixels, int32_t band_len) {
+  if (!geom || view_count <= 0 || num_pixels <= 0 || band_len <= 0) return 0;
+  const BackShape s = back_shape(geom, view_count, num_pixels, band_len, (size_t)1 << 40);
+  const size_t sino = align_up((size_t)view_count * geom->num_det_rows * geom->num_det_channels *
+                               sizeof(float));
+  return back_partial_bytes(s, num_pixels, band_len) + sino;
+}
+
+int32_t mbir_back_project(const mbir_geometry *geom, const float *view_params, int32_t view_start,
+                          int32_t view_count, const float *sino, int32_t sino_layout,
+                          const int64_t *pixel_indices, int64_t num_pixels, int32_t coeff_power,
+                          int32_t slice_start, int32_t band_len, float *out, void *workspace,
+                          size_t workspace_bytes, void *stream) {
+  int rc = validate_geometry(geom);
+  if (rc) return rc;
+  if (view_start < 0 || view_count < 0 || view_start + view_count > geom->num_views)
+    return fail(MBIR_ERR_INVALID, "view range [%d, %d) outside [0, %d)", view_start,
+                view_start + view_count, geom->num_views);
+  if (coeff_power != 1 && coeff_power != 2)
+    return fail(MBIR_ERR_INVALID, "coeff_power must be 1 or 2, got %d", coeff_power);
+  if (band_len <= 0 || slice_start < 0 || slice_start + band_len > geom->num_slices)
+    return fail(MBIR_ERR_INVALID, "slice band [%d, %d) outside [0, %d)", slice_start,
+                slice_start + band_len, geom->num_slices);
+  if (geom->geometry == MBIR_PARALLEL && (slice_start != 0 || band_len != geom->num_det_rows))
+    return fail(MBIR_ERR_INVALID, "parallel beam back-projects whole cylinders (band == rows)");
+  if (sino_layout != MBIR_LAYOUT_VRC && sino_layout != MBIR_LAYOUT_VCR)
+    return fail(MBIR_ERR_INVALID, "unknown layout %d", sino_layout);
+  if (num_pixels < 0 || num_pixels >= (1LL << 31)) return fail(MBIR_ERR_INVALID, "bad num_pixels");
+  if (!view_params || (num_pixels > 0 && (!sino || !pixel_indices || !out)))
+    return fail(MBIR_ERR_INVALID, "NULL array argument");
+  cudaStream_t st = as_stream(stream);
+  if (num_pixels == 0) return MBIR_OK;
+  if (view_count == 0) {
+    cudaError_t e = cudaMemsetAsync(out, 0, (size_t)num_pixels * band_len * sizeof(float), st);
+    if (e != cudaSuccess) return fail(MBIR_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
+    return MBIR_OK;
+  }
+  const int C = geom->num_det_channels, R = geom->num_det_rows;
+  const size_t sino_bytes = align_up((size_t)view_count * R * C * sizeof(float));
+  const size_t need_sino = sino_layout == MBIR_LAYOUT_VRC ? sino_bytes : 0;
+  if (workspace_bytes < need_sino || (need_sino && !workspace))
+    return fail(MBIR_ERR_WORKSPACE, "workspace of %zu bytes < %zu needed for the layout change",
+                workspace_bytes, need_sino);
+  const size_t partial_budget = workspace ? workspace_bytes - need_sino : 0;
+  const BackShape s = back_shape(geom, view_count, num_pixels, band_len, partial_budget);
+  char *ws = static_cast<char *>(workspace);
+  const float *vcr = sino;
+  if (sino_layout == MBIR_LAYOUT_VRC) {
+    float *t = reinterpret_cast<float *>(ws);
+    dim3 grid((C + 31) / 32, (R + 31) / 32, view_count);
+    tpre(st);
+    vrc_to_vcr_kernel<float><<<grid, dim3(32, 8), 0, st>>>(R, C, sino, nullptr, t);
+    MBIR_CHECK_LAUNCH("layout change");
+    vcr = t;
+  }
+  float *partials = reinterpret_cast<float *>(ws ? ws + need_sino : nullptr);
+  ReadF32 rd{vcr, C, R};
+  return run_back(geom, view_params, view_start, view_count, rd, pixel_indices, num_pixels,
+                  coeff_power, slice_start, band_len, out, s, partials, st, true);
+}
+
+int32_t mbir_sino_convert(int32_t direction, int32_t views, int32_t rows, int32_t channels,
+                          const void *src, void *dst, int32_t dtype, float *scale,
+                          int32_t compute_scale, void *stream) {
+  if (views <= 0 || rows <= 0 || channels <= 0) return fail(MBIR_ERR_INVALID, "bad sinogram shape");
+  if (!src || !dst || !scale) return fail(MBIR_ERR_INVALID, "NULL array argument");
+  if (dtype != MBIR_F32 && dtype != MBIR_BF16 && dtype != MBIR_F16)
+    return fail(MBIR_ERR_INVALID, "unknown dtype %d", dtype);
+  cudaStream_t st = as_stream(stream);
+  const int R = rows, C = channels;
+  if (direction == 0) {
+    if (compute_scale) {
+      if (dtype == MBIR_F16) {
+        tpre(st);
+        view_scale_kernel<<<views, kThreads, 0, st>>>(R * C, static_cast<const float *>(src),
+                                                      1024.f, scale);
+        MBIR_CHECK_LAUNCH("view scale");
+      } else {
+        tpre(st);
+        fill_kernel<<<(views + 255) / 256, 256, 0, st>>>(views, 1.f, scale);
+        MBIR_CHECK_LAUNCH("scale fill");
+      }
+    }
+    dim3 grid((C + 31) / 32, (R + 31) / 32, views);
+    const float *s = static_cast<const float *>(src);
+    tpre(st);
+    if (dtype == MBIR_F32)
+      vrc_to_vcr_kernel<float><<<grid, dim3(32, 8), 0, st>>>(R, C, s, scale, static_cast<float *>(dst));
+    else if (dtype == MBIR_BF16)
+      vrc_to_vcr_kernel<__nv_bfloat16><<<grid, dim3(32, 8), 0, st>>>(R, C, s, scale, static_cast<__nv_bfloat16 *>(dst));
+    else
+      vrc_to_vcr_kernel<__half><<<grid, dim3(32, 8), 0, st>>>(R, C, s, scale, static_cast<__half *>(dst));
+    MBIR_CHECK_LAUNCH("sinogram conversion");
+  } else if (direction == 1) {
+    dim3 grid((R + 31) / 32, (C + 31) / 32, views);
+    float *d = static_cast<float *>(dst);
+    tpre(st);
+    if (dtype == MBIR_F32)
+      vcr_to_vrc_kernel<float><<<grid, dim3(32, 8), 0, st>>>(R, C, static_cast<const float *>(src), scale, d);
+    else if (dtype == MBIR_BF16)
+      vcr_to_vrc_kernel<__nv_bfloat16><<<grid, dim3(32, 8), 0, st>>>(R, C, static_cast<const __nv_bfloat16 *>(src), scale, d);
+    else
+      vcr_to_vrc_kernel<__half><<<grid, dim3(32, 8), 0, st>>>(R, C, static_cast<const __half *>(src), scale, d);
+    MBIR_CHECK_LAUNCH("sinogram conversion");
+  } else {
+    return fail(MBIR_ERR_INVALID, "direction must be 0 or 1");
+  }
+  return MBIR_OK;
+}
+
+size_t mbir_error_init_workspace_size(int64_t count) {
+  (void)count;
+  return align_up(sizeof(double) * 2 * 148 * 8) + 256;
+}
+
+int32_t mbir_error_init(int64_t count, const float *y, const float *ax, const float *weights,
+                        int32_t scale_to_data, float *error_out, double *alpha_out,
+                        void *workspace, size_t workspace_bytes, void *stream) {
+  if (count <= 0 || !y || !ax || !error_out || !alpha_out)
+    return fail(MBIR_ERR_INVALID, "bad error-init arguments");
+  if (!workspace || workspace_bytes < mbir_error_init_workspace_size(count))
+    return fail(MBIR_ERR_WORKSPACE, "error init needs %zu workspace bytes",
+                mbir_error_init_workspace_size(count));
+  cudaStream_t st = as_stream(stream);
+  const int nb = 148 * 8;
+  double *part = static_cast<double *>(workspace);
+  tpre(st);
+  init_dots_kernel<<<nb, kThreads, 0, st>>>((size_t)count, y, ax, weights, part);
+  MBIR_CHECK_LAUNCH("init dots");
+  tpre(st);
+  init_alpha_kernel<<<1, kThreads, 0, st>>>(nb, part, scale_to_data, alpha_out);
+  MBIR_CHECK_LAUNCH("init alpha");
+  tpre(st);
+  init_error_kernel<<<nb, 256, 0, st>>>((size_t)count, y, ax, alpha_out, error_out);
+  MBIR_CHECK_LAUNCH("init error");
+  return MBIR_OK;
+}
+
+size_t mbir_vcd_workspace_size(const mbir_geometry *geom, int64_t max_subset_pixels,
+                               const mbir_vcd_params *params) {
+  if (!geom || !params || max_subset_pixels <= 0) return 0;
+  return vcd_layout(geom, max_subset_pixels, params, nullptr).bytes;
+}
+
+int32_t mbir_vcd_subset_update(const mbir_geometry *geom, const float *view_params,
+                               const mbir_vcd_params *params, float *flat_recon, void *error_sino,
+                               const float *err_scale, const void *weights,
+                               const float *w_scale, const float *fm_hessian,
+                               const float *dc_profile, const int64_t *pixel_indices,
+                               int64_t num_pixels, double *accum, float *alpha_out,
+                               void *workspace, size_t workspace_bytes, void *stream) {
+  int rc = validate_vcd(geom, params, flat_recon, error_sino, err_scale, weights, w_scale,
+                        fm_hessian, num_pixels);
+  if (rc) return rc;
+  if (!view_params || !pixel_indices || !accum) return fail(MBIR_ERR_INVALID, "NULL argument");
+  VcdWs w = vcd_layout(geom, num_pixels, params, workspace);
+  if (!workspace || workspace_bytes < w.bytes)
+    return fail(MBIR_ERR_WORKSPACE, "VCD workspace of %zu bytes < %zu needed", workspace_bytes,
+                w.bytes);
+  cudaStream_t st = as_stream(stream);
+  switch (params->storage) {
+    case MBIR_F32:
+      return vcd_subset_t<float>(geom, view_params, params, flat_recon,
+                                 static_cast<float *>(error_sino), err_scale,
+                                 static_cast<const float *>(weights), w_scale, fm_hessian,
+                                 dc_profile, pixel_indices, num_pixels, accum, alpha_out, w, st);
+    case MBIR_BF16:
+      return vcd_subset_t<__nv_bfloat16>(geom, view_params, params, flat_recon,
+                                         static_cast<__nv_bfloat16 *>(error_sino), err_scale,
+                                         static_cast<const __nv_bfloat16 *>(weights), w_scale,
+                                         fm_hessian, dc_profile, pixel_indices, num_pixels, accum,
+                                         alpha_out, w, st);
+    default:
+      return vcd_subset_t<__half>(geom, view_params, params, flat_recon,
+                                  static_cast<__half *>(error_sino), err_scale,
+                                  static_cast<const __half *>(weights), w_scale, fm_hessian,
+                                  dc_profile, pixel_indices, num_pixels, accum, alpha_out, w, st);
+  }
+}
+
+int32_t mbir_vcd_partition_pass(const mbir_geometry *geom, const float *view_params,
+                                const mbir_vcd_params *params, float *flat_recon, void *error_sino,
+                                const float *err_scale, const void *weights, const float *w_scale,
+                                const float *fm_hessian, const float *dc_profile,
+                                const int64_t *partition, int32_t num_subsets,
+                                int64_t subset_pixels, const int32_t *order, double *accum,
+                                void *workspace, size_t workspace_bytes, void *stream) {
+  if (num_subsets <= 0 || !order || !partition)
+    return fail(MBIR_ERR_INVALID, "partition pass needs subsets, a partition and an order");
+  for (int i = 0; i < num_subsets; ++i)
+    if (order[i] < 0 || order[i] >= num_subsets)
+      return fail(MBIR_ERR_INVALID, "order[%d] = %d outside [0, %d)", i, order[i], num_subsets);
+  for (int i = 0; i < num_subsets; ++i) {
+    const int rc = mbir_vcd_subset_update(
+        geom, view_params, params, flat_recon, error_sino, err_scale, weights, w_scale,
+        fm_hessian, dc_profile, partition + (size_t)order[i] * subset_pixels, subset_pixels, accum,
+        nullptr, workspace, workspace_bytes, stream);
+    if (rc) return rc;
+  }
+  return MBIR_OK;
+}
+
+size_t mbir_iteration_stats_workspace_size(void) {
+  return align_up(sizeof(double) * 3 * 148 * 4) + align_up(sizeof(double) * 148 * 4);
+}
+
+int32_t mbir_iteration_stats(int32_t views, int32_t rows, int32_t channels, const void *error_sino,
+                             const float *err_scale, const void *weights, const float *w_scale,
+                             int32_t storage, const float *flat_recon, int64_t recon_count,
+                             double *out, void *workspace, size_t workspace_bytes, void *stream) {
+  if (views <= 0 || rows <= 0 || channels <= 0 || !error_sino || !err_scale || !out ||
+      (weights && !w_scale) || (recon_count > 0 && !flat_recon))
+    return fail(MBIR_ERR_INVALID, "bad statistics arguments");
+  if (!workspace || workspace_bytes < mbir_iteration_stats_workspace_size())
+    return fail(MBIR_ERR_WORKSPACE, "statistics need %zu workspace bytes",
+                mbir_iteration_stats_workspace_size());
+  cudaStream_t st = as_stream(stream);
+  const int nb = 148 * 4;
+  double *sp = static_cast<double *>(workspace);
+  double *lp = reinterpret_cast<double *>(static_cast<char *>(workspace) +
+                                          align_up(sizeof(double) * 3 * nb));
+  const int CR = rows * channels;
+  switch (storage) {
+    case MBIR_F32:
+      tpre(st);
+      stats_sino_kernel<float><<<nb, kThreads, 0, st>>>(views, CR, static_cast<const float *>(error_sino),
+          err_scale, static_cast<const float *>(weights), w_scale, sp);
+      break;
+    case MBIR_BF16:
+      tpre(st);
+      stats_sino_kernel<__nv_bfloat16><<<nb, kThreads, 0, st>>>(views, CR,
+          static_cast<const __nv_bfloat16 *>(error_sino), err_scale,
+          static_cast<const __nv_bfloat16 *>(weights), w_scale, sp);
+      break;
+    case MBIR_F16:
+      tpre(st);
+      stats_sino_kernel<__half><<<nb, kThreads, 0, st>>>(views, CR, static_cast<const __half *>(error_sino),
+          err_scale, static_cast<const __half *>(weights), w_scale, sp);
+      break;
+    default:
+      return fail(MBIR_ERR_INVALID, "unknown storage dtype %d", storage);
+  }
+  MBIR_CHECK_LAUNCH("stats (sinogram)");
+  tpre(st);
+  stats_l1_kernel<<<nb, kThreads, 0, st>>>((size_t)std::max<int64_t>(recon_count, 0), flat_recon, lp);
+  MBIR_CHECK_LAUNCH("stats (recon)");
+  tpre(st);
+  stats_finish_kernel<<<1, kThreads, 0, st>>>(nb, sp, nb, lp, out);
+  MBIR_CHECK_LAUNCH("stats finish");
+  return MBIR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,182 @@
+// Shared device-side definitions for the sm_100a MBIR kernels.
+//
+// Geometry: the per-(view, pixel) chains of the reference are recomputed
+// in-kernel from a handful of per-model constants (struct Geo) instead of
+// being materialized per call as the reference's Triton wrappers do
+// (triton_cone.py:469-497 charges 48 B per view-pixel for that).  The FP32
+// operation order follows the reference torch bodies:
+//   parallel  parallel_beam.py:22-53
+//   cone      cone_beam.py:59-158
+// Scalars that the reference forms in Python double precision before they
+// meet an FP32 tensor (e.g. (num_rows - 1) / 2.0, 1.0 / magnification) are
+// formed the same way on the host (make_geo) and rounded once to float.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/mbir_b200.h"
+
+namespace mbir {
+
+constexpr int kMaxTaps = 2 * MBIR_MAX_TAP_RADIUS + 1;
+
+struct Geo {
+  int cone;
+  int V, R, C, NR, NC, S;
+  int psf, bp, curved;
+  float ddc, ddr, offc, offr, dv, dvr, dvs, rso, sdd;
+  // derived (host, double -> float)
+  float rc_row;      // (NR - 1) / 2
+  float rc_col;      // (NC - 1) / 2
+  float det_cc;      // (C - 1) / 2
+  float det_cr;      // (R - 1) / 2
+  float slice_c;     // (S - 1) / 2
+  float half_z;      // dvs * (S - 1) / 2
+  float inv_M;       // 1 / magnification
+  float sid;         // sdd / magnification
+  float area;        // dvr * dv
+  float inv_sdd;     // 1 / sdd (0 at sdd = inf)
+};
+
+inline Geo make_geo(const mbir_geometry &g) {
+  Geo o;
+  o.cone = g.geometry == MBIR_CONE;
+  o.V = g.num_views;
+  o.R = g.num_det_rows;
+  o.C = g.num_det_channels;
+  o.NR = g.num_recon_rows;
+  o.NC = g.num_recon_cols;
+  o.S = g.num_slices;
+  o.psf = g.psf_radius;
+  o.bp = g.bp_psf_radius;
+  o.curved = g.use_curved_detector;
+  o.ddc = g.delta_det_channel;
+  o.ddr = g.delta_det_row;
+  o.offc = g.det_channel_offset;
+  o.offr = g.det_row_offset;
+  o.dv = g.delta_voxel;
+  o.dvr = g.delta_voxel_row;
+  o.dvs = g.delta_voxel_slice;
+  o.rso = g.recon_slice_offset;
+  o.sdd = g.source_detector_dist;
+  o.rc_row = (float)((g.num_recon_rows - 1) / 2.0);
+  o.rc_col = (float)((g.num_recon_cols - 1) / 2.0);
+  o.det_cc = (float)((g.num_det_channels - 1) / 2.0);
+  o.det_cr = (float)((g.num_det_rows - 1) / 2.0);
+  o.slice_c = (float)((g.num_slices - 1) / 2.0);
+  o.half_z = (float)((double)g.delta_voxel_slice * (g.num_slices - 1) / 2.0);
+  o.inv_M = (float)(1.0 / (double)g.magnification);
+  o.sid = (float)((double)g.source_detector_dist / (double)g.magnification);
+  o.area = (float)((double)g.delta_voxel_row * (double)g.delta_voxel);
+  o.inv_sdd = (float)(1.0 / (double)g.source_detector_dist);
+  return o;
+}
+
+// ── storage types ──────────────────────────────────────────────────────────
+__device__ __forceinline__ float to_f32(float v) { return v; }
+__device__ __forceinline__ float to_f32(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_f32(__half v) { return __half2float(v); }
+
+template <typename T> __device__ __forceinline__ T from_f32(float v);
+template <> __device__ __forceinline__ float from_f32<float>(float v) { return v; }
+template <> __device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float v) {
+  return __float2bfloat16_rn(v);
+}
+template <> __device__ __forceinline__ __half from_f32<__half>(float v) {
+  return __float2half_rn(v);
+}
+
+// ── geometry chains ────────────────────────────────────────────────────────
+// Un-rotated pixel centre (x, y) relative to iso (note the (i, j) -> (y, x)
+// order of the reference).
+__device__ __forceinline__ void pixel_xy(const Geo &g, int pix, float &xt, float &yt) {
+  int row = pix / g.NC;
+  int col = pix - row * g.NC;
+  yt = __fmul_rn(g.dvr, __fsub_rn((float)row, g.rc_row));
+  xt = __fmul_rn(g.dv, __fsub_rn((float)col, g.rc_col));
+}
+
+// Trapezoid weight of channel tap n (horizontal_fan.py:51-71): the overlap
+// of the projected voxel with detector cell n, zeroed off the detector.
+__device__ __forceinline__ float tap_weight(float n_p, int n, float half_w1, float lmax,
+                                            float ws, int C) {
+  float a = fmaxf(__fsub_rn(half_w1, fabsf(__fsub_rn(n_p, (float)n))), 0.f);
+  a = __fmul_rn(fminf(a, lmax), ws);
+  return (n >= 0 && n < C) ? a : 0.f;
+}
+
+// Per-view constants of the parallel chain (W and the weight scale depend
+// on the view only).
+struct ParView {
+  float c, s, half_w1, lmax, ws;
+};
+
+__device__ __forceinline__ ParView parallel_view(const Geo &g, float angle) {
+  ParView o;
+  o.c = cosf(angle);
+  o.s = sinf(angle);
+  float fp = fmaxf(__fmul_rn(fabsf(o.c), g.dv), __fmul_rn(fabsf(o.s), g.dvr));
+  float W = __fdiv_rn(fp, g.ddc);
+  o.half_w1 = __fdiv_rn(__fadd_rn(W, 1.f), 2.f);
+  o.lmax = fminf(W, 1.f);
+  o.ws = __fdiv_rn(g.area, fp);
+  return o;
+}
+
+// Continuous channel coordinate of a pixel in a parallel view.
+__device__ __forceinline__ float parallel_np(const Geo &g, const ParView &pv, float xt,
+                                             float yt) {
+  float x = __fsub_rn(__fmul_rn(pv.c, xt), __fmul_rn(pv.s, yt));
+  return __fadd_rn(__fdiv_rn(__fadd_rn(x, g.offc), g.ddc), g.det_cc);
+}
+
+// Cone: per (view, pixel) horizontal fan data + the vertical affine pair.
+struct ConeVP {
+  float n_p, half_w1, lmax, ws;  // horizontal fan
+  float mag, m0, w_r;            // vertical fan: m(k) = m0 + w_r * k
+  int ctr;
+};
+
+__device__ __forceinline__ ConeVP cone_vp(const Geo &g, float angle, float c, float s,
+                                          float z_off, float xt, float yt) {
+  ConeVP o;
+  float x = __fsub_rn(__fmul_rn(c, xt), __fmul_rn(s, yt));
+  float y = __fadd_rn(__fmul_rn(s, xt), __fmul_rn(c, yt));
+  float mag = __fdiv_rn(1.f, __fsub_rn(g.inv_M, __fdiv_rn(y, g.sdd)));
+  float u, theta;
+  if (!g.curved) {
+    u = __fmul_rn(mag, x);
+    theta = atan2f(u, g.sdd);
+  } else {
+    u = __fmul_rn(g.sdd, atan2f(x, __fsub_rn(g.sid, y)));
+    theta = __fdiv_rn(u, g.sdd);
+  }
+  o.n_p = __fadd_rn(__fdiv_rn(__fadd_rn(u, g.offc), g.ddc), g.det_cc);
+  float da = __fsub_rn(angle, theta);
+  float fp = fmaxf(__fmul_rn(fabsf(cosf(da)), g.dv), __fmul_rn(fabsf(sinf(da)), g.dvr));
+  float W = __fmul_rn(mag, __fdiv_rn(fp, g.ddc));
+  if (!g.curved) W = __fdiv_rn(W, cosf(theta));
+  o.half_w1 = __fdiv_rn(__fadd_rn(W, 1.f), 2.f);
+  o.lmax = fminf(W, 1.f);
+  o.ws = __fdiv_rn(g.area, fp);
+  o.ctr = (int)fminf(fmaxf(rintf(o.n_p), -1.0e6f), 1.0e6f);
+  o.mag = mag;
+  o.w_r = __fdiv_rn(__fmul_rn(mag, g.dvs), g.ddr);
+  float z0 = __fsub_rn(z_off, g.half_z);
+  o.m0 = __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(mag, z0), g.offr), g.ddr), g.det_cr);
+  return o;
+}
+
+// 1 / cos(phi) for the voxel at global slice k of a cone (view, pixel):
+// sqrt(1 + (v / SDD)^2) with v = mag * z_k, the same quantity as the
+// reference's 1 / cos(atan2(v, SDD)) (exactly 1 at SDD = inf).
+__device__ __forceinline__ float cone_inv_cos(const Geo &g, float mag, float z_off, float k) {
+  float z = __fadd_rn(__fmul_rn(g.dvs, __fsub_rn(k, g.slice_c)), z_off);
+  float t = __fmul_rn(__fmul_rn(mag, z), g.inv_sdd);
+  return sqrtf(fmaf(t, t, 1.f));
+}
+
+}  // namespace mbir

@@ -1,0 +1,552 @@
+// VCD subset-step kernels for sm_100a.
+//
+// One subset update (tomography_model.py:2508-2657) runs as a short chain of
+// launches on one stream, with no host synchronization:
+//   1. gradient      back projection of (w * e) at the subset's cylinders,
+//                    view-chunked partials (projectors.cuh)
+//   2. direction     chunk reduction + qGGMRF surrogate gradient/Hessian
+//                    (qggmrf.py:77-183) + the preconditioned direction
+//                    (tomography_model.py:54-57) + prior line-term partials
+//   2'. DC damping   (cone) per-slice H^-1-weighted gradient means and the
+//                    damped direction (cone_beam.py:48-55)
+//   3. forward       A delta with the line-search reductions fused into the
+//                    epilogue (sum w e Ad, sum w Ad^2) and Ad stored in the
+//                    storage precision
+//   4. alpha         one CTA: FP64 reduction of all partials, the clamped
+//                    step (tomography_model.py:2612-2617)
+//   5. update        recon += alpha delta with per-slice sum of squares and
+//                    ell1, then e -= alpha Ad
+// Every reduction is a fixed-order tree over per-CTA partials, so a subset
+// update is bit-reproducible run to run.
+#pragma once
+
+#include "projectors.cuh"
+
+namespace mbir {
+
+constexpr float kF32Eps = 1.1920928955078125e-07f;
+
+struct VcdScalars {
+  float fmc;        // 1 / sigma_y^2
+  float a_min;      // T * sigma_x * eps_f32
+  float t_sx;       // T * sigma_x
+  float q_minus_p;  // q - p
+  float p_minus_2;  // p - 2
+  float two_sx_p;   // 2 * sigma_x ** p
+  float q_over_p;   // q / p
+  float two_b[6];   // 2 * b[j]  (get_2_b_tilde's b_for_delta * 2.0)
+  float b[6];
+  float max_alpha;
+};
+
+inline VcdScalars make_scalars(const mbir_vcd_params &p) {
+  VcdScalars s;
+  s.fmc = p.fm_constant;
+  s.a_min = (float)((double)p.T * (double)p.sigma_x * 1.1920928955078125e-07);
+  s.t_sx = (float)((double)p.T * (double)p.sigma_x);
+  s.q_minus_p = (float)((double)p.q - (double)p.p);
+  s.p_minus_2 = (float)((double)p.p - 2.0);
+  s.two_sx_p = (float)(2.0 * pow((double)p.sigma_x, (double)p.p));
+  s.q_over_p = (float)((double)p.q / (double)p.p);
+  for (int j = 0; j < 6; ++j) {
+    s.b[j] = p.b[j];
+    s.two_b[j] = (float)((double)p.b[j] * 2.0);
+  }
+  s.max_alpha = p.max_alpha;
+  return s;
+}
+
+// b_tilde_by_definition (qggmrf.py:35-57) without the factor b * 2.
+__device__ __forceinline__ float b_tilde(float delta, const VcdScalars &s) {
+  const float ad = fmaxf(fabsf(delta), s.a_min);
+  const float ds = __fdiv_rn(ad, s.t_sx);
+  const float dqp = powf(ds, s.q_minus_p);
+  const float dp2 = powf(ad, s.p_minus_2);
+  float num = __fdiv_rn(dp2, s.two_sx_p);
+  num = __fmul_rn(__fmul_rn(num, dqp), __fadd_rn(s.q_over_p, dqp));
+  const float den = __fadd_rn(1.f, dqp);
+  return __fdiv_rn(num, __fmul_rn(den, den));
+}
+
+// Block-wide sum of two doubles; returns the totals in thread 0.
+__device__ __forceinline__ void block_sum2(double &a, double &b) {
+  __shared__ double sa[kThreads / 32], sb[kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    sa[warp] = a;
+    sb[warp] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      ta += sa[w];
+      tb += sb[w];
+    }
+    a = ta;
+    b = tb;
+  }
+}
+
+// ── 2. direction ─────────────────────────────────────────────────────────
+// Thread per (pixel p, slice l).  DC = 0: writes delta and the prior
+// line-term partials.  DC = 1: writes g, 1/h, g_p, h_p for the damping pass.
+template <bool DC>
+__global__ void __launch_bounds__(kThreads)
+vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int NC,
+                     const float *__restrict__ part, int nchunks,
+                     const float *__restrict__ flat, const float *__restrict__ H,
+                     VcdScalars sc, float *__restrict__ delta, float *__restrict__ gbuf,
+                     float *__restrict__ hinv, float *__restrict__ gpbuf,
+                     float *__restrict__ hpbuf, double *__restrict__ partials) {
+  const size_t n = (size_t)P * S;
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  double pl = 0.0, pq = 0.0;
+  if (i < n) {
+    const int p = (int)(i / S), l = (int)(i - (size_t)p * S);
+    float bp = 0.f;
+    for (int c = 0; c < nchunks; ++c) bp += part[(size_t)c * n + i];
+    const int pixel = (int)pix[p];
+    const float g_f = __fmul_rn(-sc.fmc, bp);
+    const float h_f = __fmul_rn(sc.fmc, H[(size_t)pixel * S + l]);
+    // qGGMRF surrogate (qggmrf.py:117-183): slice term with reflected ends,
+    // then the 4 clamped in-plane neighbours.
+    const float *cyl = flat + (size_t)pixel * S;
+    const float xs = cyl[l];
+    const float dp = (l + 1 < S) ? __fsub_rn(cyl[l + 1], xs) : 0.f;  // delta[l+1]
+    const float dm = (l > 0) ? __fsub_rn(xs, cyl[l - 1]) : 0.f;      // delta[l]
+    const float bt_p = __fmul_rn(2.f, b_tilde(dp, sc));
+    const float bt_m = __fmul_rn(2.f, b_tilde(dm, sc));
+    float g_p = __fadd_rn(__fmul_rn(-sc.b[4], __fmul_rn(bt_p, dp)),
+                          __fmul_rn(sc.b[5], __fmul_rn(bt_m, dm)));
+    float h_p = __fadd_rn(__fmul_rn(sc.b[4], bt_p), __fmul_rn(sc.b[5], bt_m));
+    const int row = pixel / NC, col = pixel - (pixel / NC) * NC;
+    const int dr[4] = {1, -1, 0, 0}, dc[4] = {0, 0, 1, -1};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int rr = min(max(row + dr[k], 0), NR - 1);
+      const int cc = min(max(col + dc[k], 0), NC - 1);
+      const float d = __fsub_rn(xs, flat[((size_t)rr * NC + cc) * S + l]);
+      const float w = __fmul_rn(sc.two_b[k], b_tilde(d, sc));
+      g_p = __fadd_rn(g_p, __fmul_rn(w, d));
+      h_p = __fadd_rn(h_p, w);
+    }
+    if (!DC) {
+      const float dl = -__fdiv_rn(__fadd_rn(g_f, g_p), __fadd_rn(h_f, h_p));
+      delta[i] = dl;
+      pl = (double)__fmul_rn(g_p, dl);
+      pq = (double)__fmul_rn(__fmul_rn(h_p, dl), dl);
+    } else {
+      gbuf[i] = __fadd_rn(g_f, g_p);
+      hinv[i] = __fdiv_rn(1.f, __fadd_rn(h_f, h_p));
+      gpbuf[i] = g_p;
+      hpbuf[i] = h_p;
+    }
+  }
+  if (!DC) {
+    block_sum2(pl, pq);
+    if (threadIdx.x == 0) {
+      partials[2 * blockIdx.x] = pl;
+      partials[2 * blockIdx.x + 1] = pq;
+    }
+  }
+}
+
+// ── 2'. DC damping ───────────────────────────────────────────────────────
+// Per-slice sums over pixel chunks: part[chunk][l] = (sum h^-1 g, sum h^-1).
+__global__ void vcd_dc_sums_kernel(int P, int S, int pchunk, const float *__restrict__ gbuf,
+                                   const float *__restrict__ hinv, double *__restrict__ part) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  const int chunk = blockIdx.y;
+  if (l >= S) return;
+  const int p0 = chunk * pchunk, p1 = min(P, p0 + pchunk);
+  double num = 0.0, den = 0.0;
+  for (int p = p0; p < p1; ++p) {
+    const size_t i = (size_t)p * S + l;
+    const float hi = hinv[i];
+    num += (double)__fmul_rn(hi, gbuf[i]);
+    den += (double)hi;
+  }
+  part[((size_t)chunk * S + l) * 2] = num;
+  part[((size_t)chunk * S + l) * 2 + 1] = den;
+}
+
+// delta = -(g - (1 - s_l) * gbar_l) * h^-1, plus the prior line-term partials.
+__global__ void __launch_bounds__(kThreads)
+vcd_dc_direction_kernel(int P, int S, int nchunks, const double *__restrict__ sums,
+                        const float *__restrict__ s_prof, const float *__restrict__ gbuf,
+                        const float *__restrict__ hinv, const float *__restrict__ gpbuf,
+                        const float *__restrict__ hpbuf, float *__restrict__ delta,
+                        double *__restrict__ partials) {
+  const size_t n = (size_t)P * S;
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  double pl = 0.0, pq = 0.0;
+  if (i < n) {
+    const int l = (int)(i % S);
+    double num = 0.0, den = 0.0;
+    for (int c = 0; c < nchunks; ++c) {
+      num += sums[((size_t)c * S + l) * 2];
+      den += sums[((size_t)c * S + l) * 2 + 1];
+    }
+    const float gbar = (float)(num / den);
+    const float damp = __fmul_rn(__fsub_rn(1.f, s_prof[l]), gbar);
+    const float dl = __fmul_rn(-__fsub_rn(gbuf[i], damp), hinv[i]);
+    delta[i] = dl;
+    const float g_p = gpbuf[i], h_p = hpbuf[i];
+    pl = (double)__fmul_rn(g_p, dl);
+    pq = (double)__fmul_rn(__fmul_rn(h_p, dl), dl);
+  }
+  block_sum2(pl, pq);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = pl;
+    partials[2 * blockIdx.x + 1] = pq;
+  }
+}
+
+// ── 3. forward epilogue: line search + Ad store ───────────────────────────
+template <typename T>
+struct LineSearchEpi {
+  const T *e;
+  const float *es;
+  const T *w;
+  const float *wsc;
+  T *ad;
+  int C, R;
+  double *partials;
+  int with_sums;
+  double fl, fq;
+  __device__ __forceinline__ bool channel_fastest() const { return false; }
+  __device__ __forceinline__ void begin() {
+    fl = 0.0;
+    fq = 0.0;
+  }
+  __device__ __forceinline__ void cell(int v, int c, int m, float val) {
+    const size_t i = ((size_t)v * C + c) * R + m;
+    const float scale = __ldg(es + v);
+    const T stored = from_f32<T>(__fdiv_rn(val, scale));
+    ad[i] = stored;
+    if (!with_sums) return;
+    const float adv = __fmul_rn(to_f32(stored), scale);
+    const float ev = __fmul_rn(to_f32(e[i]), scale);
+    if (w != nullptr) {
+      const float wv = __fmul_rn(to_f32(w[i]), __ldg(wsc + v));
+      fl += (double)__fmul_rn(__fmul_rn(wv, ev), adv);
+      fq += (double)__fmul_rn(__fmul_rn(adv, adv), wv);
+    } else {
+      fl += (double)__fmul_rn(ev, adv);
+      fq += (double)__fmul_rn(adv, adv);
+    }
+  }
+  __device__ __forceinline__ void end(int slot) {
+    if (!with_sums) return;
+    block_sum2(fl, fq);
+    if (threadIdx.x == 0) {
+      partials[2 * slot] = fl;
+      partials[2 * slot + 1] = fq;
+    }
+  }
+};
+
+// ── 4. alpha ─────────────────────────────────────────────────────────────
+// One CTA.  prior: np pairs (pl, pq); fwd: nf pairs (fl, fq).
+__global__ void __launch_bounds__(kThreads)
+vcd_alpha_kernel(const double *__restrict__ prior, int np, const double *__restrict__ fwd, int nf,
+                 float fmc, float max_alpha, float *__restrict__ alpha_out,
+                 float *__restrict__ alpha_user) {
+  double pl = 0.0, pq = 0.0, fl = 0.0, fq = 0.0;
+  for (int i = threadIdx.x; i < np; i += kThreads) {
+    pl += prior[2 * i];
+    pq += prior[2 * i + 1];
+  }
+  for (int i = threadIdx.x; i < nf; i += kThreads) {
+    fl += fwd[2 * i];
+    fq += fwd[2 * i + 1];
+  }
+  block_sum2(pl, pq);
+  block_sum2(fl, fq);
+  if (threadIdx.x == 0) {
+    // tomography_model.py:2612-2617, with the sums in FP64.
+    const double num = (double)fmc * fl - pl;
+    const double den = (double)fmc * fq + pq + (double)kF32Eps;
+    double a = num / den;
+    a = fmin(fmax(a, (double)kF32Eps), (double)max_alpha);
+    alpha_out[0] = (float)a;
+    if (alpha_user) alpha_user[0] = (float)a;
+  }
+}
+
+// Positivity: delta = max(-x / (alpha + eps), delta) (tomography_model.py:2624-2633).
+__global__ void vcd_positivity_kernel(int P, int S, const int64_t *__restrict__ pix,
+                                      const float *__restrict__ flat,
+                                      const float *__restrict__ alpha, float *__restrict__ delta) {
+  const size_t n = (size_t)P * S;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = (int)(i / S), l = (int)(i - (size_t)p * S);
+  const float pos_c = __fdiv_rn(1.f, __fadd_rn(alpha[0], kF32Eps));
+  const float x = flat[(size_t)pix[p] * S + l];
+  delta[i] = fmaxf(__fmul_rn(-pos_c, x), delta[i]);
+}
+
+// ── 5. update ────────────────────────────────────────────────────────────
+// Recon scatter-add over a (pixel chunk, slice block) tile; per-slice sum of
+// squares and ell1 partials.
+__global__ void __launch_bounds__(kThreads)
+vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pix,
+                        const float *__restrict__ delta, const float *__restrict__ alpha,
+                        float *__restrict__ flat, double *__restrict__ sq_part,
+                        double *__restrict__ l1_part) {
+  const int l = blockIdx.y * kThreads + threadIdx.x;
+  const int chunk = blockIdx.x;
+  const int p0 = chunk * pchunk, p1 = min(P, p0 + pchunk);
+  const float a = alpha[0];
+  double sq = 0.0, l1 = 0.0;
+  if (l < S) {
+    for (int p = p0; p < p1; ++p) {
+      const float ds = __fmul_rn(a, delta[(size_t)p * S + l]);
+      float *x = flat + (size_t)pix[p] * S + l;
+      *x = __fadd_rn(*x, ds);
+      sq += (double)__fmul_rn(ds, ds);
+      l1 += (double)fabsf(ds);
+    }
+    sq_part[(size_t)chunk * S + l] = sq;
+  }
+  double dummy = 0.0;
+  block_sum2(l1, dummy);
+  if (threadIdx.x == 0) l1_part[(size_t)blockIdx.y * gridDim.x + chunk] = l1;
+}
+
+// accum[0] += ell1, accum[1] += alpha, accum[2 + l] += sum_p ds^2.
+__global__ void __launch_bounds__(kThreads)
+vcd_finish_kernel(int S, int nchunks, int nl1, const double *__restrict__ sq_part,
+                  const double *__restrict__ l1_part, const float *__restrict__ alpha,
+                  double *__restrict__ accum) {
+  for (int l = threadIdx.x; l < S; l += kThreads) {
+    double s = 0.0;
+    for (int c = 0; c < nchunks; ++c) s += sq_part[(size_t)c * S + l];
+    accum[2 + l] += s;
+  }
+  double l1 = 0.0, dummy = 0.0;
+  for (int i = threadIdx.x; i < nl1; i += kThreads) l1 += l1_part[i];
+  block_sum2(l1, dummy);
+  if (threadIdx.x == 0) {
+    accum[0] += l1;
+    accum[1] += (double)alpha[0];
+  }
+}
+
+// e -= alpha * Ad over the whole resident sinogram (both share the per-view
+// scale, so the update is scale-free in the stored units).
+template <typename T>
+__global__ void vcd_sino_update_kernel(size_t n, const float *__restrict__ alpha,
+                                       T *__restrict__ e, const T *__restrict__ ad) {
+  const float a = alpha[0];
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float ev = to_f32(e[i]);
+    const float dv = to_f32(ad[i]);
+    e[i] = from_f32<T>(__fsub_rn(ev, __fmul_rn(a, dv)));
+  }
+}
+
+template <>
+__global__ void vcd_sino_update_kernel<float>(size_t n, const float *__restrict__ alpha,
+                                              float *__restrict__ e,
+                                              const float *__restrict__ ad) {
+  const float a = alpha[0];
+  const size_t n4 = n / 4;
+  float4 *e4 = reinterpret_cast<float4 *>(e);
+  const float4 *d4 = reinterpret_cast<const float4 *>(ad);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float4 ev = e4[i];
+    const float4 dv = d4[i];
+    ev.x = __fsub_rn(ev.x, __fmul_rn(a, dv.x));
+    ev.y = __fsub_rn(ev.y, __fmul_rn(a, dv.y));
+    ev.z = __fsub_rn(ev.z, __fmul_rn(a, dv.z));
+    ev.w = __fsub_rn(ev.w, __fmul_rn(a, dv.w));
+    e4[i] = ev;
+  }
+  for (size_t i = n4 * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    e[i] = __fsub_rn(e[i], __fmul_rn(a, ad[i]));
+}
+
+// ── iteration statistics / init / conversion ─────────────────────────────
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+stats_sino_kernel(int V, int CR, const T *__restrict__ e, const float *__restrict__ es,
+                  const T *__restrict__ w, const float *__restrict__ wsc,
+                  double *__restrict__ part) {
+  double a = 0.0, b = 0.0, c = 0.0;
+  const size_t n = (size_t)V * CR;
+  for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * kThreads) {
+    const int v = (int)(i / CR);
+    const float ev = __fmul_rn(to_f32(e[i]), es[v]);
+    const float e2 = __fmul_rn(ev, ev);
+    if (w != nullptr) {
+      const float wv = __fmul_rn(to_f32(w[i]), wsc[v]);
+      a += (double)__fmul_rn(e2, wv);
+      b += (double)wv;
+    } else {
+      a += (double)e2;
+      b += 1.0;
+    }
+    c += (double)e2;
+  }
+  double dummy = 0.0;
+  block_sum2(a, b);
+  block_sum2(c, dummy);
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = a;
+    part[3 * blockIdx.x + 1] = b;
+    part[3 * blockIdx.x + 2] = c;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+stats_l1_kernel(size_t n, const float *__restrict__ x, double *__restrict__ part) {
+  double a = 0.0, dummy = 0.0;
+  for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * kThreads)
+    a += (double)fabsf(x[i]);
+  block_sum2(a, dummy);
+  if (threadIdx.x == 0) part[blockIdx.x] = a;
+}
+
+__global__ void __launch_bounds__(kThreads)
+stats_finish_kernel(int nsino, const double *__restrict__ sino_part, int nl1,
+                    const double *__restrict__ l1_part, double *__restrict__ out) {
+  double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
+  for (int i = threadIdx.x; i < nsino; i += kThreads) {
+    a += sino_part[3 * i];
+    b += sino_part[3 * i + 1];
+    c += sino_part[3 * i + 2];
+  }
+  for (int i = threadIdx.x; i < nl1; i += kThreads) d += l1_part[i];
+  block_sum2(a, b);
+  block_sum2(c, d);
+  if (threadIdx.x == 0) {
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
+    out[3] = d;
+  }
+}
+
+// Error init: dots (sum w f f, sum w f y) per block.
+__global__ void __launch_bounds__(kThreads)
+init_dots_kernel(size_t n, const float *__restrict__ y, const float *__restrict__ f,
+                 const float *__restrict__ w, double *__restrict__ part) {
+  double ff = 0.0, fy = 0.0;
+  for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * kThreads) {
+    const float fv = f[i];
+    const float wf = w ? __fmul_rn(w[i], fv) : fv;
+    ff += (double)__fmul_rn(wf, fv);
+    fy += (double)__fmul_rn(wf, y[i]);
+  }
+  block_sum2(ff, fy);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = ff;
+    part[2 * blockIdx.x + 1] = fy;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+init_alpha_kernel(int nb, const double *__restrict__ part, int scale, double *__restrict__ alpha) {
+  double ff = 0.0, fy = 0.0;
+  for (int i = threadIdx.x; i < nb; i += kThreads) {
+    ff += part[2 * i];
+    fy += part[2 * i + 1];
+  }
+  block_sum2(ff, fy);
+  if (threadIdx.x == 0) {
+    // The reference forms alpha from FP32 sums and takes it to the host as
+    // a python float (tomography_model.py:1700-1706).
+    alpha[0] = (ff > 0.0 && scale) ? (double)(float)(fy / ff) : 1.0;
+  }
+}
+
+__global__ void init_error_kernel(size_t n, const float *__restrict__ y,
+                                  const float *__restrict__ f, const double *__restrict__ alpha,
+                                  float *__restrict__ e) {
+  const float a = (float)alpha[0];
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    e[i] = __fsub_rn(y[i], __fmul_rn(a, f[i]));
+}
+
+__global__ void fill_kernel(int n, float v, float *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = v;
+}
+
+// Per-view max |value| of an f32 VRC sinogram -> scale (f16 storage).
+__global__ void __launch_bounds__(kThreads)
+view_scale_kernel(int RC, const float *__restrict__ src, float target, float *__restrict__ scale) {
+  const int v = blockIdx.x;
+  float m = 0.f;
+  for (int i = threadIdx.x; i < RC; i += kThreads) m = fmaxf(m, fabsf(src[(size_t)v * RC + i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  __shared__ float sm[kThreads / 32];
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < kThreads / 32; ++w) t = fmaxf(t, sm[w]);
+    scale[v] = t > 0.f ? t / target : 1.f;
+  }
+}
+
+// Tiled transpose per view: f32 (R, C) <-> T (C, R) with scale.
+template <typename T>
+__global__ void vrc_to_vcr_kernel(int R, int C, const float *__restrict__ src,
+                                  const float *__restrict__ scale, T *__restrict__ dst) {
+  __shared__ float t[32][33];
+  const int v = blockIdx.z;
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  const float inv = scale ? 1.f / scale[v] : 1.f;
+  const float *s = src + (size_t)v * R * C;
+  T *d = dst + (size_t)v * R * C;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = r0 + j, c = c0 + threadIdx.x;
+    if (r < R && c < C) t[j][threadIdx.x] = s[(size_t)r * C + c];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int c = c0 + j, r = r0 + threadIdx.x;
+    if (r < R && c < C) {
+      const float val = t[threadIdx.x][j];
+      d[(size_t)c * R + r] = from_f32<T>(scale ? __fmul_rn(val, inv) : val);
+    }
+  }
+}
+
+template <typename T>
+__global__ void vcr_to_vrc_kernel(int R, int C, const T *__restrict__ src,
+                                  const float *__restrict__ scale, float *__restrict__ dst) {
+  __shared__ float t[32][33];
+  const int v = blockIdx.z;
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const float sc = scale ? scale[v] : 1.f;
+  const T *s = src + (size_t)v * R * C;
+  float *d = dst + (size_t)v * R * C;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int c = c0 + j, r = r0 + threadIdx.x;
+    if (r < R && c < C) t[j][threadIdx.x] = __fmul_rn(to_f32(s[(size_t)c * R + r]), sc);
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = r0 + j, c = c0 + threadIdx.x;
+    if (r < R && c < C) d[(size_t)r * C + c] = t[threadIdx.x][j];
+  }
+}
+
+}  // namespace mbir

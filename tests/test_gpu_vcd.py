@@ -1,0 +1,186 @@
+"""VCD reconstruction parity on the GPU.
+
+* Seeded recon() against the reference's own seeded recon (golden traces):
+  relative L2 <= 1e-4 on the volume after the fixed iteration count, and
+  the fm_rmse / alpha traces to 1e-4 (north_star reconstruction bar).
+* The same against the FP64 oracle.
+* Mixed-precision storage (bfloat16, float16) against the FP64 oracle at
+  relative L2 <= 1e-3.
+* Bitwise reproducibility and the subset-updater / partition seams.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import mbirtorch_b200 as mb
+from conftest import load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+GRANULARITY = [1, 2, 4, 8, 16, 32, 64, 128, 128, 128, 128]
+SEQUENCE = [2, 4, 6] + [7, 8, 9, 10] * 25
+
+
+def _model(name, d):
+    V = d['sino'].shape[0]
+    if name.startswith('recon_parallel'):
+        m = mb.ParallelBeamModel(d['sino'].shape, np.linspace(0, np.pi, V, endpoint=False))
+    else:
+        zs = d['z_shifts'] if name == 'recon_cone_helical' else None
+        ang = np.linspace(0, (4 if name == 'recon_cone_helical' else 2) * np.pi, V,
+                          endpoint=False)
+        m = mb.ConeBeamModel(d['sino'].shape, ang, 64.0, 32.0, helical_z_shifts=zs)
+    m.set_params(no_warning=True, verbose=0)
+    if name == 'recon_parallel_weighted':
+        m.set_params(no_warning=True, positivity_flag=True)
+    return m
+
+
+def _run(name, storage='float32'):
+    d = load_golden(f'{name}.npz')
+    m = _model(name, d)
+    m.set_storage_precision(storage)
+    np.random.seed(int(d['seed']))
+    w = d['weights'] if 'weights' in d.files else None
+    rec, rd = m.recon(d['sino'], weights=w, max_iterations=int(d['max_iterations']),
+                      stop_threshold_change_pct=0, logfile_path=None, print_logs=False)
+    return d, m, rec, rd
+
+
+def _oracle(name, m, d):
+    from oracle import OracleGeometry, vcd
+    g = m._geometry()
+    og = OracleGeometry(
+        num_det_rows=g.num_det_rows, num_det_channels=g.num_det_channels,
+        num_recon_rows=g.num_recon_rows, num_recon_cols=g.num_recon_cols,
+        num_slices=g.num_slices, delta_det_channel=g.delta_det_channel,
+        delta_det_row=g.delta_det_row, det_channel_offset=g.det_channel_offset,
+        det_row_offset=g.det_row_offset, delta_voxel=g.delta_voxel,
+        delta_voxel_row=g.delta_voxel_row, delta_voxel_slice=g.delta_voxel_slice,
+        recon_slice_offset=g.recon_slice_offset, magnification=g.magnification,
+        source_detector_dist=g.source_detector_dist,
+        use_curved_detector=bool(g.use_curved_detector), psf_radius=g.psf_radius,
+        bp_psf_radius=g.bp_psf_radius)
+    kind = 'cone' if name.startswith('recon_cone') else 'parallel'
+    prob = vcd.Problem(kind, og, m._view_params_array(), m.get_params('recon_shape'),
+                       source_iso_dist=32.0)
+    np.random.seed(int(d['seed']))
+    parts = [vcd.pixel_partition(prob.recon_shape, n) for n in GRANULARITY]
+    seq = vcd.partition_sequence(SEQUENCE, int(d['max_iterations']))
+    w = d['weights'] if 'weights' in d.files else None
+    dc = vcd.dc_damping_profile(prob) if kind == 'cone' else None
+    return vcd.recon(prob, d['sino'], d['reg'][0], d['reg'][1], parts, seq, weights=w,
+                     dc_profile=dc, positivity=w is not None)
+
+
+NAMES = ["recon_parallel", "recon_parallel_weighted", "recon_cone", "recon_cone_helical"]
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_recon_matches_reference_and_oracle(name):
+    d, m, rec, rd = _run(name)
+    rp = rd['recon_params']
+    np.testing.assert_allclose(rp['regularization_params']['sigma_y'], d['reg'][0], rtol=1e-6)
+    assert rel_l2(rec, d['recon']) <= 1e-4
+    np.testing.assert_allclose(rp['fm_rmse'], d['fm_rmse'], rtol=1e-4)
+    np.testing.assert_allclose(rp['alpha_values'], d['alpha'], rtol=1e-4)
+    orec, _ = _oracle(name, m, d)
+    assert rel_l2(rec, orec) <= 1e-4
+    assert rp['num_iterations'] == int(d['max_iterations'])
+    assert len(rp['delta_norm_per_slice']) == int(d['max_iterations'])
+
+
+@pytest.mark.parametrize("storage", ["bfloat16", "float16"])
+@pytest.mark.parametrize("name", ["recon_parallel", "recon_cone", "recon_parallel_weighted"])
+def test_mixed_precision_vs_fp64_oracle(name, storage):
+    d, m, rec, _ = _run(name, storage)
+    orec, _ = _oracle(name, m, d)
+    assert rel_l2(rec, orec) <= 1e-3
+
+
+def test_recon_is_bitwise_reproducible():
+    _, _, r1, d1 = _run("recon_cone")
+    _, _, r2, d2 = _run("recon_cone")
+    assert np.array_equal(r1, r2)
+    assert d1['recon_params']['fm_rmse'] == d2['recon_params']['fm_rmse']
+
+
+def test_subset_updater_seam_matches_oracle_step():
+    """create_vcd_subset_updater on a (V, R, C) tensor: one subset step
+    against the FP64 oracle's SubsetUpdater from the same state."""
+    from oracle import vcd as ovcd
+    d = load_golden('recon_cone.npz')
+    m = _model('recon_cone', d)
+    m.auto_set_regularization_params(d['sino'])
+    rs = m.get_params('recon_shape')
+    rng = np.random.default_rng(5)
+    x0 = (0.1 * rng.random(rs)).astype(np.float32)
+    e0 = d['sino'] - m.forward_project(x0)
+    H = m.compute_hessian_diagonal()
+    upd = m.create_vcd_subset_updater(H, weights=1)
+    idx = np.sort(rng.choice(mb.gen_full_indices(rs), size=20, replace=False)).astype(np.int64)
+    flat = torch.as_tensor(x0.reshape(-1, rs[2]), device='cuda').clone()
+    err = torch.as_tensor(e0, device='cuda').clone()
+    flat, err, ell1, alpha, sumsq = upd(flat, err, torch.as_tensor(idx, device='cuda'))
+    prob = _oracle_problem(m)
+    sy, sx = m.get_params(['sigma_y', 'sigma_x'])
+    ou = ovcd.SubsetUpdater(prob, H.reshape(-1, rs[2]), None, sy, sx,
+                            dc_profile=ovcd.dc_damping_profile(prob))
+    oflat = x0.reshape(-1, rs[2]).astype(np.float64)
+    oerr = e0.astype(np.float64)
+    oell1, oalpha, osumsq = ou(oflat, oerr, idx)
+    assert abs(float(alpha) - oalpha) / oalpha <= 1e-4
+    assert rel_l2(flat.cpu().numpy(), oflat) <= 1e-5
+    assert rel_l2(err.cpu().numpy(), oerr) <= 1e-5
+    assert abs(float(ell1) - oell1) / oell1 <= 1e-4
+    assert rel_l2(sumsq.cpu().numpy(), osumsq) <= 1e-4
+
+
+def _oracle_problem(m):
+    from oracle import OracleGeometry, vcd
+    g = m._geometry()
+    og = OracleGeometry(
+        num_det_rows=g.num_det_rows, num_det_channels=g.num_det_channels,
+        num_recon_rows=g.num_recon_rows, num_recon_cols=g.num_recon_cols,
+        num_slices=g.num_slices, delta_det_channel=g.delta_det_channel,
+        delta_det_row=g.delta_det_row, det_channel_offset=g.det_channel_offset,
+        det_row_offset=g.det_row_offset, delta_voxel=g.delta_voxel,
+        delta_voxel_row=g.delta_voxel_row, delta_voxel_slice=g.delta_voxel_slice,
+        recon_slice_offset=g.recon_slice_offset, magnification=g.magnification,
+        source_detector_dist=g.source_detector_dist,
+        use_curved_detector=bool(g.use_curved_detector), psf_radius=g.psf_radius,
+        bp_psf_radius=g.bp_psf_radius)
+    kind = 'cone' if g.geometry == 1 else 'parallel'
+    return vcd.Problem(kind, og, m._view_params_array(), m.get_params('recon_shape'),
+                       source_iso_dist=m.get_params('source_iso_dist') if kind == 'cone'
+                       else None)
+
+
+def test_checkpoint_resume_matches_continuous_run():
+    """_vcd_recon's init_error_sinogram / fm_hessian resume path: 2 + 1
+    iterations equal 3 (same partition order)."""
+    d = load_golden('recon_parallel.npz')
+    m = _model('recon_parallel', d)
+    m.auto_set_regularization_params(d['sino'])
+    rs = m.get_params('recon_shape')
+    parts = [mb.gen_pixel_partition(rs, n) for n in (4, 16, 64)]
+    np.random.seed(1)
+    full, _ = m._vcd_recon(d['sino'], parts, np.array([0, 1, 2]), 0)
+    np.random.seed(1)
+    r1, _, ck = m._vcd_recon(d['sino'], parts, np.array([0, 1]), 0, return_checkpoint=True)
+    r2, _ = m._vcd_recon(d['sino'], parts, np.array([2]), 0, init_recon=r1,
+                         init_error_sinogram=ck['error_sinogram'], fm_hessian=ck['fm_hessian'])
+    assert rel_l2(r2.cpu().numpy(), full.cpu().numpy()) <= 1e-6
+
+
+def test_recon_simple_parallel_equals_model_path():
+    d = load_golden('recon_parallel.npz')
+    np.random.seed(3)
+    r1, _ = mb.recon_simple_parallel(d['sino'], np.linspace(0, np.pi, d['sino'].shape[0],
+                                                            endpoint=False), max_iterations=2)
+    np.random.seed(3)
+    m = mb.ParallelBeamModel(d['sino'].shape, np.linspace(0, np.pi, d['sino'].shape[0],
+                                                          endpoint=False))
+    r2, _ = m.recon(d['sino'], max_iterations=2)
+    assert rel_l2(r1, r2) <= 1e-6
