@@ -159,6 +159,17 @@ int32_t mbir_forward_project(const mbir_geometry *geom, const float *view_params
                              const int64_t *pixel_indices, float *sino_out,
                              int32_t out_layout, void *stream);
 
+/* Forward projection of whole cylinders read straight from a flat
+ * (N*N, num_slices) f32 volume at the rows pixel_indices[p] (no gathered
+ * copy); otherwise as mbir_forward_project with slice_start 0 and
+ * band_len num_slices.  Replaces the gather + sparse_forward_project of
+ * forward_project (tomography_model.py:1877-1909). */
+int32_t mbir_forward_project_volume(const mbir_geometry *geom, const float *view_params,
+                                    int32_t view_start, int32_t view_count,
+                                    const float *flat_volume, const int64_t *pixel_indices,
+                                    int64_t num_pixels, float *sino_out, int32_t out_layout,
+                                    void *stream);
+
 /* Workspace bytes mbir_back_project needs for this call shape. */
 size_t mbir_back_project_workspace_size(const mbir_geometry *geom,
                                         int32_t view_count, int64_t num_pixels,
@@ -181,7 +192,7 @@ int32_t mbir_back_project(const mbir_geometry *geom, const float *view_params,
 /* Layout / precision conversion of a whole sinogram between the public f32
  * VRC form and the resident VCR form in `dtype` with a per-view scale:
  * stored = value / scale[v].  direction 0: f32 VRC -> dtype VCR (computing
- * scale[v] when compute_scale != 0: 1 for f32/bf16, max|value_v| / 1024 for
+ * scale[v] when compute_scale != 0: 1 for f32/bf16, max|value_v| / 256 for
  * f16); direction 1: dtype VCR -> f32 VRC (reading scale). */
 int32_t mbir_sino_convert(int32_t direction, int32_t views, int32_t rows,
                           int32_t channels, const void *src, void *dst,
@@ -239,6 +250,17 @@ int32_t mbir_vcd_partition_pass(const mbir_geometry *geom,
                                 int64_t subset_pixels, const int32_t *order,
                                 double *accum, void *workspace,
                                 size_t workspace_bytes, void *stream);
+
+/* Re-form the resident error sinogram from the measured one:
+ * error = (y - A x) / err_scale[v] in `storage`, with y the FP32 sinogram
+ * in the (V, C, R) layout and x the flat (N*N, S) recon at pixel_indices.
+ * Part of the storage-precision layer (no counterpart in the reference,
+ * whose error sinogram is FP32 and updated in place only): it bounds the
+ * drift that in-place 16-bit updates accumulate. */
+int32_t mbir_vcd_refresh_error(const mbir_geometry *geom, const float *view_params,
+                               const float *flat_recon, const int64_t *pixel_indices,
+                               int64_t num_pixels, const float *y_vcr, void *error_sino,
+                               const float *err_scale, int32_t storage, void *stream);
 
 /* Per-iteration statistics in FP64 (device out[4]):
  *   out[0] = sum(w e^2)  (sum(e^2) without weights)

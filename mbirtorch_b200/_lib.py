@@ -85,6 +85,9 @@ SIGNATURES = {
     "mbir_timing_collect": (_i32, [_c.c_char_p, _i32, _vp, _vp, _i32]),
     "mbir_forward_project": (_i32, [_GP, _vp, _i32, _i32, _vp, _i64, _i32, _i32, _vp, _vp,
                                     _i32, _vp]),
+    "mbir_forward_project_volume": (_i32, [_GP, _vp, _i32, _i32, _vp, _vp, _i64, _vp, _i32,
+                                           _vp]),
+    "mbir_vcd_refresh_error": (_i32, [_GP, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i32, _vp]),
     "mbir_back_project_workspace_size": (_sz, [_GP, _i32, _i64, _i32]),
     "mbir_back_project": (_i32, [_GP, _vp, _i32, _i32, _vp, _i32, _vp, _i64, _i32, _i32, _i32,
                                  _vp, _vp, _sz, _vp]),

@@ -100,7 +100,7 @@ class _ChunkedResidualLoss(torch.autograd.Function):
             r = model.projector.forward(voxel_values, pixel_indices, view_start=v0,
                                         view_count=vc) - y[v0:v0 + vc]
             total += (r * r * weights[v0:v0 + vc]).sum(dtype=torch.float64)
-        return total.to(torch.float32)
+        return total
 
     @staticmethod
     def backward(ctx, grad_out):
@@ -120,7 +120,8 @@ class _ChunkedResidualLoss(torch.autograd.Function):
 
 def weighted_residual_loss(model, volume, y, weights=None, max_chunk_bytes=2 << 30):
     """sum w (A x - y)^2 for one volume (or a sum over a batch), with the
-    sinogram formed in view chunks of at most ``max_chunk_bytes``."""
+    sinogram formed in view chunks of at most ``max_chunk_bytes``.  The
+    projections are FP32; the loss is accumulated and returned in FP64."""
     model._require_cuda()
     vols, _ = _volumes(volume.to(device=model.torch_device, dtype=torch.float32))
     ys = y.to(device=model.torch_device, dtype=torch.float32)

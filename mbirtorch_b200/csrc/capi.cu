@@ -133,8 +133,9 @@ BackShape back_shape(const mbir_geometry *g, int view_count, long long P, int ba
   BackShape s;
   if (g->geometry == MBIR_CONE) {
     s.T = 32;
-    s.SPL = band <= 32 ? 1 : (band <= 64 ? 2 : 4);
-    s.smem = (size_t)(kThreads / 32) * g->num_det_rows * sizeof(float);
+    s.SPL = band <= 32 ? 1 : (band <= 64 ? 2 : (band <= 128 ? 4 : 8));
+    s.smem = (size_t)(kThreads / 32) * (g->num_det_rows + 2 * kPad) * sizeof(float) +
+             (size_t)(kThreads / 32) * 32 * sizeof(ConeRec);
   } else {
     if (band <= 8) { s.T = 8; s.SPL = 1; }
     else if (band <= 16) { s.T = 4; s.SPL = 4; }
@@ -168,36 +169,53 @@ size_t back_partial_bytes(const BackShape &s, long long P, int band) {
   return s.nchunks > 1 ? align_up((size_t)s.nchunks * P * band * sizeof(float)) : 0;
 }
 
-template <int CP, int SPL, typename RD>
+template <int CP, int SPL, int NT, typename RD>
 int launch_back_t(const Geo &geo, const mbir_geometry *g, const float *vp, int v_start,
                   int v_count, const BackShape &s, const RD &rd, const int64_t *pix, long long P,
                   int slice_start, int band, float *dst, cudaStream_t st, const char *what) {
   dim3 grid(s.blocks_x, s.nchunks);
   if (g->geometry == MBIR_CONE) {
-    auto k = back_cone_kernel<CP, SPL, RD>;
+    auto k = back_cone_kernel<CP, SPL, NT, RD>;
     if (s.smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     tpre(st);
     k<<<grid, kThreads, s.smem, st>>>(geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P,
                                       slice_start, band, s.slice_chunks, dst);
   } else {
     tpre(st);
-    back_parallel_kernel<CP, SPL, RD><<<grid, kThreads, 0, st>>>(
+    back_parallel_kernel<CP, SPL, NT, RD><<<grid, kThreads, 0, st>>>(
         geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P, band, s.T, s.slice_chunks, dst);
   }
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
 }
 
-template <int CP, typename RD>
+template <int CP, int NT, typename RD>
 int launch_back_spl(const Geo &geo, const mbir_geometry *g, const float *vp, int v_start,
                     int v_count, const BackShape &s, const RD &rd, const int64_t *pix,
                     long long P, int slice_start, int band, float *dst, cudaStream_t st,
                     const char *what) {
-  switch (s.SPL) {
-    case 1: return launch_back_t<CP, 1>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
-    case 2: return launch_back_t<CP, 2>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
-    default: return launch_back_t<CP, 4>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
+#define MBIR_BACK(SPLV) \
+  launch_back_t<CP, SPLV, NT>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what)
+  if (g->geometry == MBIR_CONE) {
+    switch (s.SPL) {
+      case 1: return MBIR_BACK(1);
+      case 2: return MBIR_BACK(2);
+      case 4: return MBIR_BACK(4);
+      default: return MBIR_BACK(8);
+    }
   }
+  return s.SPL == 1 ? MBIR_BACK(1) : MBIR_BACK(4);
+#undef MBIR_BACK
+}
+
+template <int CP, typename RD>
+int launch_back_nt(const Geo &geo, const mbir_geometry *g, const float *vp, int v_start,
+                   int v_count, const BackShape &s, const RD &rd, const int64_t *pix,
+                   long long P, int slice_start, int band, float *dst, cudaStream_t st,
+                   const char *what) {
+  if (g->psf_radius == 1)
+    return launch_back_spl<CP, 3>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
+  return launch_back_spl<CP, 0>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
 }
 
 // Back projection with a given reader into `out` (or chunk partials in
@@ -209,8 +227,8 @@ int run_back(const mbir_geometry *g, const float *vp, int v_start, int v_count, 
              const char *what = "back projection") {
   const Geo geo = make_geo(*g);
   float *dst = s.nchunks > 1 ? partials : out;
-  int rc = cp == 2 ? launch_back_spl<2>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what)
-                   : launch_back_spl<1>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
+  int rc = cp == 2 ? launch_back_nt<2>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what)
+                   : launch_back_nt<1>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
   if (rc) return rc;
   if (s.nchunks > 1 && reduce_into_out) {
     const size_t n = (size_t)P * band;
@@ -230,19 +248,20 @@ FwdShape fwd_shape(const mbir_geometry *g, int band) {
   fs.RPT = (fs.rows + fs.TG - 1) / fs.TG;
   const int G = kThreads / fs.TG;
   const int RS = fs.TG * fs.RPT + 1;
-  int cb = (int)(48 * 1024 / (sizeof(float) * (size_t)G * RS));
+  int cb = (int)(32 * 1024 / (sizeof(float) * (size_t)G * RS));
   cb = std::max(8, std::min(cb, 128));
   fs.CB = std::min(cb, g->num_det_channels);
   return fs;
 }
 
-template <bool CONE, typename EPI>
+template <bool CONE, int NT, typename EPI>
 int launch_forward(const mbir_geometry *g, const float *vp, int v_start, int v_count,
                    const float *values, long long P, int band, int slice_start, const int64_t *pix,
-                   const FwdShape &fs, const EPI &epi, cudaStream_t st, const char *what) {
+                   const FwdShape &fs, const EPI &epi, cudaStream_t st, const char *what,
+                   int by_pixel) {
   const Geo geo = make_geo(*g);
   const size_t smem = fs.smem_bytes();
-  auto k = forward_kernel<CONE, EPI>;
+  auto k = forward_kernel<CONE, NT, EPI>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
@@ -251,7 +270,8 @@ int launch_forward(const mbir_geometry *g, const float *vp, int v_start, int v_c
   }
   dim3 grid((g->num_det_channels + fs.CB - 1) / fs.CB, v_count);
   tpre(st);
-  k<<<grid, kThreads, smem, st>>>(geo, vp, v_start, values, (int)P, band, slice_start, pix, fs, epi);
+  k<<<grid, kThreads, smem, st>>>(geo, vp, v_start, values, (int)P, band, slice_start, pix, fs,
+                                  by_pixel, epi);
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
 }
@@ -259,11 +279,15 @@ int launch_forward(const mbir_geometry *g, const float *vp, int v_start, int v_c
 template <typename EPI>
 int run_forward(const mbir_geometry *g, const float *vp, int v_start, int v_count,
                 const float *values, long long P, int band, int slice_start, const int64_t *pix,
-                const EPI &epi, cudaStream_t st, const char *what = "forward projection") {
+                const EPI &epi, cudaStream_t st, const char *what = "forward projection",
+                int by_pixel = 0) {
   const FwdShape fs = fwd_shape(g, band);
-  if (g->geometry == MBIR_CONE)
-    return launch_forward<true>(g, vp, v_start, v_count, values, P, band, slice_start, pix, fs, epi, st, what);
-  return launch_forward<false>(g, vp, v_start, v_count, values, P, band, slice_start, pix, fs, epi, st, what);
+#define MBIR_FWD(CONEV, NTV) \
+  launch_forward<CONEV, NTV>(g, vp, v_start, v_count, values, P, band, slice_start, pix, fs, epi, st, what, by_pixel)
+  const bool r1 = g->psf_radius == 1;
+  if (g->geometry == MBIR_CONE) return r1 ? MBIR_FWD(true, 3) : MBIR_FWD(true, 0);
+  return r1 ? MBIR_FWD(false, 3) : MBIR_FWD(false, 0);
+#undef MBIR_FWD
 }
 
 int fwd_blocks(const mbir_geometry *g, int band, int v_count) {
@@ -503,6 +527,68 @@ int32_t mbir_forward_project(const mbir_geometry *geom, const float *view_params
                      slice_start, pixel_indices, epi, st);
 }
 
+int32_t mbir_forward_project_volume(const mbir_geometry *geom, const float *view_params,
+                                    int32_t view_start, int32_t view_count,
+                                    const float *flat_volume, const int64_t *pixel_indices,
+                                    int64_t num_pixels, float *sino_out, int32_t out_layout,
+                                    void *stream) {
+  int rc = validate_geometry(geom);
+  if (rc) return rc;
+  if (view_start < 0 || view_count < 0 || view_start + view_count > geom->num_views)
+    return fail(MBIR_ERR_INVALID, "view range [%d, %d) outside [0, %d)", view_start,
+                view_start + view_count, geom->num_views);
+  if (num_pixels < 0 || num_pixels >= (1LL << 31)) return fail(MBIR_ERR_INVALID, "bad num_pixels");
+  if (out_layout != MBIR_LAYOUT_VRC && out_layout != MBIR_LAYOUT_VCR)
+    return fail(MBIR_ERR_INVALID, "unknown layout %d", out_layout);
+  if (!view_params || !sino_out || (num_pixels > 0 && (!flat_volume || !pixel_indices)))
+    return fail(MBIR_ERR_INVALID, "NULL array argument");
+  if (view_count == 0) return MBIR_OK;
+  cudaStream_t st = as_stream(stream);
+  if (num_pixels == 0) {
+    cudaError_t e = cudaMemsetAsync(sino_out, 0,
+        (size_t)view_count * geom->num_det_rows * geom->num_det_channels * sizeof(float), st);
+    if (e != cudaSuccess) return fail(MBIR_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
+    return MBIR_OK;
+  }
+  StoreSino epi{sino_out, out_layout, geom->num_det_channels, geom->num_det_rows};
+  return run_forward(geom, view_params, view_start, view_count, flat_volume, num_pixels,
+                     geom->num_slices, 0, pixel_indices, epi, st, "forward projection", 1);
+}
+
+int32_t mbir_vcd_refresh_error(const mbir_geometry *geom, const float *view_params,
+                               const float *flat_recon, const int64_t *pixel_indices,
+                               int64_t num_pixels, const float *y_vcr, void *error_sino,
+                               const float *err_scale, int32_t storage, void *stream) {
+  int rc = validate_geometry(geom);
+  if (rc) return rc;
+  if (!view_params || !flat_recon || !pixel_indices || !y_vcr || !error_sino || !err_scale ||
+      num_pixels <= 0)
+    return fail(MBIR_ERR_INVALID, "bad refresh arguments");
+  cudaStream_t st = as_stream(stream);
+  const int C = geom->num_det_channels, R = geom->num_det_rows, V = geom->num_views;
+  const int S = geom->num_slices;
+  switch (storage) {
+    case MBIR_F32: {
+      RefreshEpi<float> epi{y_vcr, static_cast<float *>(error_sino), err_scale, C, R};
+      return run_forward(geom, view_params, 0, V, flat_recon, num_pixels, S, 0, pixel_indices,
+                         epi, st, "vcd error refresh", 1);
+    }
+    case MBIR_BF16: {
+      RefreshEpi<__nv_bfloat16> epi{y_vcr, static_cast<__nv_bfloat16 *>(error_sino), err_scale,
+                                    C, R};
+      return run_forward(geom, view_params, 0, V, flat_recon, num_pixels, S, 0, pixel_indices,
+                         epi, st, "vcd error refresh", 1);
+    }
+    case MBIR_F16: {
+      RefreshEpi<__half> epi{y_vcr, static_cast<__half *>(error_sino), err_scale, C, R};
+      return run_forward(geom, view_params, 0, V, flat_recon, num_pixels, S, 0, pixel_indices,
+                         epi, st, "vcd error refresh", 1);
+    }
+    default:
+      return fail(MBIR_ERR_INVALID, "unknown storage dtype %d", storage);
+  }
+}
+
 size_t mbir_back_project_workspace_size(const mbir_geometry *geom, int32_t view_count,
                                         int64_t num_pixels, int32_t band_len) {
   if (!geom || view_count <= 0 || num_pixels <= 0 || band_len <= 0) return 0;
@@ -579,7 +665,7 @@ int32_t mbir_sino_convert(int32_t direction, int32_t views, int32_t rows, int32_
       if (dtype == MBIR_F16) {
         tpre(st);
         view_scale_kernel<<<views, kThreads, 0, st>>>(R * C, static_cast<const float *>(src),
-                                                      1024.f, scale);
+                                                      256.f, scale);
         MBIR_CHECK_LAUNCH("view scale");
       } else {
         tpre(st);

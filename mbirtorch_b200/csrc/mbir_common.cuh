@@ -133,6 +133,29 @@ __device__ __forceinline__ float parallel_np(const Geo &g, const ParView &pv, fl
   return __fadd_rn(__fdiv_rn(__fadd_rn(x, g.offc), g.ddc), g.det_cc);
 }
 
+// Cone, first half of the chain: rotated pixel, magnification and the
+// continuous channel coordinate (all the forward projector's pixel scan
+// needs to decide whether a pixel reaches its channel block).
+struct ConeCenter {
+  float n_p, mag, u, y;
+  int ctr;
+};
+
+__device__ __forceinline__ ConeCenter cone_center(const Geo &g, float c, float s, float xt,
+                                                  float yt) {
+  ConeCenter o;
+  const float x = __fsub_rn(__fmul_rn(c, xt), __fmul_rn(s, yt));
+  o.y = __fadd_rn(__fmul_rn(s, xt), __fmul_rn(c, yt));
+  o.mag = __fdiv_rn(1.f, __fsub_rn(g.inv_M, __fdiv_rn(o.y, g.sdd)));
+  if (!g.curved)
+    o.u = __fmul_rn(o.mag, x);
+  else
+    o.u = __fmul_rn(g.sdd, atan2f(x, __fsub_rn(g.sid, o.y)));
+  o.n_p = __fadd_rn(__fdiv_rn(__fadd_rn(o.u, g.offc), g.ddc), g.det_cc);
+  o.ctr = (int)fminf(fmaxf(rintf(o.n_p), -1.0e6f), 1.0e6f);
+  return o;
+}
+
 // Cone: per (view, pixel) horizontal fan data + the vertical affine pair.
 struct ConeVP {
   float n_p, half_w1, lmax, ws;  // horizontal fan
@@ -140,34 +163,45 @@ struct ConeVP {
   int ctr;
 };
 
-__device__ __forceinline__ ConeVP cone_vp(const Geo &g, float angle, float c, float s,
-                                          float z_off, float xt, float yt) {
+// Second half of the chain (cone_beam.py:93-158): footprint, width, weight
+// scale and the vertical affine pair.
+__device__ __forceinline__ ConeVP cone_finish(const Geo &g, float angle, float z_off,
+                                              const ConeCenter &cc) {
   ConeVP o;
-  float x = __fsub_rn(__fmul_rn(c, xt), __fmul_rn(s, yt));
-  float y = __fadd_rn(__fmul_rn(s, xt), __fmul_rn(c, yt));
-  float mag = __fdiv_rn(1.f, __fsub_rn(g.inv_M, __fdiv_rn(y, g.sdd)));
-  float u, theta;
-  if (!g.curved) {
-    u = __fmul_rn(mag, x);
-    theta = atan2f(u, g.sdd);
-  } else {
-    u = __fmul_rn(g.sdd, atan2f(x, __fsub_rn(g.sid, y)));
-    theta = __fdiv_rn(u, g.sdd);
-  }
-  o.n_p = __fadd_rn(__fdiv_rn(__fadd_rn(u, g.offc), g.ddc), g.det_cc);
-  float da = __fsub_rn(angle, theta);
-  float fp = fmaxf(__fmul_rn(fabsf(cosf(da)), g.dv), __fmul_rn(fabsf(sinf(da)), g.dvr));
-  float W = __fmul_rn(mag, __fdiv_rn(fp, g.ddc));
+  const float theta = !g.curved ? atan2f(cc.u, g.sdd) : __fdiv_rn(cc.u, g.sdd);
+  o.n_p = cc.n_p;
+  o.ctr = cc.ctr;
+  o.mag = cc.mag;
+  const float da = __fsub_rn(angle, theta);
+  const float fp = fmaxf(__fmul_rn(fabsf(cosf(da)), g.dv), __fmul_rn(fabsf(sinf(da)), g.dvr));
+  float W = __fmul_rn(cc.mag, __fdiv_rn(fp, g.ddc));
   if (!g.curved) W = __fdiv_rn(W, cosf(theta));
   o.half_w1 = __fdiv_rn(__fadd_rn(W, 1.f), 2.f);
   o.lmax = fminf(W, 1.f);
   o.ws = __fdiv_rn(g.area, fp);
-  o.ctr = (int)fminf(fmaxf(rintf(o.n_p), -1.0e6f), 1.0e6f);
-  o.mag = mag;
-  o.w_r = __fdiv_rn(__fmul_rn(mag, g.dvs), g.ddr);
-  float z0 = __fsub_rn(z_off, g.half_z);
-  o.m0 = __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(mag, z0), g.offr), g.ddr), g.det_cr);
+  o.w_r = __fdiv_rn(__fmul_rn(cc.mag, g.dvs), g.ddr);
+  const float z0 = __fsub_rn(z_off, g.half_z);
+  o.m0 = __fadd_rn(__fdiv_rn(__fadd_rn(__fmul_rn(cc.mag, z0), g.offr), g.ddr), g.det_cr);
   return o;
+}
+
+__device__ __forceinline__ ConeVP cone_vp(const Geo &g, float angle, float c, float s,
+                                          float z_off, float xt, float yt) {
+  return cone_finish(g, angle, z_off, cone_center(g, c, s, xt, yt));
+}
+
+// t(k) = mag * z_k / SDD = a0 + a1 * k for global slice k, the argument of
+// 1 / cos(phi) = sqrt(1 + t^2) (cone_beam.py:207-212, 282-286).
+__device__ __forceinline__ void cone_tcoef(const Geo &g, float mag, float z_off, float &a0,
+                                           float &a1) {
+  a1 = __fmul_rn(__fmul_rn(mag, g.dvs), g.inv_sdd);
+  a0 = __fmul_rn(__fmul_rn(mag, __fsub_rn(z_off, __fmul_rn(g.dvs, g.slice_c))), g.inv_sdd);
+}
+
+// sqrt(1 + t^2) from the fast reciprocal square root (q * rsqrt(q)).
+__device__ __forceinline__ float inv_cos_from_t(float t) {
+  const float q = fmaf(t, t, 1.f);
+  return q * rsqrtf(q);
 }
 
 // 1 / cos(phi) for the voxel at global slice k of a cone (view, pixel):

@@ -1,24 +1,29 @@
 // Projector kernels (parallel and cone; forward and back) for sm_100a.
 //
-// BACK (gather, adjoint): a TEAM of T lanes owns one pixel's cylinder
-// (a chunk of up to T*SPL slices) and walks a contiguous range of views,
-// accumulating in registers.  The sinogram is read in the resident VCR
-// layout, so every gather along the slice/row axis is unit-stride and
-// coalesced.  For cone beam the warp first forms the view's horizontal
-// detector column h(m) = sum_tc Wc * sino[v, c + tc, m] for the rows its
-// slices reach (shared memory, one buffer per warp), then applies the
-// vertical taps per slice -- the separable form of
-// cone_beam.py:237-299.  View chunks (grid.y) write partial sums that
-// reduce in a fixed order, so results are deterministic.
+// BACK (gather, adjoint).  A TEAM of T lanes owns one pixel's cylinder (a
+// chunk of up to T*SPL slices) and walks a contiguous range of views,
+// accumulating in registers.  The per-(view, pixel) geometry -- the
+// transcendental-heavy part of the chain -- is computed LANE-PARALLEL: each
+// lane of the team takes one view of the next T, writes a small record to
+// the team's shared-memory table, and the team then consumes the T records
+// (broadcast reads).  The sinogram is read in the resident channel-major
+// (V, C, R) layout, so every walk along the slice/row axis is unit-stride.
+// For cone beam the warp first forms the view's horizontal detector column
+// h(m) = sum_tc Wc * sino[v, c + tc, m] for the rows its slices reach (a
+// zero-padded shared buffer per warp), then applies the vertical taps per
+// slice: the separable form of cone_beam.py:237-299.  View chunks (grid.y)
+// write partial sums reduced in a fixed order: deterministic.
 //
-// FORWARD (scatter, expressed as a gather): a CTA owns one view and a block
-// of CB detector channels over all rows.  It scans the pixel set, computes
-// each pixel's centre channel, keeps the pixels whose footprint reaches its
-// channel block (warp-ballot compaction in pixel order) and accumulates
-// their taps into shared-memory tiles that each thread group owns
-// privately; the groups' tiles are summed in a fixed order.  No atomics
-// anywhere, so the forward is bit-reproducible.  The epilogue writes the
-// block in either sinogram layout or, for VCD, fuses the line-search
+// FORWARD (scatter, expressed as a gather).  The cylinders are either a
+// (P, band) array in pixel-list order or, with by_pixel, the rows pix[p] of
+// a flat (N*N, band) volume.  A CTA owns one view and a block
+// of CB detector channels over all rows.  It scans the pixel set computing
+// only each pixel's centre channel, compacts the pixels whose footprint
+// reaches its block (warp ballot, in pixel order), builds full records for
+// those only, and accumulates their taps into shared-memory tiles owned
+// privately by thread groups; the groups' tiles are summed in group order.
+// No atomics anywhere: the forward is bit-reproducible.  The epilogue writes
+// the block in either sinogram layout or, for VCD, fuses the line-search
 // reductions against the error sinogram.
 #pragma once
 
@@ -27,16 +32,17 @@
 namespace mbir {
 
 constexpr int kThreads = 256;
-constexpr int kViewTab = 64;   // views staged per shared-memory table refill
 constexpr int kListCap = 512;  // forward: pixel records per processing round
+constexpr int kPad = 8;        // cone back: zero rows either side of the column buffer
 
 // ── sinogram readers (resident VCR layout) ─────────────────────────────────
+// value(v, c, m) = scale(v) * get(base(v, c) + m)
 struct ReadF32 {
   const float *s;
   int C, R;
-  __device__ __forceinline__ float operator()(int v, int c, int m) const {
-    return __ldg(s + ((size_t)v * C + c) * R + m);
-  }
+  __device__ __forceinline__ size_t base(int v, int c) const { return ((size_t)v * C + c) * R; }
+  __device__ __forceinline__ float scale(int) const { return 1.f; }
+  __device__ __forceinline__ float get(size_t i) const { return __ldg(s + i); }
 };
 
 template <typename T>
@@ -44,9 +50,9 @@ struct ReadScaled {
   const T *e;
   const float *es;
   int C, R;
-  __device__ __forceinline__ float operator()(int v, int c, int m) const {
-    return __fmul_rn(to_f32(e[((size_t)v * C + c) * R + m]), __ldg(es + v));
-  }
+  __device__ __forceinline__ size_t base(int v, int c) const { return ((size_t)v * C + c) * R; }
+  __device__ __forceinline__ float scale(int v) const { return __ldg(es + v); }
+  __device__ __forceinline__ float get(size_t i) const { return to_f32(e[i]); }
 };
 
 // weights * error, the gradient's operand (tomography_model.py:2548-2552).
@@ -57,25 +63,41 @@ struct ReadWeighted {
   const T *w;
   const float *ws;
   int C, R;
-  __device__ __forceinline__ float operator()(int v, int c, int m) const {
-    size_t i = ((size_t)v * C + c) * R + m;
-    float wv = __fmul_rn(to_f32(w[i]), __ldg(ws + v));
-    float ev = __fmul_rn(to_f32(e[i]), __ldg(es + v));
-    return __fmul_rn(wv, ev);
+  __device__ __forceinline__ size_t base(int v, int c) const { return ((size_t)v * C + c) * R; }
+  __device__ __forceinline__ float scale(int v) const {
+    return __fmul_rn(__ldg(ws + v), __ldg(es + v));
+  }
+  __device__ __forceinline__ float get(size_t i) const {
+    return __fmul_rn(to_f32(w[i]), to_f32(e[i]));
   }
 };
 
-struct ConeView {
-  float ang, c, s, z_off;
+// Tap loops: NT is the compile-time tap count (3 for psf radius 1, the
+// common case) or 0 for a run-time count of 2 psf + 1 <= kMaxTaps.
+#define MBIR_TAPS(NT) ((NT) ? (NT) : kMaxTaps)
+#define MBIR_TAP_ON(NT, t, nt) ((NT) != 0 || (t) < (nt))
+
+// Per-(view, pixel) records the back projectors share across a team.
+struct ParRec {
+  int ctr;
+  float w[kMaxTaps];
+};
+
+struct ConeRec {
+  int ctr;
+  float w[kMaxTaps];
+  float m0, w_r, hw1r, lmaxr, a0, a1;
 };
 
 // ── back projection: parallel ─────────────────────────────────────────────
-template <int CP, int SPL, typename RD>
+template <int CP, int SPL, int NT, typename RD>
 __global__ void __launch_bounds__(kThreads)
 back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
                      RD rd, const int64_t *__restrict__ pix, int P, int band, int T,
                      int slice_chunks, float *__restrict__ out) {
-  __shared__ ParView tab[kViewTab];
+  __shared__ ParRec tab[kThreads];
+  constexpr int MT = MBIR_TAPS(NT);
+  const int RT = NT ? (NT - 1) / 2 : g.psf, nt = 2 * RT + 1;
   const int tid = threadIdx.x;
   const int team = tid / T, tl = tid - team * T;
   const int teams_per_block = kThreads / T;
@@ -86,47 +108,52 @@ back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_cou
   const int l0 = sc * T * SPL;
   const int chunk = blockIdx.y;
   const int vb = chunk * vpc, ve = min(v_count, vb + vpc);
-  const int r = g.psf, ntaps = 2 * g.psf + 1;
+  ParRec *mytab = tab + team * T;
   float xt = 0.f, yt = 0.f;
   if (active) pixel_xy(g, (int)pix[p], xt, yt);
   float acc[SPL];
 #pragma unroll
   for (int j = 0; j < SPL; ++j) acc[j] = 0.f;
 
-  for (int v0 = vb; v0 < ve; v0 += kViewTab) {
-    const int nv = min(kViewTab, ve - v0);
-    __syncthreads();
-    if (tid < nv) tab[tid] = parallel_view(g, vp[2 * (v_start + v0 + tid)]);
-    __syncthreads();
+  for (int vg = vb; vg < ve; vg += T) {
+    const int nv = min(T, ve - vg);
+    __syncwarp();
+    if (active && tl < nv) {
+      const ParView pv = parallel_view(g, vp[2 * (v_start + vg + tl)]);
+      const float n_p = parallel_np(g, pv, xt, yt);
+      ParRec r;
+      r.ctr = (int)fminf(fmaxf(rintf(n_p), -1.0e6f), 1.0e6f);
+#pragma unroll
+      for (int t = 0; t < MT; ++t) {
+        float a = MBIR_TAP_ON(NT, t, nt)
+                      ? tap_weight(n_p, r.ctr + t - RT, pv.half_w1, pv.lmax, pv.ws, g.C)
+                      : 0.f;
+        r.w[t] = CP == 2 ? __fmul_rn(a, a) : a;
+      }
+      mytab[tl] = r;
+    }
+    __syncwarp();
     if (!active) continue;
     for (int i = 0; i < nv; ++i) {
-      const ParView pv = tab[i];
-      const float n_p = parallel_np(g, pv, xt, yt);
-      const int ctr = (int)fminf(fmaxf(rintf(n_p), -1.0e6f), 1.0e6f);
-      float w[kMaxTaps];
-      int n[kMaxTaps];
+      const int v = vg + i;
+      const int ctr = mytab[i].ctr;
+      float w[MT];
+      size_t base[MT];
 #pragma unroll
-      for (int t = 0; t < kMaxTaps; ++t) {
-        w[t] = 0.f;
-        n[t] = 0;
-        if (t < ntaps) {
-          const int nn = ctr + t - r;
-          float a = tap_weight(n_p, nn, pv.half_w1, pv.lmax, pv.ws, g.C);
-          if (CP == 2) a = __fmul_rn(a, a);
-          w[t] = a;
-          n[t] = min(max(nn, 0), g.C - 1);
-        }
+      for (int t = 0; t < MT; ++t) {
+        w[t] = mytab[i].w[t];
+        base[t] = rd.base(v, min(max(ctr + t - RT, 0), g.C - 1));
       }
-      const int v = v0 + i;
+      const float scl = rd.scale(v);
 #pragma unroll
       for (int j = 0; j < SPL; ++j) {
         const int l = l0 + tl + T * j;
         if (l < band) {
           float s = 0.f;
 #pragma unroll
-          for (int t = 0; t < kMaxTaps; ++t)
-            if (t < ntaps && w[t] != 0.f) s = fmaf(w[t], rd(v, n[t], l), s);
-          acc[j] += s;
+          for (int t = 0; t < MT; ++t)
+            if (MBIR_TAP_ON(NT, t, nt)) s = fmaf(w[t], rd.get(base[t] + l), s);
+          acc[j] = fmaf(scl, s, acc[j]);
         }
       }
     }
@@ -142,117 +169,125 @@ back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_cou
 }
 
 // ── back projection: cone ─────────────────────────────────────────────────
-// One warp per (pixel, slice chunk of 32*SPL slices).  Dynamic shared memory:
-// 8 warps x R floats of detector-column buffer.
-template <int CP, int SPL, typename RD>
+// One warp per (pixel, chunk of 32*SPL slices).  Dynamic shared memory:
+// 8 warps x (R + 2 kPad) floats of column buffer, then 8 x 32 ConeRec.
+template <int CP, int SPL, int NT, typename RD>
 __global__ void __launch_bounds__(kThreads)
 back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc, RD rd,
                  const int64_t *__restrict__ pix, int P, int slice_start, int band,
                  int slice_chunks, float *__restrict__ out) {
-  extern __shared__ float colbuf[];
-  __shared__ ConeView tab[kViewTab];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  extern __shared__ float smem[];
+  constexpr int MT = MBIR_TAPS(NT);
+  const int RT = NT ? (NT - 1) / 2 : g.psf, nt = 2 * RT + 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long gw = (long long)blockIdx.x * (kThreads / 32) + warp;
   const int p = (int)(gw / slice_chunks);
+  if (p >= P) return;  // whole warp: no block-level barrier in this kernel
   const int sc = (int)(gw - (long long)p * slice_chunks);
-  const bool active = p < P;
+  const int hs = g.R + 2 * kPad;
+  float *h = smem + warp * hs + kPad;
+  ConeRec *tab = reinterpret_cast<ConeRec *>(smem + (kThreads / 32) * hs) + warp * 32;
+  for (int i = lane; i < kPad; i += 32) {
+    h[i - kPad] = 0.f;
+    h[g.R + i] = 0.f;
+  }
   const int l0 = sc * 32 * SPL;
   const int l_end = min(band, l0 + 32 * SPL);
   const int chunk = blockIdx.y;
   const int vb = chunk * vpc, ve = min(v_count, vb + vpc);
-  const int r = g.psf, ntaps = 2 * g.psf + 1;
-  float *h = colbuf + warp * g.R;
-  float xt = 0.f, yt = 0.f;
-  if (active) pixel_xy(g, (int)pix[p], xt, yt);
+  float xt, yt;
+  pixel_xy(g, (int)pix[p], xt, yt);
   float acc[SPL];
 #pragma unroll
   for (int j = 0; j < SPL; ++j) acc[j] = 0.f;
   const float kf = (float)(slice_start + l0);
   const float kl = (float)(slice_start + max(l_end - 1, l0));
+  const float mlo_clamp = -(float)(RT + 1), mhi_clamp = (float)(g.R + RT);
 
-  for (int v0 = vb; v0 < ve; v0 += kViewTab) {
-    const int nv = min(kViewTab, ve - v0);
-    __syncthreads();
-    if (tid < nv) {
-      const int gv = v_start + v0 + tid;
-      ConeView cv;
-      cv.ang = vp[2 * gv];
-      cv.c = cosf(cv.ang);
-      cv.s = sinf(cv.ang);
-      cv.z_off = __fsub_rn(g.rso, vp[2 * gv + 1]);
-      tab[tid] = cv;
-    }
-    __syncthreads();
-    if (!active) continue;
-    for (int i = 0; i < nv; ++i) {
-      const ConeView cv = tab[i];
-      const ConeVP q = cone_vp(g, cv.ang, cv.c, cv.s, cv.z_off, xt, yt);
-      float w[kMaxTaps];
-      int n[kMaxTaps];
+  for (int vg = vb; vg < ve; vg += 32) {
+    const int nv = min(32, ve - vg);
+    __syncwarp();
+    if (lane < nv) {
+      const int gv = v_start + vg + lane;
+      const float ang = vp[2 * gv];
+      const float z_off = __fsub_rn(g.rso, vp[2 * gv + 1]);
+      const ConeVP q = cone_vp(g, ang, cosf(ang), sinf(ang), z_off, xt, yt);
+      ConeRec r;
+      r.ctr = q.ctr;
 #pragma unroll
-      for (int t = 0; t < kMaxTaps; ++t) {
-        w[t] = 0.f;
-        n[t] = 0;
-        if (t < ntaps) {
-          const int nn = q.ctr + t - r;
-          float a = tap_weight(q.n_p, nn, q.half_w1, q.lmax, q.ws, g.C);
-          if (CP == 2) a = __fmul_rn(a, a);
-          w[t] = a;
-          n[t] = min(max(nn, 0), g.C - 1);
-        }
+      for (int t = 0; t < MT; ++t) {
+        float a = MBIR_TAP_ON(NT, t, nt)
+                      ? tap_weight(q.n_p, q.ctr + t - RT, q.half_w1, q.lmax, q.ws, g.C)
+                      : 0.f;
+        r.w[t] = CP == 2 ? __fmul_rn(a, a) : a;
       }
-      const int v = v0 + i;
-      // Rows reached by this chunk's slices (the affine map is monotone in k).
-      const float ma = __fadd_rn(q.m0, __fmul_rn(q.w_r, kf));
-      const float mb = __fadd_rn(q.m0, __fmul_rn(q.w_r, kl));
-      const float lo = fmaxf(floorf(fminf(ma, mb)) - (float)(r + 1), 0.f);
-      const float hi = fminf(ceilf(fmaxf(ma, mb)) + (float)(r + 1), (float)(g.R - 1));
+      r.m0 = q.m0;
+      r.w_r = q.w_r;
+      r.hw1r = __fdiv_rn(__fadd_rn(q.w_r, 1.f), 2.f);
+      r.lmaxr = fminf(q.w_r, 1.f);
+      cone_tcoef(g, q.mag, z_off, r.a0, r.a1);
+      tab[lane] = r;
+    }
+    __syncwarp();
+    for (int i = 0; i < nv; ++i) {
+      const int v = vg + i;
+      const ConeRec &r = tab[i];
+      const float m0 = r.m0, w_r = r.w_r, hw1r = r.hw1r, lmaxr = r.lmaxr;
+      const float a0 = r.a0, a1 = r.a1;
+      float w[MT];
+      size_t base[MT];
+#pragma unroll
+      for (int t = 0; t < MT; ++t) {
+        w[t] = r.w[t];
+        base[t] = rd.base(v, min(max(r.ctr + t - RT, 0), g.C - 1));
+      }
+      const float scl = rd.scale(v);
+      // Rows this chunk's slices reach (the map is affine in k).
+      const float ma = fmaf(w_r, kf, m0), mb = fmaf(w_r, kl, m0);
+      const float lo = fmaxf(floorf(fminf(ma, mb)) - (float)(RT + 1), 0.f);
+      const float hi = fminf(ceilf(fmaxf(ma, mb)) + (float)(RT + 1), (float)(g.R - 1));
       if (lo <= hi) {
         const int m_lo = (int)lo, m_hi = (int)hi;
         for (int m = m_lo + lane; m <= m_hi; m += 32) {
           float s = 0.f;
 #pragma unroll
-          for (int t = 0; t < kMaxTaps; ++t)
-            if (t < ntaps && w[t] != 0.f) s = fmaf(w[t], rd(v, n[t], m), s);
-          h[m] = s;
+          for (int t = 0; t < MT; ++t)
+            if (MBIR_TAP_ON(NT, t, nt)) s = fmaf(w[t], rd.get(base[t] + m), s);
+          h[m] = __fmul_rn(s, scl);
         }
-        __syncwarp();
-        const float half_wr1 = __fdiv_rn(__fadd_rn(q.w_r, 1.f), 2.f);
-        const float lmax_r = fminf(q.w_r, 1.f);
+      }
+      __syncwarp();
 #pragma unroll
-        for (int j = 0; j < SPL; ++j) {
-          const int l = l0 + lane + 32 * j;
-          if (l < band) {
-            const float k = (float)(slice_start + l);
-            const float m_p = __fadd_rn(q.m0, __fmul_rn(q.w_r, k));
-            const float mpc = fminf(fmaxf(m_p, -(float)(r + 2)), (float)(g.R + r + 1));
-            const int mc = (int)rintf(mpc);
-            const float inv_cos = cone_inv_cos(g, q.mag, cv.z_off, k);
-            float s = 0.f;
+      for (int j = 0; j < SPL; ++j) {
+        const int l = l0 + lane + 32 * j;
+        if (l < band) {
+          const float k = (float)(slice_start + l);
+          const float m_p = fminf(fmaxf(fmaf(w_r, k, m0), mlo_clamp), mhi_clamp);
+          const float mcf = rintf(m_p);
+          const int mc = (int)mcf;
+          const float d = m_p - mcf;
+          float s = 0.f;
 #pragma unroll
-            for (int t = 0; t < kMaxTaps; ++t) {
-              if (t < ntaps) {
-                const int mm = mc + t - r;
-                float a = fmaxf(__fsub_rn(half_wr1, fabsf(__fsub_rn(m_p, (float)mm))), 0.f);
-                a = __fmul_rn(fminf(a, lmax_r), inv_cos);
-                if (CP == 2) a = __fmul_rn(a, a);
-                if (mm >= 0 && mm < g.R && a != 0.f) s = fmaf(a, h[mm], s);
-              }
+          for (int t = 0; t < MT; ++t) {
+            if (MBIR_TAP_ON(NT, t, nt)) {
+              float a = fminf(fmaxf(hw1r - fabsf(d - (float)(t - RT)), 0.f), lmaxr);
+              if (CP == 2) a = a * a;
+              s = fmaf(a, h[mc + t - RT], s);
             }
-            acc[j] += s;
           }
+          const float tk = fmaf(a1, k, a0);
+          const float ic = CP == 2 ? fmaf(tk, tk, 1.f) : inv_cos_from_t(tk);
+          acc[j] = fmaf(ic, s, acc[j]);
         }
       }
       __syncwarp();
     }
   }
-  if (active) {
-    float *o = out + (size_t)chunk * P * band + (size_t)p * band;
+  float *o = out + (size_t)chunk * P * band + (size_t)p * band;
 #pragma unroll
-    for (int j = 0; j < SPL; ++j) {
-      const int l = l0 + lane + 32 * j;
-      if (l < band) o[l] = acc[j];
-    }
+  for (int j = 0; j < SPL; ++j) {
+    const int l = l0 + lane + 32 * j;
+    if (l < band) o[l] = acc[j];
   }
 }
 
@@ -268,15 +303,18 @@ __global__ void reduce_chunks_kernel(const float *__restrict__ part, int chunks,
 }
 
 // ── forward projection ────────────────────────────────────────────────────
+constexpr int kConeFields = 7;  // m0, w_r, hw1r, lmaxr, inv_wr, a0, a1
+
 struct FwdShape {
-  int CB;   // channels per CTA
-  int TG;   // threads per group (row lanes)
-  int RPT;  // rows per thread
-  int rows; // output rows (detector rows; == band for parallel)
+  int CB;    // channels per CTA
+  int TG;    // threads per group (row lanes)
+  int RPT;   // rows per thread
+  int rows;  // output rows (detector rows; == band for parallel)
   __host__ __device__ int RS() const { return TG * RPT + 1; }
   __host__ __device__ int G() const { return kThreads / TG; }
   size_t smem_bytes() const {
-    return sizeof(float) * ((size_t)G() * CB * RS() + (size_t)kListCap * (2 + kMaxTaps + 6));
+    return sizeof(float) *
+           ((size_t)G() * CB * RS() + (size_t)kListCap * (2 + kMaxTaps + kConeFields));
   }
 };
 
@@ -295,19 +333,21 @@ struct StoreSino {
   __device__ __forceinline__ void end(int) {}
 };
 
-template <bool CONE, typename EPI>
+template <bool CONE, int NT, typename EPI>
 __global__ void __launch_bounds__(kThreads)
 forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__restrict__ values,
                int P, int band, int slice_start, const int64_t *__restrict__ pix, FwdShape fs,
-               EPI epi) {
+               int by_pixel, EPI epi) {
   extern __shared__ float sm[];
+  constexpr int MT = MBIR_TAPS(NT);
+  const int RT = NT ? (NT - 1) / 2 : g.psf, nt = 2 * RT + 1;
   const int TG = fs.TG, G = fs.G(), RS = fs.RS(), CB = fs.CB, RPT = fs.RPT;
   const int rows = fs.rows;
   float *tile = sm;
   int *l_ctr = (int *)(tile + (size_t)G * CB * RS);
   int *l_pix = l_ctr + kListCap;
   float *l_w = (float *)(l_pix + kListCap);
-  float *l_c = l_w + kMaxTaps * kListCap;  // cone: m0, w_r, half_wr1, lmax_r, inv_wr, mag
+  float *l_c = l_w + kMaxTaps * kListCap;
   __shared__ int s_wcount[kThreads / 32];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -315,7 +355,7 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
   const int v = v_start + vl;
   const int c0 = blockIdx.x * CB;
   const int ncb = min(CB, g.C - c0);
-  const int r = g.psf, ntaps = 2 * g.psf + 1, bp = g.bp;
+  const int bp = g.bp;
   const float ang = vp[2 * v];
   const float cs = cosf(ang), sn = sinf(ang);
   const float z_off = __fsub_rn(g.rso, vp[2 * v + 1]);
@@ -324,6 +364,7 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
 
   for (int i = tid; i < G * CB * RS; i += kThreads) tile[i] = 0.f;
   const int grp = tid / TG, tg = tid - grp * TG;
+  float *mytile = tile + (size_t)grp * CB * RS;
 
   int pos = 0;
   while (pos < P) {
@@ -332,21 +373,21 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
     while (pos < P && n <= kListCap - kThreads) {
       const int p = pos + tid;
       bool keep = false;
-      float xt = 0.f, yt = 0.f;
       int ctr = 0;
       float n_p = 0.f;
-      ConeVP q;
+      ConeCenter cc;
       if (p < P) {
+        float xt, yt;
         pixel_xy(g, (int)pix[p], xt, yt);
         if (CONE) {
-          q = cone_vp(g, ang, cs, sn, z_off, xt, yt);
-          ctr = q.ctr;
-          n_p = q.n_p;
+          cc = cone_center(g, cs, sn, xt, yt);
+          ctr = cc.ctr;
+          n_p = cc.n_p;
         } else {
           n_p = parallel_np(g, pv, xt, yt);
           ctr = (int)fminf(fmaxf(rintf(n_p), -1.0e6f), 1.0e6f);
         }
-        keep = (ctr + r >= c0) && (ctr - r < c0 + ncb);
+        keep = (ctr + RT >= c0) && (ctr - RT < c0 + ncb);
       }
       const unsigned bal = __ballot_sync(0xffffffffu, keep);
       if (lane == 0) s_wcount[warp] = __popc(bal);
@@ -361,20 +402,29 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
       if (keep) {
         const int slot = off + __popc(bal & ((1u << lane) - 1u));
         l_ctr[slot] = ctr;
-        l_pix[slot] = p;
-        const float hw1 = CONE ? q.half_w1 : pv.half_w1;
-        const float lmx = CONE ? q.lmax : pv.lmax;
-        const float wsc = CONE ? q.ws : pv.ws;
-#pragma unroll
-        for (int t = 0; t < kMaxTaps; ++t)
-          l_w[t * kListCap + slot] = (t < ntaps) ? tap_weight(n_p, ctr + t - r, hw1, lmx, wsc, g.C) : 0.f;
+        l_pix[slot] = by_pixel ? (int)pix[p] : p;  // row of `values` holding the cylinder
         if (CONE) {
+          const ConeVP q = cone_finish(g, ang, z_off, cc);
+#pragma unroll
+          for (int t = 0; t < MT; ++t)
+            l_w[t * kListCap + slot] =
+                MBIR_TAP_ON(NT, t, nt)
+                    ? tap_weight(n_p, ctr + t - RT, q.half_w1, q.lmax, q.ws, g.C) : 0.f;
+          float a0, a1;
+          cone_tcoef(g, q.mag, z_off, a0, a1);
           l_c[0 * kListCap + slot] = q.m0;
           l_c[1 * kListCap + slot] = q.w_r;
           l_c[2 * kListCap + slot] = __fdiv_rn(__fadd_rn(q.w_r, 1.f), 2.f);
           l_c[3 * kListCap + slot] = fminf(q.w_r, 1.f);
           l_c[4 * kListCap + slot] = 1.f / q.w_r;
-          l_c[5 * kListCap + slot] = q.mag;
+          l_c[5 * kListCap + slot] = a0;
+          l_c[6 * kListCap + slot] = a1;
+        } else {
+#pragma unroll
+          for (int t = 0; t < MT; ++t)
+            l_w[t * kListCap + slot] =
+                MBIR_TAP_ON(NT, t, nt)
+                    ? tap_weight(n_p, ctr + t - RT, pv.half_w1, pv.lmax, pv.ws, g.C) : 0.f;
         }
       }
       n += tot;
@@ -382,21 +432,21 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
       __syncthreads();
     }
     // Accumulate the listed pixels: group grp takes entries grp, grp + G, ...
-    float *mytile = tile + (size_t)grp * CB * RS;
     for (int e = grp; e < n; e += G) {
-      const int ctr = l_ctr[e];
+      const int cb0 = l_ctr[e] - RT - c0;  // tile channel of tap 0
       const float *vrow = values + (size_t)l_pix[e] * band;
-      float w[kMaxTaps];
+      float w[MT];
 #pragma unroll
-      for (int t = 0; t < kMaxTaps; ++t) w[t] = l_w[t * kListCap + e];
-      float m0 = 0.f, w_r = 0.f, half_wr1 = 0.f, lmax_r = 0.f, inv_wr = 0.f, mag = 0.f;
+      for (int t = 0; t < MT; ++t) w[t] = l_w[t * kListCap + e];
+      float m0 = 0.f, w_r = 0.f, hw1r = 0.f, lmaxr = 0.f, inv_wr = 0.f, a0 = 0.f, a1 = 0.f;
       if (CONE) {
         m0 = l_c[0 * kListCap + e];
         w_r = l_c[1 * kListCap + e];
-        half_wr1 = l_c[2 * kListCap + e];
-        lmax_r = l_c[3 * kListCap + e];
+        hw1r = l_c[2 * kListCap + e];
+        lmaxr = l_c[3 * kListCap + e];
         inv_wr = l_c[4 * kListCap + e];
-        mag = l_c[5 * kListCap + e];
+        a0 = l_c[5 * kListCap + e];
+        a1 = l_c[6 * kListCap + e];
       }
       for (int j = 0; j < RPT; ++j) {
         const int m = tg + TG * j;
@@ -405,30 +455,27 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
         if (!CONE) {
           det = __ldg(vrow + m);
         } else {
-          // Detector-side vertical fan (cone_beam.py:203-226).
-          const float k_m = __fmul_rn(__fsub_rn((float)m, m0), inv_wr);
+          // Detector-side vertical fan (cone_beam.py:203-226): slice taps
+          // around k(m) = (m - m0) / w_r, values scaled by 1 / cos(phi).
+          const float k_m = ((float)m - m0) * inv_wr;
           const float kc = rintf(fminf(fmaxf(k_m, -1.0e6f), 1.0e6f));
-          const float d = __fmul_rn(w_r, __fsub_rn(kc, k_m));
+          const float d = w_r * (kc - k_m);
           det = 0.f;
           for (int ko = -bp; ko <= bp; ++ko) {
             const int k_ind = (int)kc + ko;
-            if (k_ind < slice_start || k_ind >= slice_start + band) continue;
-            float a = fmaxf(__fsub_rn(half_wr1, fabsf(__fadd_rn(d, __fmul_rn(w_r, (float)ko)))), 0.f);
-            a = fminf(a, lmax_r);
-            if (a == 0.f) continue;
-            const float sv = __fmul_rn(__ldg(vrow + (k_ind - slice_start)),
-                                       cone_inv_cos(g, mag, z_off, (float)k_ind));
-            det = fmaf(a, sv, det);
+            const float a = fminf(fmaxf(hw1r - fabsf(fmaf(w_r, (float)ko, d)), 0.f), lmaxr);
+            if (a > 0.f && k_ind >= slice_start && k_ind < slice_start + band) {
+              const float tk = fmaf(a1, (float)k_ind, a0);
+              det = fmaf(a * inv_cos_from_t(tk), __ldg(vrow + (k_ind - slice_start)), det);
+            }
           }
         }
-        if (det == 0.f) continue;
+        float *col = mytile + m;
 #pragma unroll
-        for (int t = 0; t < kMaxTaps; ++t) {
-          const int ch = ctr + t - r - c0;
-          if (t < ntaps && ch >= 0 && ch < ncb && w[t] != 0.f) {
-            float *cell = mytile + (size_t)ch * RS + m;
-            *cell = fmaf(w[t], det, *cell);
-          }
+        for (int t = 0; t < MT; ++t) {
+          const int ch = cb0 + t;
+          if (MBIR_TAP_ON(NT, t, nt) && ch >= 0 && ch < ncb)
+            col[(size_t)ch * RS] = fmaf(w[t], det, col[(size_t)ch * RS]);
         }
       }
     }
@@ -445,6 +492,7 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
       epi.cell(vl, c0 + ch, m, s);
     }
   } else {
+#pragma unroll 4
     for (int i = tid; i < cells; i += kThreads) {
       const int ch = i / rows, m = i - (i / rows) * rows;
       float s = 0.f;

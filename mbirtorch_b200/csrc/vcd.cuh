@@ -252,6 +252,24 @@ struct LineSearchEpi {
   }
 };
 
+// Refresh epilogue: e = (y - A x) / scale[v] stored in T, with y the FP32
+// measured sinogram in the same (V, C, R) layout.  Re-forming the error
+// sinogram from y bounds the drift that in-place 16-bit updates accumulate.
+template <typename T>
+struct RefreshEpi {
+  const float *y;
+  T *e;
+  const float *es;
+  int C, R;
+  __device__ __forceinline__ bool channel_fastest() const { return false; }
+  __device__ __forceinline__ void begin() {}
+  __device__ __forceinline__ void cell(int v, int c, int m, float val) {
+    const size_t i = ((size_t)v * C + c) * R + m;
+    e[i] = from_f32<T>(__fdiv_rn(__fsub_rn(__ldg(y + i), val), __ldg(es + v)));
+  }
+  __device__ __forceinline__ void end(int) {}
+};
+
 // ── 4. alpha ─────────────────────────────────────────────────────────────
 // One CTA.  prior: np pairs (pl, pq); fwd: nf pairs (fl, fq).
 __global__ void __launch_bounds__(kThreads)

@@ -18,7 +18,6 @@ Two layers:
 
 import math
 
-import numpy as np
 import torch
 
 from . import _lib
@@ -84,6 +83,25 @@ class DeviceProjector:
         check(lib.mbir_forward_project(g, ptr(self.view_params), view_start, vc, ptr(values),
                                        idx.shape[0], L, slice_start, ptr(idx), ptr(out), layout,
                                        stream_of(values.device)))
+        return out
+
+    def forward_volume(self, flat_volume, pixel_indices, layout=MBIR_LAYOUT_VRC, out=None):
+        """Whole cylinders read at rows ``pixel_indices`` of a flat (N*N, S)
+        volume (no gathered copy) -> (V, R, C) [VRC] or (V, C, R) [VCR]."""
+        g = self.geom
+        flat = as_f32_contig(flat_volume)
+        idx = as_i64_contig(pixel_indices)
+        require_cuda(flat, idx)
+        if flat.shape[-1] != g.num_slices or flat.shape[0] != g.num_recon_rows * g.num_recon_cols:
+            raise ValueError(f"flat volume must be ({g.num_recon_rows * g.num_recon_cols}, "
+                             f"{g.num_slices}); got {tuple(flat.shape)}")
+        shape = ((g.num_views, g.num_det_rows, g.num_det_channels) if layout == MBIR_LAYOUT_VRC
+                 else (g.num_views, g.num_det_channels, g.num_det_rows))
+        if out is None:
+            out = torch.empty(shape, dtype=torch.float32, device=flat.device)
+        check(_lib.load().mbir_forward_project_volume(
+            g, ptr(self.view_params), 0, g.num_views, ptr(flat), ptr(idx), idx.shape[0],
+            ptr(out), layout, stream_of(flat.device)))
         return out
 
     def back(self, sino, pixel_indices, coeff_power=1, slice_start=0, band_slices=None,

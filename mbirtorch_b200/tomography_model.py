@@ -56,6 +56,10 @@ class TomographyModel(ParameterHandler):
         self.view_batch_size = view_batch_size
         self.compile_mode = compile_mode
         self.storage_dtype = 'float32'
+        # With 16-bit storage the resident error sinogram is re-formed from
+        # the measured one every this many iterations (None: every
+        # iteration for 16-bit storage, never for float32).
+        self.error_refresh_interval = None
         self._torch_device = None
         self._projector = None
         self._full_indices_cache = None
@@ -205,8 +209,8 @@ class TomographyModel(ParameterHandler):
         ROR pixels when use_ror_mask is set)."""
         recon = self._recon_device(recon)
         idx = self.full_indices_device()
-        vals = recon.reshape(-1, recon.shape[-1]).index_select(0, idx)
-        return self._out(self.projector.forward(vals, idx), output_sharded)
+        flat = recon.reshape(-1, recon.shape[-1])
+        return self._out(self.projector.forward_volume(flat, idx), output_sharded)
 
     def back_project(self, sinogram, output_sharded=False):
         """Full back projection to a (rows, cols, slices) volume (zero outside
@@ -260,10 +264,8 @@ class TomographyModel(ParameterHandler):
 
     # ── auto-regularization (host numpy, tomography_model.py:2057-2276) ────
     def auto_set_regularization_params(self, sinogram, weights=None):
-        if torch.is_tensor(sinogram):
-            sinogram = sinogram.detach().cpu().numpy()
-        if torch.is_tensor(weights):
-            weights = weights.detach().cpu().numpy()
+        # Only a ~20-view subsample reaches the host (subsample_views takes
+        # it on the device for a tensor).
         if self.get_params('auto_regularize_flag'):
             small = self.subsample_views(sinogram)
             small_w = 1 if weights is None else self.subsample_views(weights)
@@ -287,6 +289,10 @@ class TomographyModel(ParameterHandler):
                           f"image quality.")
 
     def auto_set_sigma_y(self, sinogram, sino_indicator, weights=1):
+        if torch.is_tensor(sinogram):
+            sinogram = sinogram.detach().cpu().numpy()
+        if torch.is_tensor(weights):
+            weights = weights.detach().cpu().numpy()
         snr_db = self.get_params('snr_db')
         magnification = self.get_magnification()
         delta_voxel, delta_det_channel = self.get_params(['delta_voxel', 'delta_det_channel'])
@@ -536,6 +542,12 @@ class TomographyModel(ParameterHandler):
             raise ValueError('init_error_sinogram requires init_recon (the pair must be a '
                              'consistent resume state; see the docstring).')
         sino = None if init_error_sinogram is not None else self._sino_device(sinogram)
+        refresh = self.error_refresh_interval
+        if refresh is None:
+            refresh = 0 if storage == _lib.MBIR_F32 else 1
+        y_vcr = None
+        if refresh and sino is not None:
+            y_vcr = ResidentSinogram.from_vrc(sino, _lib.MBIR_F32).data
         scale = init_recon is None
         if init_recon is None:
             self.logger.info('Starting direct recon for initial reconstruction')
@@ -591,6 +603,8 @@ class TomographyModel(ParameterHandler):
             order = order_array(part.shape[0])
             engine.accum.zero_()
             engine.partition_pass(flat, err, part, order)
+            if y_vcr is not None and (i + 1) % refresh == 0:
+                engine.refresh_error(flat, err, self.full_indices_device(), y_vcr)
             stats = iteration_stats(err, w_res, flat)
             host = torch.cat([engine.accum, stats]).cpu().numpy()
             acc, st = host[:2 + recon_shape[2]], host[2 + recon_shape[2]:]

@@ -158,6 +158,19 @@ class VcdEngine:
         return accum
 
 
+def _refresh(engine, flat_recon, err, pixel_indices, y_vcr):
+    idx = _lib.as_i64_contig(pixel_indices)
+    require_cuda(flat_recon, idx, y_vcr)
+    check(_lib.load().mbir_vcd_refresh_error(
+        engine.geom, ptr(engine.view_params), ptr(flat_recon), ptr(idx), idx.shape[0],
+        ptr(y_vcr), ptr(err.data), ptr(err.scale), err.storage, stream_of(engine.device)))
+
+
+VcdEngine.refresh_error = _refresh
+VcdEngine.refresh_error.__doc__ = (
+    "Re-form err = y - A x from the FP32 measured sinogram ``y_vcr`` (V, C, R).")
+
+
 def iteration_stats(err, weights, flat_recon):
     """FP64 [sum w e^2, sum w, sum e^2, sum |x|] as a device tensor."""
     V, C, R = err.data.shape

@@ -91,7 +91,7 @@ def test_chunked_loss_equals_unchunked_and_batches():
     assert sino.shape == (3,) + ss
     l_full = ((sino - y) ** 2).sum()
     l_full.backward()
-    assert abs(float(l_small) - float(l_full)) / float(l_full) < 1e-5
+    assert abs(float(l_small.detach()) - float(l_full.detach())) / float(l_full.detach()) < 1e-5
     assert float((g_small - xb.grad).abs().max() / xb.grad.abs().max()) < 1e-5
     proj = mb.TorchProjector(m)
     assert proj(xb[0]).shape == ss and proj.adjoint(sino[0]).shape == rs

@@ -80,13 +80,23 @@ def test_body_seam_functions_match_reference(name):
 
 @pytest.mark.parametrize("name", PROJECTOR_NAMES)
 def test_adjoint_identity(name):
+    """<Ax, y> == <x, A^T y>: relative 1e-5 on positive inputs (the
+    reference's test_adjoint.py:15-34 uses uniform [0, 1) values), and for
+    signed inputs normalised by ||Ax|| ||y|| (the signed inner product
+    cancels, so its own magnitude is no scale)."""
     d = load_projector_case(name)
     m = build_model(d)
     idx = _t(d['full_indices'], torch.int64)
-    x, y = _t(d['full_values']), _t(d['full_sino'])
-    lhs = float((m.sparse_forward_project(x, idx).double() * y.double()).sum())
-    rhs = float((x.double() * m.sparse_back_project(y, idx).double()).sum())
-    assert abs(lhs - rhs) / max(abs(lhs), abs(rhs)) <= TOL
+    for x, y, signed in ((_t(np.abs(d['full_values'])), _t(np.abs(d['full_sino'])), False),
+                         (_t(d['full_values']), _t(d['full_sino']), True)):
+        ax = m.sparse_forward_project(x, idx).double()
+        aty = m.sparse_back_project(y, idx).double()
+        lhs = float((ax * y.double()).sum())
+        rhs = float((x.double() * aty).sum())
+        if signed:
+            assert abs(lhs - rhs) / float(ax.norm() * y.double().norm()) <= 1e-6
+        else:
+            assert abs(lhs - rhs) / max(abs(lhs), abs(rhs)) <= TOL
 
 
 def _cone_model(views=90, rows=40, chans=56, curved=False, helical=False, sdd=300.0, sid=150.0):
