@@ -189,6 +189,28 @@ int32_t mbir_back_project(const mbir_geometry *geom, const float *view_params,
                           int32_t band_len, float *out, void *workspace,
                           size_t workspace_bytes, void *stream);
 
+/* mbir_back_project for callers that cannot allocate device memory (no
+ * counterpart in the reference, whose bodies allocate through torch).
+ * An application whose device memory belongs to another allocator -- a
+ * framework's caching pool, a pipeline with a fixed memory budget -- cannot
+ * hand this library a fresh workspace, and a cudaMalloc of our own would
+ * bypass that owner.  This variant allocates nothing: its scratch is a
+ * file-scope device array of 32 MiB that every GPU loading the library
+ * holds until the process exits.  It holds the channel-major copy of a
+ * (views, rows, channels) input (such an input above 32 MiB is rejected
+ * with MBIR_ERR_WORKSPACE; pass the channel-major layout instead) and the
+ * view-chunk partial sums, whose count shrinks to fit.  The first call on
+ * each device looks up the array's device address (cudaGetSymbolAddress,
+ * with that device current), so make the first call on a device before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race on it.  Arguments and results are those of mbir_back_project. */
+int32_t mbir_back_project_noalloc(const mbir_geometry *geom, const float *view_params,
+                                  int32_t view_start, int32_t view_count,
+                                  const float *sino, int32_t sino_layout,
+                                  const int64_t *pixel_indices, int64_t num_pixels,
+                                  int32_t coeff_power, int32_t slice_start,
+                                  int32_t band_len, float *out, void *stream);
+
 /* Layout / precision conversion of a whole sinogram between the public f32
  * VRC form and the resident VCR form in `dtype` with a per-view scale:
  * stored = value / scale[v].  direction 0: f32 VRC -> dtype VCR (computing

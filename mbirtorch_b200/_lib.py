@@ -91,6 +91,8 @@ SIGNATURES = {
     "mbir_back_project_workspace_size": (_sz, [_GP, _i32, _i64, _i32]),
     "mbir_back_project": (_i32, [_GP, _vp, _i32, _i32, _vp, _i32, _vp, _i64, _i32, _i32, _i32,
                                  _vp, _vp, _sz, _vp]),
+    "mbir_back_project_noalloc": (_i32, [_GP, _vp, _i32, _i32, _vp, _i32, _vp, _i64, _i32,
+                                         _i32, _i32, _vp, _vp]),
     "mbir_sino_convert": (_i32, [_i32, _i32, _i32, _i32, _vp, _vp, _i32, _vp, _i32, _vp]),
     "mbir_error_init": (_i32, [_i64, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _sz, _vp]),
     "mbir_error_init_workspace_size": (_sz, [_i64]),

@@ -843,3 +843,67 @@ int32_t mbir_iteration_stats(int32_t views, int32_t rows, int32_t channels, cons
 }
 
 }  // extern "C"
+
+// ── back projection without allocation ─────────────────────────────────────
+// Some callers cannot allocate device memory: an application whose device
+// memory belongs to another allocator (a framework's caching pool, a
+// pipeline with a fixed memory budget) has no way to hand this library a
+// fresh workspace, and calling cudaMalloc itself would bypass that owner.
+// For them mbir_back_project_noalloc keeps its scratch in the file-scope
+// array below.  Every GPU that loads this library holds the array until the
+// process exits; every call shares it, and each call overwrites what it
+// uses, so nothing in it needs clearing, but calls that overlap on the GPU
+// race on it.
+constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;  // 32 MiB
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kMaxDevices] = {};
+
+// The scratch array's device address on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, once per device, with that device current.
+int noalloc_scratch(void **out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(MBIR_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return fail(MBIR_ERR_INVALID, "device ordinal %d", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(MBIR_ERR_CUDA, "cudaGetSymbolAddress(static scratch): %s",
+                  cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return MBIR_OK;
+}
+}  // namespace
+
+extern "C" int32_t mbir_back_project_noalloc(const mbir_geometry *geom,
+                                             const float *view_params, int32_t view_start,
+                                             int32_t view_count, const float *sino,
+                                             int32_t sino_layout,
+                                             const int64_t *pixel_indices, int64_t num_pixels,
+                                             int32_t coeff_power, int32_t slice_start,
+                                             int32_t band_len, float *out, void *stream) {
+  if (geom && sino_layout == MBIR_LAYOUT_VRC && view_count > 0) {
+    const size_t need = align_up((size_t)view_count * geom->num_det_rows *
+                                 geom->num_det_channels * sizeof(float));
+    if (need > kNoAllocScratchBytes)
+      return fail(MBIR_ERR_WORKSPACE,
+                  "a (views, rows, channels) sinogram of %zu bytes exceeds the %zu-byte static "
+                  "scratch of mbir_back_project_noalloc; pass the channel-major layout or "
+                  "use mbir_back_project with a workspace", need, kNoAllocScratchBytes);
+  }
+  void *scratch = nullptr;
+  const int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  return mbir_back_project(geom, view_params, view_start, view_count, sino, sino_layout,
+                           pixel_indices, num_pixels, coeff_power, slice_start, band_len, out,
+                           scratch, kNoAllocScratchBytes, stream);
+}
