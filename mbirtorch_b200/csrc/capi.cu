@@ -276,11 +276,50 @@ int launch_forward(const mbir_geometry *g, const float *vp, int v_start, int v_c
   return MBIR_OK;
 }
 
+// The register-tiled cone forward covers psf radius 1 and up to 1024
+// detector rows (one thread per row); other shapes use forward_kernel.
+bool use_cone_rt(const mbir_geometry *g) {
+  return g->geometry == MBIR_CONE && g->psf_radius == 1 && g->bp_psf_radius <= 3 &&
+         g->num_det_rows <= 1024;
+}
+
+int cone_rt_threads(const mbir_geometry *g) { return (g->num_det_rows + 31) / 32 * 32; }
+
+size_t cone_rt_smem(const mbir_geometry *g, int band) {
+  const int nthr = cone_rt_threads(g);
+  return sizeof(float) * ((size_t)kFwdEB * (band + 2 * kFwdVPad) + (size_t)fwd_cap(nthr) * kFwdRec);
+}
+
+template <typename EPI>
+int launch_cone_rt(const mbir_geometry *g, const float *vp, int v_start, int v_count,
+                   const float *values, long long P, int band, int slice_start,
+                   const int64_t *pix, const EPI &epi, cudaStream_t st, const char *what,
+                   int by_pixel) {
+  const Geo geo = make_geo(*g);
+  const size_t smem = cone_rt_smem(g, band);
+  auto k = forward_cone_rt_kernel<EPI>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+      return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s", smem,
+                  cudaGetErrorString(e));
+  }
+  dim3 grid((g->num_det_channels + kFwdCB - 1) / kFwdCB, v_count);
+  tpre(st);
+  k<<<grid, cone_rt_threads(g), smem, st>>>(geo, vp, v_start, values, (int)P, band, slice_start,
+                                             pix, by_pixel, epi);
+  MBIR_CHECK_LAUNCH(what);
+  return MBIR_OK;
+}
+
 template <typename EPI>
 int run_forward(const mbir_geometry *g, const float *vp, int v_start, int v_count,
                 const float *values, long long P, int band, int slice_start, const int64_t *pix,
                 const EPI &epi, cudaStream_t st, const char *what = "forward projection",
                 int by_pixel = 0) {
+  if (use_cone_rt(g))
+    return launch_cone_rt(g, vp, v_start, v_count, values, P, band, slice_start, pix, epi, st,
+                          what, by_pixel);
   const FwdShape fs = fwd_shape(g, band);
 #define MBIR_FWD(CONEV, NTV) \
   launch_forward<CONEV, NTV>(g, vp, v_start, v_count, values, P, band, slice_start, pix, fs, epi, st, what, by_pixel)
@@ -291,6 +330,7 @@ int run_forward(const mbir_geometry *g, const float *vp, int v_start, int v_coun
 }
 
 int fwd_blocks(const mbir_geometry *g, int band, int v_count) {
+  if (use_cone_rt(g)) return ((g->num_det_channels + kFwdCB - 1) / kFwdCB) * v_count;
   const FwdShape fs = fwd_shape(g, band);
   return ((g->num_det_channels + fs.CB - 1) / fs.CB) * v_count;
 }

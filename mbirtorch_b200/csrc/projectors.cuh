@@ -503,4 +503,191 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
   epi.end(blockIdx.y * gridDim.x + blockIdx.x);
 }
 
+// ── forward projection, cone, register-tiled ───────────────────────────────
+// The cone forward for psf radius 1 and up to 1024 detector rows.  A CTA
+// owns one view and kFwdCB channels; thread m owns detector row m and keeps
+// the row's kFwdCB channel sums in registers.  Pixels reaching the block are
+// compacted as in forward_kernel, then processed in batches of kFwdEB: the
+// batch's cylinders, scaled by 1 / cos(phi) per slice, are staged in
+// zero-padded shared memory (one rsqrt per voxel), and every thread forms
+// its row's detector-side vertical fan from them (cone_beam.py:203-226)
+// and adds the three channel taps into registers.  The tap -> register map
+// depends on the pixel's centre channel, which is the same for all threads,
+// so it is a warp-uniform switch over compile-time register indices: no
+// shared-memory read-modify-write chains, no atomics, fixed summation order.
+constexpr int kFwdCB = 16;   // channels per CTA
+constexpr int kFwdEB = 16;   // pixels staged per batch
+constexpr int kFwdVPad = 8;  // zero slices either side of a staged cylinder (>= 2 bp + 1)
+constexpr int kFwdRec = 12;  // record words per pixel
+
+// Record capacity of one compaction round: at least one scan chunk.
+__host__ __device__ inline int fwd_cap(int nthr) { return nthr > 512 ? nthr : 512; }
+
+template <int J>
+__device__ __forceinline__ void fwd_taps(float (&acc)[kFwdCB], float w0, float w1, float w2,
+                                         float det) {
+  // Case J: the pixel's centre channel is c0 + J - 1, so tap t lands on
+  // block channel J - 2 + t.
+  if (J - 2 >= 0 && J - 2 < kFwdCB) acc[(J - 2 >= 0 && J - 2 < kFwdCB) ? J - 2 : 0] =
+      fmaf(w0, det, acc[(J - 2 >= 0 && J - 2 < kFwdCB) ? J - 2 : 0]);
+  if (J - 1 >= 0 && J - 1 < kFwdCB) acc[(J - 1 >= 0 && J - 1 < kFwdCB) ? J - 1 : 0] =
+      fmaf(w1, det, acc[(J - 1 >= 0 && J - 1 < kFwdCB) ? J - 1 : 0]);
+  if (J >= 0 && J < kFwdCB) acc[(J >= 0 && J < kFwdCB) ? J : 0] =
+      fmaf(w2, det, acc[(J >= 0 && J < kFwdCB) ? J : 0]);
+}
+
+template <typename EPI>
+__global__ void __launch_bounds__(1024)
+forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
+                       const float *__restrict__ values, int P, int band, int slice_start,
+                       const int64_t *__restrict__ pix, int by_pixel, EPI epi) {
+  extern __shared__ float sm[];
+  const int nthr = blockDim.x;
+  const int kFwdCap = fwd_cap(nthr);
+  const int SP = band + 2 * kFwdVPad;                 // staged cylinder pitch
+  float *stage = sm;                                  // kFwdEB x SP
+  int *r_ctr = (int *)(stage + kFwdEB * SP);          // kFwdCap
+  int *r_row = r_ctr + kFwdCap;                       // kFwdCap
+  float *r_f = (float *)(r_row + kFwdCap);            // 10 x kFwdCap
+  __shared__ int s_wcount[32];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+  const int vl = blockIdx.y;
+  const int v = v_start + vl;
+  const int c0 = blockIdx.x * kFwdCB;
+  const int ncb = min(kFwdCB, g.C - c0);
+  const float ang = vp[2 * v];
+  const float cs = cosf(ang), sn = sinf(ang);
+  const float z_off = __fsub_rn(g.rso, vp[2 * v + 1]);
+  const int m = tid;
+  const float mf = (float)m;
+  const int bp = g.bp;
+  // Clamp of the centre slice: a centre outside [ss - bp - 1, ss + band + bp]
+  // has no tap inside the band, and the clamped one only meets zero padding
+  // (kFwdVPad >= 2 bp + 1).
+  const float kc_lo = (float)(slice_start - bp - 1),
+              kc_hi = (float)(slice_start + band + bp);
+  const int R = g.R;
+
+  for (int i = tid; i < kFwdEB * SP; i += nthr) stage[i] = 0.f;
+  float acc[kFwdCB];
+#pragma unroll
+  for (int j = 0; j < kFwdCB; ++j) acc[j] = 0.f;
+
+  int pos = 0;
+  while (pos < P) {
+    int n = 0;
+    __syncthreads();
+    while (pos < P && n + nthr <= kFwdCap) {
+      const int p = pos + tid;
+      bool keep = false;
+      ConeCenter cc;
+      if (p < P) {
+        float xt, yt;
+        pixel_xy(g, (int)pix[p], xt, yt);
+        cc = cone_center(g, cs, sn, xt, yt);
+        keep = (cc.ctr + 1 >= c0) && (cc.ctr - 1 < c0 + ncb);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (lane == 0) s_wcount[warp] = __popc(bal);
+      __syncthreads();
+      int off = n, tot = 0;
+      for (int w = 0; w < nwarps; ++w) {
+        const int c = s_wcount[w];
+        if (w < warp) off += c;
+        tot += c;
+      }
+      if (keep) {
+        const int s = off + __popc(bal & ((1u << lane) - 1u));
+        const ConeVP q = cone_finish(g, ang, z_off, cc);
+        float a0, a1;
+        cone_tcoef(g, q.mag, z_off, a0, a1);
+        r_ctr[s] = cc.ctr - c0 + 1;  // switch case: centre channel + 1, in [0, kFwdCB + 1]
+        r_row[s] = by_pixel ? (int)pix[p] : p;
+        r_f[0 * kFwdCap + s] = tap_weight(cc.n_p, cc.ctr - 1, q.half_w1, q.lmax, q.ws, g.C);
+        r_f[1 * kFwdCap + s] = tap_weight(cc.n_p, cc.ctr, q.half_w1, q.lmax, q.ws, g.C);
+        r_f[2 * kFwdCap + s] = tap_weight(cc.n_p, cc.ctr + 1, q.half_w1, q.lmax, q.ws, g.C);
+        r_f[3 * kFwdCap + s] = q.m0;
+        r_f[4 * kFwdCap + s] = q.w_r;
+        r_f[5 * kFwdCap + s] = __fdiv_rn(__fadd_rn(q.w_r, 1.f), 2.f);
+        r_f[6 * kFwdCap + s] = fminf(q.w_r, 1.f);
+        r_f[7 * kFwdCap + s] = 1.f / q.w_r;
+        r_f[8 * kFwdCap + s] = a0;
+        r_f[9 * kFwdCap + s] = a1;
+      }
+      n += tot;
+      pos += nthr;
+      __syncthreads();
+    }
+    for (int b0 = 0; b0 < n; b0 += kFwdEB) {
+      const int nb = min(kFwdEB, n - b0);
+      // Stage the batch's scaled cylinders.
+      for (int i = tid; i < nb * band; i += nthr) {
+        const int e = i / band, k = i - e * band;
+        const int r = b0 + e;
+        const float tk = fmaf(r_f[9 * kFwdCap + r], (float)(slice_start + k), r_f[8 * kFwdCap + r]);
+        stage[e * SP + kFwdVPad + k] =
+            __ldg(values + (size_t)r_row[r] * band + k) * inv_cos_from_t(tk);
+      }
+      __syncthreads();
+      if (m < R) {
+        for (int e = 0; e < nb; ++e) {
+          const int r = b0 + e;
+          const float m0 = r_f[3 * kFwdCap + r], w_r = r_f[4 * kFwdCap + r];
+          const float hw1r = r_f[5 * kFwdCap + r], lmaxr = r_f[6 * kFwdCap + r];
+          const float inv_wr = r_f[7 * kFwdCap + r];
+          const float k_m = (mf - m0) * inv_wr;
+          const float kc = fminf(fmaxf(rintf(k_m), kc_lo), kc_hi);
+          const float d = w_r * (kc - k_m);
+          const float *st = stage + e * SP + kFwdVPad + ((int)kc - slice_start);
+          float det;
+          if (bp == 1) {
+            const float am = fminf(fmaxf(hw1r - fabsf(d - w_r), 0.f), lmaxr);
+            const float a0 = fminf(fmaxf(hw1r - fabsf(d), 0.f), lmaxr);
+            const float ap = fminf(fmaxf(hw1r - fabsf(d + w_r), 0.f), lmaxr);
+            det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
+          } else {
+            det = 0.f;
+            for (int ko = -bp; ko <= bp; ++ko) {
+              const float a = fminf(fmaxf(hw1r - fabsf(fmaf(w_r, (float)ko, d)), 0.f), lmaxr);
+              det = fmaf(a, st[ko], det);
+            }
+          }
+          const float w0 = r_f[0 * kFwdCap + r], w1 = r_f[1 * kFwdCap + r];
+          const float w2 = r_f[2 * kFwdCap + r];
+          switch (r_ctr[r]) {
+            case 0: fwd_taps<0>(acc, w0, w1, w2, det); break;
+            case 1: fwd_taps<1>(acc, w0, w1, w2, det); break;
+            case 2: fwd_taps<2>(acc, w0, w1, w2, det); break;
+            case 3: fwd_taps<3>(acc, w0, w1, w2, det); break;
+            case 4: fwd_taps<4>(acc, w0, w1, w2, det); break;
+            case 5: fwd_taps<5>(acc, w0, w1, w2, det); break;
+            case 6: fwd_taps<6>(acc, w0, w1, w2, det); break;
+            case 7: fwd_taps<7>(acc, w0, w1, w2, det); break;
+            case 8: fwd_taps<8>(acc, w0, w1, w2, det); break;
+            case 9: fwd_taps<9>(acc, w0, w1, w2, det); break;
+            case 10: fwd_taps<10>(acc, w0, w1, w2, det); break;
+            case 11: fwd_taps<11>(acc, w0, w1, w2, det); break;
+            case 12: fwd_taps<12>(acc, w0, w1, w2, det); break;
+            case 13: fwd_taps<13>(acc, w0, w1, w2, det); break;
+            case 14: fwd_taps<14>(acc, w0, w1, w2, det); break;
+            case 15: fwd_taps<15>(acc, w0, w1, w2, det); break;
+            case 16: fwd_taps<16>(acc, w0, w1, w2, det); break;
+            default: fwd_taps<17>(acc, w0, w1, w2, det); break;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // Epilogue: thread m hands over its row's cells, channel by channel.
+  epi.begin();
+  if (m < R) {
+#pragma unroll
+    for (int j = 0; j < kFwdCB; ++j)
+      if (j < ncb) epi.cell(vl, c0 + j, m, acc[j]);
+  }
+  epi.end(blockIdx.y * gridDim.x + blockIdx.x);
+}
+
 }  // namespace mbir

@@ -70,7 +70,7 @@ __device__ __forceinline__ float b_tilde(float delta, const VcdScalars &s) {
 
 // Block-wide sum of two doubles; returns the totals in thread 0.
 __device__ __forceinline__ void block_sum2(double &a, double &b) {
-  __shared__ double sa[kThreads / 32], sb[kThreads / 32];
+  __shared__ double sa[32], sb[32];
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_down_sync(0xffffffffu, a, o);
     b += __shfl_down_sync(0xffffffffu, b, o);

@@ -1,0 +1,276 @@
+"""Continuous-batching reconstruction server.
+
+Requests -- reconstructions of mixed geometry and size -- arrive over time.
+The server admits a request as soon as a slot and device memory allow it
+(a byte ledger, not a queue alone), keeps every admitted job's volume, error
+sinogram and VCD state resident on the device, and advances all admitted
+jobs concurrently: each job owns a CUDA stream, and the scheduler enqueues
+a job's next VCD iteration as soon as its previous one has finished, so the
+iterations of different jobs overlap on the GPU.  A finished job releases
+its memory and slot, which admits the next waiting request.
+
+Each job draws its partitions and subset orders from its own seeded
+RandomState (in the reference's call order), and every kernel is
+deterministic, so a job's result is bitwise the same whether it runs alone
+or in a mix.  Latency is measured from arrival to result on the host clock;
+:meth:`ReconServer.stats` reports p50/p99 and recons/s.
+
+The device memory ledger follows the closed-form design of the reference's
+memory model (_memory_ledger.py:1-38): a job is charged its peak bytes
+during preparation (sinogram-sized FP32 transients of the direct-recon init)
+and its resident bytes afterwards.
+"""
+
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _lib, vcd_utils
+from .vcd_engine import make_vcd_params, storage_code
+from .vcd_run import VcdRun
+
+
+class MemoryLedger:
+    """Admission by device bytes: ``fits`` / ``take`` / ``release``."""
+
+    def __init__(self, budget_bytes):
+        self.budget = int(budget_bytes)
+        self.used = 0
+
+    def fits(self, nbytes):
+        return self.used + int(nbytes) <= self.budget
+
+    def take(self, nbytes):
+        self.used += int(nbytes)
+
+    def release(self, nbytes):
+        self.used -= int(nbytes)
+
+    @staticmethod
+    def job_bytes(model, storage_dtype, weighted, max_subset_pixels):
+        """(peak during preparation, resident afterwards) in bytes."""
+        V, R, C = model.get_params('sinogram_shape')
+        nr, nc, ns = model.get_params('recon_shape')
+        n_sino, n_vol = V * R * C, nr * nc * ns
+        code = storage_code(storage_dtype)
+        s = 4 if code == _lib.MBIR_F32 else 2
+        prm = make_vcd_params(1.0, 1.0, 2.0, 1.2, 1.0, [1 / 6] * 6, 1.5, False, code)
+        ws = int(_lib.load().mbir_vcd_workspace_size(model._geometry(), int(max_subset_pixels),
+                                                     prm))
+        y = 4 * n_sino if code != _lib.MBIR_F32 else 0
+        resident = y + (2 if weighted else 1) * s * n_sino + ws + 8 * n_vol
+        init = 4 * 4 * n_sino + 3 * 4 * n_vol + y + (4 * n_sino if weighted else 0)
+        return max(init, resident), resident
+
+
+class Request:
+    """One reconstruction request and, once served, its result."""
+
+    def __init__(self, rid, model, sinogram, weights, max_iterations, stop_threshold_change_pct,
+                 seed, arrival):
+        self.id = rid
+        self.model = model
+        self.sinogram = sinogram
+        self.weights = weights
+        self.max_iterations = int(max_iterations)
+        self.stop_pct = float(stop_threshold_change_pct)
+        self.seed = int(seed)
+        self.arrival = arrival
+        self.admitted = None
+        self.finished = None
+        self.recon = None
+        self.recon_params = None
+        self.error = None
+        self._run = None
+        self._stream = None
+        self._charge = 0
+        self._out = None
+        self._out_event = None
+
+    def done(self):
+        return self.finished is not None
+
+    @property
+    def latency(self):
+        return None if self.finished is None else self.finished - self.arrival
+
+    def result(self):
+        if self.error is not None:
+            raise self.error
+        return self.recon
+
+
+class ReconServer:
+    """Serve reconstructions with continuous batching on one GPU.
+
+    Args:
+        device: CUDA device (default: the current one).
+        memory_budget_bytes: ledger budget (default: 80% of the free memory).
+        max_active: most jobs resident at once.
+        storage_dtype: resident precision of the error sinogram, weights and
+            delta sinogram ('float16' by default; see TomographyModel).
+    """
+
+    def __init__(self, device=None, memory_budget_bytes=None, max_active=8,
+                 storage_dtype='float16'):
+        self.device = torch.device('cuda', torch.cuda.current_device()) if device is None \
+            else torch.device(device)
+        if memory_budget_bytes is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            memory_budget_bytes = int(0.8 * free)
+        self.ledger = MemoryLedger(memory_budget_bytes)
+        self.max_active = int(max_active)
+        self.storage_dtype = storage_dtype
+        storage_code(storage_dtype)
+        self.waiting = []
+        self.active = []
+        self.completed = []
+        self._next_id = 0
+        self.max_concurrent = 0
+        self.t0 = None
+
+    # ── requests ───────────────────────────────────────────────────────────
+    def submit(self, model, sinogram, weights=None, max_iterations=10,
+               stop_threshold_change_pct=0.0, seed=0, arrival=None):
+        """Queue a reconstruction; returns its :class:`Request`."""
+        now = time.perf_counter()
+        if self.t0 is None:
+            self.t0 = now
+        r = Request(self._next_id, model, sinogram, weights, max_iterations,
+                    stop_threshold_change_pct, seed, now if arrival is None else arrival)
+        self._next_id += 1
+        self.waiting.append(r)
+        return r
+
+    # ── scheduling ─────────────────────────────────────────────────────────
+    def _admit(self, r):
+        m = r.model
+        m.storage_dtype = self.storage_dtype
+        m.configure_devices(devices=[self.device])
+        m.setup_logger(logfile_path=None, print_logs=False)
+        rng = np.random.RandomState(r.seed)
+        rs, gran, ror = m.get_params(['recon_shape', 'granularity', 'use_ror_mask'])
+        parts = [vcd_utils.gen_pixel_partition(rs, n, use_ror_mask=ror, rng=rng) for n in gran]
+        seq = vcd_utils.gen_partition_sequence(m.get_params('partition_sequence'),
+                                               r.max_iterations)
+        max_ps = max((int(parts[int(i)].shape[1]) for i in seq), default=1)
+        peak, resident = MemoryLedger.job_bytes(m, self.storage_dtype, r.weights is not None,
+                                                max_ps)
+        if not self.ledger.fits(peak) and self.active:
+            return False
+        m.auto_set_regularization_params(r.sinogram, weights=r.weights)
+        r._stream = torch.cuda.Stream(self.device)
+        r._run = VcdRun(m, r.sinogram, parts, seq, r.stop_pct, weights=r.weights, rng=rng,
+                        stream=r._stream)
+        self.ledger.take(peak)
+        r._charge = peak
+        r.admitted = time.perf_counter()
+        with torch.cuda.device(self.device):
+            r._run.prepare()
+        self.ledger.release(peak - resident)
+        r._charge = resident
+        if not r._run.finished:
+            r._run.enqueue_iteration()
+        return True
+
+    def _finish(self, r):
+        run = r._run
+        with torch.cuda.stream(r._stream):
+            r._out = torch.empty(run.flat.shape, dtype=torch.float32, pin_memory=True)
+            r._out.copy_(run.flat, non_blocking=True)
+            r._out_event = torch.cuda.Event()
+            r._out_event.record(r._stream)
+        fm, _, nmae, alphas, dnorm = run.losses()
+        r.recon_params = {'num_iterations': run.done, 'fm_rmse': [float(v) for v in fm],
+                          'stop_threshold_change_pct': [100 * float(v) for v in nmae],
+                          'alpha_values': [float(v) for v in alphas]}
+
+    def step(self):
+        """One scheduler pass; returns True if it did anything."""
+        busy = False
+        # advance the admitted jobs
+        for r in list(self.active):
+            if r._out_event is not None:
+                if r._out_event.query():
+                    rs = r._run.recon_shape
+                    r.recon = r._out.numpy().reshape(rs)
+                    r.finished = time.perf_counter()
+                    r._run = None
+                    self.ledger.release(r._charge)
+                    r._charge = 0
+                    self.active.remove(r)
+                    self.completed.append(r)
+                    busy = True
+                continue
+            if r._run.ready():
+                if r._run.collect():
+                    self._finish(r)
+                else:
+                    r._run.enqueue_iteration()
+                busy = True
+        # admit waiting requests in arrival order while slots and memory allow
+        while self.waiting and len(self.active) < self.max_active:
+            r = self.waiting[0]
+            try:
+                if not self._admit(r):
+                    break
+            except Exception as exc:  # a failing job frees its slot, others go on
+                r.error = exc
+                r.finished = time.perf_counter()
+                if r._charge:
+                    self.ledger.release(r._charge)
+                    r._charge = 0
+                self.waiting.pop(0)
+                self.completed.append(r)
+                busy = True
+                continue
+            self.waiting.pop(0)
+            self.active.append(r)
+            busy = True
+        self.max_concurrent = max(self.max_concurrent, len(self.active))
+        return busy
+
+    def run_until_idle(self, poll_s=2e-4, timeout_s=None):
+        t_end = None if timeout_s is None else time.perf_counter() + timeout_s
+        while self.waiting or self.active:
+            if not self.step():
+                time.sleep(poll_s)
+            if t_end is not None and time.perf_counter() > t_end:
+                raise TimeoutError('server did not drain in time')
+
+    def serve_schedule(self, schedule, poll_s=2e-4, timeout_s=None):
+        """Submit requests at their arrival offsets (seconds from now) while
+        serving: ``schedule`` is a list of (offset_s, submit_kwargs)."""
+        start = time.perf_counter()
+        if self.t0 is None:
+            self.t0 = start
+        pending = sorted(schedule, key=lambda s: s[0])
+        t_end = None if timeout_s is None else start + timeout_s
+        i = 0
+        while i < len(pending) or self.waiting or self.active:
+            now = time.perf_counter()
+            while i < len(pending) and start + pending[i][0] <= now:
+                kw = dict(pending[i][1])
+                kw.setdefault('arrival', start + pending[i][0])
+                self.submit(**kw)
+                i += 1
+            if not self.step():
+                time.sleep(poll_s)
+            if t_end is not None and time.perf_counter() > t_end:
+                raise TimeoutError('server did not drain in time')
+        return self.completed
+
+    # ── metrics ────────────────────────────────────────────────────────────
+    def stats(self):
+        ok = [r for r in self.completed if r.error is None]
+        lat = np.array([r.latency for r in ok]) if ok else np.zeros(0)
+        span = (max(r.finished for r in ok) - min(r.arrival for r in ok)) if ok else 0.0
+        return {
+            'completed': len(ok), 'failed': len(self.completed) - len(ok),
+            'recons_per_s': (len(ok) / span) if span > 0 else math.nan,
+            'p50_latency_s': float(np.percentile(lat, 50)) if ok else math.nan,
+            'p99_latency_s': float(np.percentile(lat, 99)) if ok else math.nan,
+            'max_concurrent': self.max_concurrent, 'span_s': span,
+        }

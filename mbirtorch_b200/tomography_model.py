@@ -23,20 +23,19 @@ What differs by design:
 """
 
 import datetime
-import math
 import os
 import warnings
 
 import numpy as np
 import torch
 
-from . import _lib, tomography_utils, vcd_utils
+from . import tomography_utils, vcd_utils
 from . import qggmrf as _qggmrf
 from ._utils import AUTO_REGULARIZATION_PARAM_NAMES, Param, recon_param_names
 from .kernels import DeviceProjector
 from .parameter_handler import ParameterHandler
-from .vcd_engine import (ResidentSinogram, VcdEngine, error_init, iteration_stats,
-                         make_vcd_params, order_array, storage_code)
+from .vcd_engine import (ResidentSinogram, VcdEngine, make_vcd_params, order_array,
+                         storage_code)
 
 _F32_EPS = float(np.finfo(np.float32).eps)
 
@@ -510,14 +509,6 @@ class TomographyModel(ParameterHandler):
         recon_dict = self.get_recon_dict(recon_params, notes=notes)
         return self._out(recon, output_sharded), recon_dict
 
-    def _initial_error_state(self, sino, init_recon, weights, scale_recon_to_sinogram):
-        """(error f32 VRC, scaled init recon) -- tomography_model.py:1666-1712."""
-        self.logger.info('Initializing error sinogram')
-        fwd = self.forward_project(init_recon, output_sharded=True)
-        err, alpha = error_init(sino, fwd, weights, scale_recon_to_sinogram)
-        a = float(alpha.item())
-        return err, init_recon * a
-
     def _vcd_recon(self, sinogram, partitions, partition_sequence, stop_threshold_change_pct,
                    weights=None, init_recon=None, prox_input=None, compute_prior_loss=False,
                    first_iteration=0, init_error_sinogram=None, fm_hessian=None,
@@ -528,109 +519,14 @@ class TomographyModel(ParameterHandler):
         if prox_input is not None:
             raise NotImplementedError('the proximal-map prior is not implemented on the '
                                       'sm_100a path yet')
-        self.verify_valid_params()
-        self._require_cuda()
-        recon_shape = self.get_params('recon_shape')
-        sinogram_shape = self.get_params('sinogram_shape')
-        if tuple(sinogram.shape) != tuple(sinogram_shape):
-            raise ValueError('sinogram does not have the shape in sinogram_shape. \n'
-                             f'Expected {tuple(sinogram_shape)}, got {tuple(sinogram.shape)}.')
-        storage = storage_code(self.storage_dtype)
-        constant_weights = weights is None
-        w_dev = None if constant_weights else self._sino_device(weights)
-        if init_error_sinogram is not None and init_recon is None:
-            raise ValueError('init_error_sinogram requires init_recon (the pair must be a '
-                             'consistent resume state; see the docstring).')
-        sino = None if init_error_sinogram is not None else self._sino_device(sinogram)
-        refresh = self.error_refresh_interval
-        if refresh is None:
-            refresh = 0 if storage == _lib.MBIR_F32 else 1
-        y_vcr = None
-        if refresh and sino is not None:
-            y_vcr = ResidentSinogram.from_vrc(sino, _lib.MBIR_F32).data
-        scale = init_recon is None
-        if init_recon is None:
-            self.logger.info('Starting direct recon for initial reconstruction')
-            init_recon = self.recon_direct(sino, output_sharded=True)
-        elif isinstance(init_recon, int):
-            init_recon = torch.full(tuple(recon_shape), float(init_recon), dtype=torch.float32,
-                                    device=self.torch_device)
-        else:
-            if tuple(np.shape(init_recon)) != tuple(recon_shape):
-                raise ValueError(f"init_recon does not have the correct shape. Expected "
-                                 f"{tuple(recon_shape)}, got {tuple(np.shape(init_recon))}.")
-            init_recon = self._recon_device(init_recon)
-        if init_error_sinogram is not None:
-            self.logger.info('Resuming from init_error_sinogram')
-            err_vrc = self._sino_device(init_error_sinogram)
-        else:
-            err_vrc, init_recon = self._initial_error_state(sino, init_recon, w_dev, scale)
-        sino = None
-        if fm_hessian is None:
-            self.logger.info('Computing Hessian diagonal')
-            hess_idx = None if self.get_params('use_ror_mask') is False \
-                else self.full_indices_device()
-            fm_hessian = self.compute_hessian_diagonal(weights=w_dev, output_sharded=True,
-                                                       indices=hess_idx)
-        else:
-            self.logger.info('Using precomputed Hessian diagonal')
-            fm_hessian = self._recon_device(fm_hessian)
-        H = fm_hessian.reshape(-1, fm_hessian.shape[-1]).contiguous()
-        flat = init_recon.reshape(-1, init_recon.shape[-1]).contiguous().clone()
-
-        err = ResidentSinogram.from_vrc(err_vrc, storage)
-        del err_vrc
-        w_res = None if w_dev is None else ResidentSinogram.from_vrc(w_dev, storage)
-        del w_dev
-        parts_dev = [torch.as_tensor(np.ascontiguousarray(p), dtype=torch.int64,
-                                     device=self.torch_device) for p in partitions]
-        max_ps = max(int(partitions[int(i)].shape[1]) for i in partition_sequence) \
-            if len(partition_sequence) else 1
-        engine = self._make_engine(H, w_res, storage, max_subset_pixels=max_ps)
-        self.logger.info('Starting VCD iterations')
-
-        verbose, sigma_y = self.get_params(['verbose', 'sigma_y'])
-        total = float(math.prod(sinogram_shape))
-        n_it = len(partition_sequence)
-        fm_rmse = np.zeros(n_it)
-        pm_loss = np.zeros(n_it)
-        nmae = np.zeros(n_it)
-        alphas = np.zeros(n_it)
-        dnorm = np.zeros((n_it, recon_shape[2]))
-        done = 0
-        for i in range(n_it):
-            part = parts_dev[int(partition_sequence[i])]
-            order = order_array(part.shape[0])
-            engine.accum.zero_()
-            engine.partition_pass(flat, err, part, order)
-            if y_vcr is not None and (i + 1) % refresh == 0:
-                engine.refresh_error(flat, err, self.full_indices_device(), y_vcr)
-            stats = iteration_stats(err, w_res, flat)
-            host = torch.cat([engine.accum, stats]).cpu().numpy()
-            acc, st = host[:2 + recon_shape[2]], host[2 + recon_shape[2]:]
-            avg_w = 1.0 if constant_weights else st[1] / total
-            fm_rmse[i] = math.sqrt(st[0] / (avg_w * total)) / sigma_y
-            recon_l1 = st[3]
-            nmae[i] = acc[0] / recon_l1 if recon_l1 else float('nan')
-            alphas[i] = acc[1] / part.shape[0]
-            dnorm[i] = np.sqrt(acc[2:])
-            if verbose >= 1:
-                self.logger.info(
-                    '\nAfter iteration {} of a max of {}: Pct change={:.4f}, Forward loss={:.4f}'
-                    .format(i + first_iteration, n_it + first_iteration, 100 * nmae[i],
-                            fm_rmse[i]))
-                self.logger.info(f'Relative step size (alpha)={alphas[i]:.2f}, '
-                                 f'Error sino RMSE={math.sqrt(st[2] / total):.4f}')
-                self.logger.info('Number subsets = {}'.format(part.shape[0]))
-            done += 1
-            if nmae[i] < stop_threshold_change_pct / 100:
-                self.logger.warning('Change threshold stopping condition reached')
-                break
-        recon3 = flat.reshape(tuple(recon_shape[:2]) + (flat.shape[-1],))
-        losses = (fm_rmse[:done], pm_loss[:done], nmae[:done], alphas[:done], dnorm[:done])
+        from .vcd_run import VcdRun
+        run = VcdRun(self, sinogram, partitions, partition_sequence, stop_threshold_change_pct,
+                     weights=weights, init_recon=init_recon,
+                     init_error_sinogram=init_error_sinogram, fm_hessian=fm_hessian,
+                     first_iteration=first_iteration).run()
         if return_checkpoint:
-            return recon3, losses, {'error_sinogram': err.to_vrc(), 'fm_hessian': fm_hessian}
-        return recon3, losses
+            return run.recon3d(), run.losses(), run.checkpoint()
+        return run.recon3d(), run.losses()
 
     # ── model description ───────────────────────────────────────────────────
     def get_recon_dict(self, recon_params=None, notes=None, save_log=True, save_model=True,

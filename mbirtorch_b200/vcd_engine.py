@@ -202,7 +202,8 @@ def error_init(y, ax, weights, scale_to_data):
     return err, alpha
 
 
-def order_array(n_subsets):
+def order_array(n_subsets, rng=None):
     """The per-iteration subset order: one draw from numpy's global RNG,
-    exactly as the reference (tomography_model.py:2684-2686)."""
-    return np.random.permutation(n_subsets).astype(np.int32)
+    exactly as the reference (tomography_model.py:2684-2686), or from
+    ``rng`` (a RandomState) with the same call."""
+    return (np.random if rng is None else rng).permutation(n_subsets).astype(np.int32)

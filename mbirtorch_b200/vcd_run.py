@@ -1,0 +1,232 @@
+"""One reconstruction's device state, split into steps.
+
+This is the body of the reference's ``_vcd_recon`` (tomography_model.py:
+2699-3013) restructured so that the same code serves a single blocking
+``recon()`` and a server that interleaves many reconstructions:
+
+* :meth:`VcdRun.prepare` -- host prep done by the caller (partitions, the
+  partition sequence and the regularization), then, on the run's CUDA
+  stream: the sinogram upload, the direct-recon init, the optimally scaled
+  initial error state, the Hessian diagonal and the resident VCD state.
+  No host synchronization.
+* :meth:`VcdRun.enqueue_iteration` -- one VCD iteration (one partition pass
+  in an order drawn from the run's RNG), the optional 16-bit refresh and the
+  statistics, with an asynchronous copy of the statistics to pinned host
+  memory and an event.
+* :meth:`VcdRun.ready` / :meth:`VcdRun.collect` -- poll the event, then turn
+  the statistics into the reference's per-iteration traces and the stopping
+  decision.
+
+Every run owns its stream, its RNG and its buffers, and the kernels are
+deterministic, so a run's result does not depend on what else is running.
+"""
+
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .vcd_engine import ResidentSinogram, error_init, iteration_stats, order_array, storage_code
+
+
+class VcdRun:
+
+    def __init__(self, model, sinogram, partitions, partition_sequence,
+                 stop_threshold_change_pct, weights=None, init_recon=None,
+                 init_error_sinogram=None, fm_hessian=None, rng=None, first_iteration=0,
+                 stream=None):
+        model.verify_valid_params()
+        model._require_cuda()
+        self.model = model
+        self.recon_shape = tuple(model.get_params('recon_shape'))
+        self.sinogram_shape = tuple(model.get_params('sinogram_shape'))
+        if init_error_sinogram is None and tuple(sinogram.shape) != self.sinogram_shape:
+            raise ValueError('sinogram does not have the shape in sinogram_shape. \n'
+                             f'Expected {self.sinogram_shape}, got {tuple(sinogram.shape)}.')
+        if init_error_sinogram is not None and init_recon is None:
+            raise ValueError('init_error_sinogram requires init_recon (the pair must be a '
+                             'consistent resume state; see the docstring).')
+        self.sinogram = sinogram
+        self.weights = weights
+        self.init_recon = init_recon
+        self.init_error_sinogram = init_error_sinogram
+        self.fm_hessian = fm_hessian
+        self.partitions = partitions
+        self.seq = np.asarray(partition_sequence)
+        self.stop_pct = stop_threshold_change_pct
+        self.rng = rng
+        self.first_iteration = first_iteration
+        self.storage = storage_code(model.storage_dtype)
+        self.stream = stream if stream is not None else torch.cuda.current_stream(
+            model.torch_device)
+        n = len(self.seq)
+        self.fm_rmse = np.zeros(n)
+        self.pm_loss = np.zeros(n)
+        self.nmae = np.zeros(n)
+        self.alphas = np.zeros(n)
+        self.dnorm = np.zeros((n, self.recon_shape[2]))
+        self.done = 0
+        self.finished = n == 0
+        self._event = None
+        self._pending = None
+
+    # ── device preparation ───────────────────────────────────────────────
+    def prepare(self):
+        m = self.model
+        with torch.cuda.stream(self.stream):
+            self._prepare()
+        return self
+
+    def _prepare(self):
+        m = self.model
+        dev = m.torch_device
+        log = m.logger
+        w_dev = None if self.weights is None else m._sino_device(self.weights)
+        self.constant_weights = w_dev is None
+        sino = None if self.init_error_sinogram is not None else m._sino_device(self.sinogram)
+        refresh = m.error_refresh_interval
+        if refresh is None:
+            refresh = 0 if self.storage == _lib.MBIR_F32 else 1
+        self.refresh = refresh
+        self.y_vcr = None
+        if refresh and sino is not None:
+            self.y_vcr = ResidentSinogram.from_vrc(sino, _lib.MBIR_F32).data
+        init_recon = self.init_recon
+        scale = init_recon is None
+        if init_recon is None:
+            log.info('Starting direct recon for initial reconstruction')
+            init_recon = m.recon_direct(sino, output_sharded=True)
+        elif isinstance(init_recon, int):
+            init_recon = torch.full(self.recon_shape, float(init_recon), dtype=torch.float32,
+                                    device=dev)
+        else:
+            if tuple(np.shape(init_recon)) != self.recon_shape:
+                raise ValueError(f"init_recon does not have the correct shape. Expected "
+                                 f"{self.recon_shape}, got {tuple(np.shape(init_recon))}.")
+            init_recon = m._recon_device(init_recon)
+        if self.init_error_sinogram is not None:
+            log.info('Resuming from init_error_sinogram')
+            err_vrc = m._sino_device(self.init_error_sinogram)
+            x0 = init_recon
+        else:
+            log.info('Initializing error sinogram')
+            fwd = m.forward_project(init_recon, output_sharded=True)
+            err_vrc, alpha = error_init(sino, fwd, w_dev, scale)
+            del fwd
+            # alpha stays on the device: x0 = float32(alpha) * x0, as the
+            # reference's python-float scaling (tomography_model.py:1700-1711)
+            x0 = init_recon * alpha.to(torch.float32)
+        sino = None
+        if self.fm_hessian is None:
+            log.info('Computing Hessian diagonal')
+            hess_idx = None if m.get_params('use_ror_mask') is False \
+                else m.full_indices_device()
+            self.fm_hessian = m.compute_hessian_diagonal(weights=w_dev, output_sharded=True,
+                                                         indices=hess_idx)
+        else:
+            log.info('Using precomputed Hessian diagonal')
+            self.fm_hessian = m._recon_device(self.fm_hessian)
+        H = self.fm_hessian.reshape(-1, self.fm_hessian.shape[-1]).contiguous()
+        self.flat = x0.reshape(-1, x0.shape[-1]).contiguous().clone()
+        self.err = ResidentSinogram.from_vrc(err_vrc, self.storage)
+        del err_vrc
+        self.w_res = None if w_dev is None else ResidentSinogram.from_vrc(w_dev, self.storage)
+        del w_dev
+        self.total = float(math.prod(self.sinogram_shape))
+        self.parts_dev = [torch.as_tensor(np.ascontiguousarray(p), dtype=torch.int64, device=dev)
+                          for p in self.partitions]
+        max_ps = max((int(self.partitions[int(i)].shape[1]) for i in self.seq), default=1)
+        self.engine = m._make_engine(H, self.w_res, self.storage, max_subset_pixels=max_ps)
+        self.host = torch.empty(2 + self.recon_shape[2] + 4, dtype=torch.float64,
+                                pin_memory=True)
+        log.info('Starting VCD iterations')
+
+    # ── iterations ───────────────────────────────────────────────────────
+    def enqueue_iteration(self):
+        """Enqueue iteration ``self.done`` on the run's stream (no sync)."""
+        if self.finished or self._event is not None:
+            raise RuntimeError('no iteration can be enqueued now')
+        i = self.done
+        with torch.cuda.stream(self.stream):
+            part = self.parts_dev[int(self.seq[i])]
+            order = order_array(part.shape[0], self.rng)
+            self.engine.accum.zero_()
+            self.engine.partition_pass(self.flat, self.err, part, order)
+            if self.y_vcr is not None and (i + 1) % self.refresh == 0:
+                self.engine.refresh_error(self.flat, self.err, self.model.full_indices_device(),
+                                          self.y_vcr)
+            stats = iteration_stats(self.err, self.w_res, self.flat)
+            self.host.copy_(torch.cat([self.engine.accum, stats]), non_blocking=True)
+            self._event = torch.cuda.Event()
+            self._event.record(self.stream)
+            self._pending = part.shape[0]
+
+    def ready(self):
+        return self._event is not None and self._event.query()
+
+    def wait(self):
+        if self._event is not None:
+            self._event.synchronize()
+
+    def collect(self):
+        """Read the finished iteration's statistics; returns True when the
+        run is over (iteration count reached or change threshold met)."""
+        self.wait()
+        i, n_sub = self.done, self._pending
+        self._event, self._pending = None, None
+        S = self.recon_shape[2]
+        h = self.host.numpy()
+        acc, st = h[:2 + S], h[2 + S:]
+        sigma_y = self.model.get_params('sigma_y')
+        avg_w = 1.0 if self.constant_weights else st[1] / self.total
+        self.fm_rmse[i] = math.sqrt(st[0] / (avg_w * self.total)) / sigma_y
+        self.nmae[i] = acc[0] / st[3] if st[3] else float('nan')
+        self.alphas[i] = acc[1] / n_sub
+        self.dnorm[i] = np.sqrt(acc[2:])
+        log = self.model.logger
+        if self.model.get_params('verbose') >= 1:
+            n = len(self.seq) + self.first_iteration
+            log.info('\nAfter iteration {} of a max of {}: Pct change={:.4f}, Forward loss={:.4f}'
+                     .format(i + self.first_iteration, n, 100 * self.nmae[i], self.fm_rmse[i]))
+            log.info(f'Relative step size (alpha)={self.alphas[i]:.2f}, '
+                     f'Error sino RMSE={math.sqrt(st[2] / self.total):.4f}')
+            log.info('Number subsets = {}'.format(n_sub))
+        self.done += 1
+        if self.nmae[i] < self.stop_pct / 100:
+            log.warning('Change threshold stopping condition reached')
+            self.finished = True
+        if self.done >= len(self.seq):
+            self.finished = True
+        return self.finished
+
+    def run(self):
+        """Blocking: prepare, then iterate to the end."""
+        self.prepare()
+        while not self.finished:
+            self.enqueue_iteration()
+            self.collect()
+        return self
+
+    # ── results ──────────────────────────────────────────────────────────
+    def recon3d(self):
+        return self.flat.reshape(self.recon_shape[:2] + (self.flat.shape[-1],))
+
+    def losses(self):
+        d = self.done
+        return (self.fm_rmse[:d], self.pm_loss[:d], self.nmae[:d], self.alphas[:d],
+                self.dnorm[:d])
+
+    def checkpoint(self):
+        with torch.cuda.stream(self.stream):
+            return {'error_sinogram': self.err.to_vrc(), 'fm_hessian': self.fm_hessian}
+
+    def device_bytes(self):
+        """Bytes this run holds resident on the device."""
+        n = self.flat.numel() * 4 + self.fm_hessian.numel() * 4 + self.err.nbytes()
+        n += self.engine.workspace_bytes()
+        if self.w_res is not None:
+            n += self.w_res.nbytes()
+        if self.y_vcr is not None:
+            n += self.y_vcr.numel() * 4
+        return n

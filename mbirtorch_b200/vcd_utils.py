@@ -53,11 +53,14 @@ def get_support_radius(recon_shape, delta_voxel_row, delta_voxel_col, use_ror_ma
     return float(np.hypot(hr, hc))
 
 
-def gen_pixel_partition(recon_shape, num_subsets, use_ror_mask=True):
+def gen_pixel_partition(recon_shape, num_subsets, use_ror_mask=True, rng=None):
     """(num_subsets, n) int32 pixel indices, sorted within each subset, equal
     sized (vcd_utils.py:97-156).  RNG use: one np.random.permutation of the
     ROR pixels, then one np.random.choice (without replacement) of the padding
-    indices from the non-final subsets; a single subset draws nothing."""
+    indices from the non-final subsets; a single subset draws nothing.
+    ``rng`` (a numpy RandomState) replaces the global generator with the same
+    call order; None uses numpy's global state, as the reference does."""
+    rng = np.random if rng is None else rng
     nr, nc = recon_shape[:2]
     indices = np.arange(nr * nc, dtype=np.int32)
     if use_ror_mask is not False:
@@ -71,9 +74,9 @@ def gen_pixel_partition(recon_shape, num_subsets, use_ror_mask=True):
         return np.sort(indices).reshape(1, -1)
     per = int(np.ceil(len(indices) / num_subsets))
     n_extra = num_subsets * per - len(indices)
-    indices = np.random.permutation(indices)
+    indices = rng.permutation(indices)
     n_non_final = (num_subsets - 1) * per
-    extra = np.random.choice(indices[:n_non_final], size=n_extra, replace=False)
+    extra = rng.choice(indices[:n_non_final], size=n_extra, replace=False)
     indices = np.concatenate((indices, extra))
     return np.sort(indices.reshape(num_subsets, indices.size // num_subsets), axis=1)
 
