@@ -38,12 +38,14 @@ class MemoryLedger:
     def __init__(self, budget_bytes):
         self.budget = int(budget_bytes)
         self.used = 0
+        self.high_water = 0
 
     def fits(self, nbytes):
         return self.used + int(nbytes) <= self.budget
 
     def take(self, nbytes):
         self.used += int(nbytes)
+        self.high_water = max(self.high_water, self.used)
 
     def release(self, nbytes):
         self.used -= int(nbytes)

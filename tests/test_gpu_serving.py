@@ -1,0 +1,140 @@
+"""Continuous-batching server (GPU).
+
+* Each job's result is bitwise the same served alone and served in a mix of
+  concurrent jobs of different geometry and size -- and the same as
+  model.recon() with np.random seeded like the job.
+* Admission respects the memory ledger; a failing request frees its slot
+  and the others complete.
+* Latency statistics are reported.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import mbirtorch_b200 as mb
+from mbirtorch_b200.serving import MemoryLedger, ReconServer
+
+pytestmark = pytest.mark.gpu
+
+
+def _phantom(rs, seed):
+    rng = np.random.default_rng(seed)
+    g0 = np.linspace(-1, 1, rs[1])
+    g1 = np.linspace(-1, 1, rs[0])
+    z = np.linspace(-1, 1, rs[2])
+    X, Y = np.meshgrid(g0, g1)
+    vol = np.zeros(rs, np.float32)
+    for _ in range(4):
+        c, a = rng.uniform(-0.4, 0.4, 3), rng.uniform(0.1, 0.4, 3)
+        inside = ((X - c[0]) / a[0]) ** 2 + ((Y - c[1]) / a[1]) ** 2
+        vol += rng.uniform(0.2, 1.0) * ((inside[:, :, None] + ((z - c[2]) / a[2]) ** 2) <= 1)
+    return vol
+
+
+def _jobs():
+    """(model factory, sinogram) for a small mix: parallel, cone, helical."""
+    out = []
+    specs = [('parallel', (48, 8, 40)), ('cone', (40, 12, 24)), ('helical', (60, 10, 20)),
+             ('parallel', (36, 4, 30)), ('cone', (32, 16, 28))]
+    for i, (kind, shape) in enumerate(specs):
+        V = shape[0]
+        if kind == 'parallel':
+            def make(V=V, shape=shape):
+                return mb.ParallelBeamModel(shape, np.linspace(0, np.pi, V, endpoint=False))
+        elif kind == 'cone':
+            def make(V=V, shape=shape):
+                return mb.ConeBeamModel(shape, np.linspace(0, 2 * np.pi, V, endpoint=False),
+                                        source_detector_dist=4.0 * shape[2],
+                                        source_iso_dist=2.0 * shape[2])
+        else:
+            def make(V=V, shape=shape):
+                return mb.ConeBeamModel(shape, np.linspace(0, 4 * np.pi, V, endpoint=False),
+                                        source_detector_dist=4.0 * shape[2],
+                                        source_iso_dist=2.0 * shape[2],
+                                        helical_z_shifts=np.linspace(-2, 2, V))
+        m = make()
+        m.set_params(no_warning=True, verbose=0)
+        sino = m.forward_project(_phantom(m.get_params('recon_shape'), i))
+        sino = sino + np.random.default_rng(100 + i).normal(0, 0.01 * sino.max(), sino.shape)
+        out.append((make, sino.astype(np.float32)))
+    return out
+
+
+def _serve(jobs, idxs, storage, max_active=8, budget=None):
+    srv = ReconServer(storage_dtype=storage, max_active=max_active, memory_budget_bytes=budget)
+    reqs = []
+    for i in idxs:
+        make, sino = jobs[i]
+        m = make()
+        m.set_params(no_warning=True, verbose=0)
+        reqs.append(srv.submit(m, sino, max_iterations=3, seed=1000 + i))
+    srv.run_until_idle(timeout_s=300)
+    return srv, reqs
+
+
+@pytest.mark.parametrize("storage", ["float32", "float16"])
+def test_results_same_alone_and_in_mix(storage):
+    jobs = _jobs()
+    _, mix = _serve(jobs, range(len(jobs)), storage, max_active=5)
+    for i in range(len(jobs)):
+        _, alone = _serve(jobs, [i], storage)
+        assert alone[0].error is None and mix[i].error is None
+        assert np.array_equal(alone[0].recon, mix[i].recon), i
+        assert alone[0].recon_params['fm_rmse'] == mix[i].recon_params['fm_rmse']
+
+
+def test_server_equals_model_recon_with_same_seed():
+    jobs = _jobs()
+    _, reqs = _serve(jobs, [1], 'float32')
+    make, sino = jobs[1]
+    m = make()
+    m.set_params(no_warning=True, verbose=0)
+    np.random.seed(1001)
+    rec, _ = m.recon(sino, max_iterations=3, stop_threshold_change_pct=0.0, logfile_path=None,
+                     print_logs=False)
+    assert np.array_equal(rec, reqs[0].recon)
+
+
+def test_admission_respects_ledger_and_failures_are_isolated():
+    jobs = _jobs()
+    # A budget that holds one job at a time (the largest job's peak).
+    peaks = []
+    for make, _ in jobs:
+        m = make()
+        peaks.append(MemoryLedger.job_bytes(m, 'float16', False, 4096)[0])
+    srv = ReconServer(storage_dtype='float16', max_active=8,
+                      memory_budget_bytes=int(max(peaks) * 1.05))
+    reqs = []
+    for i, (make, sino) in enumerate(jobs):
+        m = make()
+        m.set_params(no_warning=True, verbose=0)
+        reqs.append(srv.submit(m, sino, max_iterations=2, seed=i))
+    bad = make()
+    bad.set_params(no_warning=True, verbose=0)
+    reqs.append(srv.submit(bad, np.zeros((3, 3, 3), np.float32), max_iterations=2))
+    srv.run_until_idle(timeout_s=300)
+    assert srv.ledger.high_water <= srv.ledger.budget
+    assert srv.max_concurrent < len(jobs)
+    assert all(r.error is None for r in reqs[:-1])
+    assert isinstance(reqs[-1].error, ValueError)
+    st = srv.stats()
+    assert st['completed'] == len(jobs) and st['failed'] == 1
+    assert st['p99_latency_s'] >= st['p50_latency_s'] > 0
+    assert srv.ledger.used == 0
+
+
+def test_poisson_schedule_overlaps_jobs():
+    jobs = _jobs()
+    rng = np.random.default_rng(0)
+    t = np.cumsum(rng.exponential(0.01, size=len(jobs)))
+    sched = []
+    for i, (make, sino) in enumerate(jobs):
+        m = make()
+        m.set_params(no_warning=True, verbose=0)
+        sched.append((float(t[i]), dict(model=m, sinogram=sino, max_iterations=4, seed=i)))
+    srv = ReconServer(storage_dtype='float16', max_active=4)
+    done = srv.serve_schedule(sched, timeout_s=300)
+    assert len(done) == len(jobs) and all(r.error is None for r in done)
+    assert srv.max_concurrent >= 2
+    torch.cuda.synchronize()

@@ -1,0 +1,35 @@
+"""Serving-layer host logic without a GPU: the memory ledger and its
+closed-form per-job charge."""
+
+import numpy as np
+
+import mbirtorch_b200 as mb
+from mbirtorch_b200.serving import MemoryLedger
+
+
+def _cone(shape):
+    return mb.ConeBeamModel(shape, np.linspace(0, 2 * np.pi, shape[0], endpoint=False),
+                            source_detector_dist=4.0 * shape[2], source_iso_dist=2.0 * shape[2])
+
+
+def test_ledger_admits_within_budget_and_releases():
+    led = MemoryLedger(1000)
+    assert led.fits(600)
+    led.take(600)
+    assert not led.fits(500) and led.fits(400)
+    led.release(600)
+    assert led.used == 0 and led.fits(1000)
+
+
+def test_job_charge_grows_with_size_and_shrinks_with_precision():
+    small, big = _cone((40, 12, 24)), _cone((80, 24, 48))
+    ps, rs = MemoryLedger.job_bytes(small, 'float32', False, 64)
+    pb, rb = MemoryLedger.job_bytes(big, 'float32', False, 64)
+    assert pb > ps and rb > rs and ps >= rs
+    _, r16 = MemoryLedger.job_bytes(big, 'float16', False, 64)
+    _, rw = MemoryLedger.job_bytes(big, 'float16', True, 64)
+    V, R, C = big.get_params('sinogram_shape')
+    # 16-bit storage keeps an FP32 copy of the measurements for the refresh
+    # but halves the error and delta sinograms; weights add one array.
+    assert rw - r16 == 2 * V * R * C
+    assert r16 > 0
