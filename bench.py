@@ -54,7 +54,39 @@ def parse():
     ap.add_argument("--storage", default="float32")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the projector, mixed-precision and CPU-baseline extras")
+    ap.add_argument("--profile-case", choices=["recon", "subset", "projectors"], default=None,
+                    help="run one untimed pass of the workload for an external profiler "
+                         "and exit (no JSON line)")
     return ap.parse_args()
+
+
+def profile_case(case, m, mb, torch, y):
+    """One pass for a profiler: 'recon' is one whole reconstruction;
+    'subset' is three VCD subset steps of a 128-subset partition (the subset
+    size of 17 of the 20 iterations) from a zero volume; 'projectors' is one
+    full-volume forward and one back projection."""
+    if case == "recon":
+        np.random.seed(0)
+        m.recon(y, max_iterations=ITERS, stop_threshold_change_pct=0, logfile_path=None,
+                print_logs=False, output_sharded=True)
+    elif case == "subset":
+        from mbirtorch_b200.vcd_engine import ResidentSinogram
+        m.auto_set_regularization_params(y)
+        H = m.compute_hessian_diagonal(output_sharded=True)
+        upd = m.create_vcd_subset_updater(H, weights=1)
+        rs = m.get_params('recon_shape')
+        flat = torch.zeros(rs[0] * rs[1], rs[2], device=y.device)
+        err = ResidentSinogram.from_vrc(y)
+        np.random.seed(0)
+        parts = torch.as_tensor(mb.gen_pixel_partition(rs, 128), device=y.device)
+        for i in range(3):
+            upd.engine.subset_update(flat, err, parts[i])
+    else:
+        idx = m.full_indices_device()
+        vals = torch.rand(idx.shape[0], NVOX, device=y.device)
+        s = m.projector.forward(vals, idx)
+        m.projector.back(s, idx)
+    torch.cuda.synchronize()
 
 
 # ── synthetic data ──────────────────────────────────────────────────────────
@@ -248,6 +280,8 @@ def main():
     m = make_model(mb)
     m.set_storage_precision(args.storage)
     vol, y = make_data(mb, m, torch, dev)
+    if args.profile_case:
+        return profile_case(args.profile_case, m, mb, torch, y)
     y_host = y.cpu().numpy()
 
     def one_recon(sino):
@@ -403,6 +437,7 @@ def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd):
         mp[st] = {"recons_per_s": 1.0 / dt, "rel_l2_vs_f32_recon": rel}
     m.set_storage_precision(args.storage)
     res["mixed_precision"] = mp
+    res["serving"] = serving_extra(mb, torch, y_host, rec_ref)
     res["fm_rmse_final"] = rd["recon_params"]["fm_rmse"][-1]
     # ── CPU baseline ──
     try:
@@ -411,6 +446,35 @@ def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd):
     except Exception as exc:  # reported, never fatal to the GPU line
         res["cpu_baseline"] = {"value": None, "error": repr(exc)[:200]}
     return res
+
+
+def serving_extra(mb, torch, y_host, rec_ref, jobs=4):
+    """The batched mixed-precision form: `jobs` reconstructions of this
+    workload submitted together to a ReconServer (float16 storage, all jobs
+    resident and advancing concurrently on their own streams).  Job 0 draws
+    its partitions like the timed FP32 recon (seed 0), so its relative L2
+    against that recon is the storage precision's error alone."""
+    from mbirtorch_b200.serving import ReconServer
+    out = {"jobs": jobs, "storage": "float16"}
+    for warm in (True, False):
+        srv = ReconServer(storage_dtype="float16", max_active=jobs)
+        reqs = []
+        t0 = time.perf_counter()
+        for j in range(jobs):
+            mj = make_model(mb)
+            reqs.append(srv.submit(mj, y_host, max_iterations=ITERS, seed=j, arrival=t0))
+        srv.run_until_idle(timeout_s=600)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    st = srv.stats()
+    ref = rec_ref.double().cpu()
+    r0 = torch.as_tensor(reqs[0].recon).double()
+    out.update({"recons_per_s": jobs / wall, "wall_s": wall,
+                "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+                "max_concurrent": st["max_concurrent"],
+                "rel_l2_job0_vs_f32_recon": float((r0 - ref).norm() / ref.norm()),
+                "failed": st["failed"]})
+    return out
 
 
 def main_reference(args, rank, world):

@@ -172,14 +172,15 @@ size_t back_partial_bytes(const BackShape &s, long long P, int band) {
 template <int CP, int SPL, int NT, typename RD>
 int launch_back_t(const Geo &geo, const mbir_geometry *g, const float *vp, int v_start,
                   int v_count, const BackShape &s, const RD &rd, const int64_t *pix, long long P,
-                  int slice_start, int band, float *dst, cudaStream_t st, const char *what) {
+                  int slice_start, int band, float *dst, cudaStream_t st, const char *what,
+                  const ConeFwdRec *recs) {
   dim3 grid(s.blocks_x, s.nchunks);
   if (g->geometry == MBIR_CONE) {
     auto k = back_cone_kernel<CP, SPL, NT, RD>;
     if (s.smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     tpre(st);
     k<<<grid, kThreads, s.smem, st>>>(geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P,
-                                      slice_start, band, s.slice_chunks, dst);
+                                      slice_start, band, s.slice_chunks, dst, recs);
   } else {
     tpre(st);
     back_parallel_kernel<CP, SPL, NT, RD><<<grid, kThreads, 0, st>>>(
@@ -193,9 +194,9 @@ template <int CP, int NT, typename RD>
 int launch_back_spl(const Geo &geo, const mbir_geometry *g, const float *vp, int v_start,
                     int v_count, const BackShape &s, const RD &rd, const int64_t *pix,
                     long long P, int slice_start, int band, float *dst, cudaStream_t st,
-                    const char *what) {
+                    const char *what, const ConeFwdRec *recs) {
 #define MBIR_BACK(SPLV) \
-  launch_back_t<CP, SPLV, NT>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what)
+  launch_back_t<CP, SPLV, NT>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what, recs)
   if (g->geometry == MBIR_CONE) {
     switch (s.SPL) {
       case 1: return MBIR_BACK(1);
@@ -212,23 +213,26 @@ template <int CP, typename RD>
 int launch_back_nt(const Geo &geo, const mbir_geometry *g, const float *vp, int v_start,
                    int v_count, const BackShape &s, const RD &rd, const int64_t *pix,
                    long long P, int slice_start, int band, float *dst, cudaStream_t st,
-                   const char *what) {
+                   const char *what, const ConeFwdRec *recs) {
   if (g->psf_radius == 1)
-    return launch_back_spl<CP, 3>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
-  return launch_back_spl<CP, 0>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
+    return launch_back_spl<CP, 3>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what, recs);
+  return launch_back_spl<CP, 0>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what, nullptr);
 }
 
 // Back projection with a given reader into `out` (or chunk partials in
-// `partials` followed by the fixed-order reduction).
+// `partials` followed by the fixed-order reduction).  `recs` (cone, psf
+// radius 1, coefficient power 1 only): the subset's per-(view, slot)
+// records from cone_bin_kernel for views [v_start, v_start + v_count),
+// loaded instead of re-formed.
 template <typename RD>
 int run_back(const mbir_geometry *g, const float *vp, int v_start, int v_count, const RD &rd,
              const int64_t *pix, long long P, int cp, int slice_start, int band, float *out,
              const BackShape &s, float *partials, cudaStream_t st, bool reduce_into_out,
-             const char *what = "back projection") {
+             const char *what = "back projection", const ConeFwdRec *recs = nullptr) {
   const Geo geo = make_geo(*g);
   float *dst = s.nchunks > 1 ? partials : out;
-  int rc = cp == 2 ? launch_back_nt<2>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what)
-                   : launch_back_nt<1>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what);
+  int rc = cp == 2 ? launch_back_nt<2>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what, nullptr)
+                   : launch_back_nt<1>(geo, g, vp, v_start, v_count, s, rd, pix, P, slice_start, band, dst, st, what, recs);
   if (rc) return rc;
   if (s.nchunks > 1 && reduce_into_out) {
     const size_t n = (size_t)P * band;
@@ -287,7 +291,8 @@ int cone_rt_threads(const mbir_geometry *g) { return (g->num_det_rows + 31) / 32
 
 size_t cone_rt_smem(const mbir_geometry *g, int band) {
   const int nthr = cone_rt_threads(g);
-  return sizeof(float) * ((size_t)kFwdEB * (band + 2 * kFwdVPad) + (size_t)fwd_cap(nthr) * kFwdRec);
+  return sizeof(ConeFwdRec) * (size_t)fwd_cap(nthr) +
+         sizeof(float) * (size_t)kFwdEB * (band + 2 * kFwdVPad);
 }
 
 template <typename EPI>
@@ -309,6 +314,90 @@ int launch_cone_rt(const mbir_geometry *g, const float *vp, int v_start, int v_c
   k<<<grid, cone_rt_threads(g), smem, st>>>(geo, vp, v_start, values, (int)P, band, slice_start,
                                              pix, by_pixel, epi);
   MBIR_CHECK_LAUNCH(what);
+  return MBIR_OK;
+}
+
+// ── binned cone forward (a subset projected by several launches) ───────────
+constexpr size_t kBinBytes = (size_t)128 << 20;  // record + list bytes per view chunk
+
+int fwd_nblk(const mbir_geometry *g) { return (g->num_det_channels + kFwdCB - 1) / kFwdCB; }
+
+// Views per binning chunk for a subset of P pixels.
+int bin_views(const mbir_geometry *g, long long P) {
+  const size_t per_view = (size_t)P * (sizeof(ConeFwdRec) + 2 * sizeof(int)) +
+                          (size_t)(fwd_nblk(g) + 1) * sizeof(int);
+  return (int)std::max<size_t>(1, std::min<size_t>(g->num_views, kBinBytes / per_view));
+}
+
+struct FwdBins {
+  ConeFwdRec *recs;
+  int *list, *offs;
+  unsigned char *touched;  // (V, nblk): the tile received a pixel (all views)
+  int views;               // views per chunk
+};
+
+size_t bin_smem(const mbir_geometry *g) {
+  return sizeof(int) * (size_t)fwd_nblk(g) * (1 + 2 * (kThreads / 32));
+}
+
+int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count,
+               const int64_t *pix, long long P, const FwdBins &b, cudaStream_t st) {
+  const Geo geo = make_geo(*g);
+  const size_t smem = bin_smem(g);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(cone_bin_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+      return fail(MBIR_ERR_CUDA, "forward binning: shared memory request of %zu bytes refused: %s",
+                  smem, cudaGetErrorString(e));
+  }
+  tpre(st);
+  cone_bin_kernel<<<v_count, kThreads, smem, st>>>(geo, vp, v_start, pix, (int)P, 0, fwd_nblk(g),
+                                                   b.recs, b.list, b.offs);
+  MBIR_CHECK_LAUNCH("vcd forward binning");
+  return MBIR_OK;
+}
+
+template <typename EPI>
+int launch_binned(const mbir_geometry *g, int v_start, int v_count, const float *values,
+                  long long P, int band, const FwdBins &b, const EPI &epi, cudaStream_t st,
+                  const char *what) {
+  const Geo geo = make_geo(*g);
+  const size_t smem = cone_rt_smem(g, band);
+  auto k = forward_cone_binned_kernel<EPI>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+      return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s", smem,
+                  cudaGetErrorString(e));
+  }
+  dim3 grid(fwd_nblk(g), v_count);
+  tpre(st);
+  k<<<grid, cone_rt_threads(g), smem, st>>>(geo, v_start, values, (int)P, band, 0, b.recs,
+                                             b.list, b.offs, b.touched, epi);
+  MBIR_CHECK_LAUNCH(what);
+  return MBIR_OK;
+}
+
+// Forward of a (P, band) subset array over all views through the bins: per
+// view chunk, bin (when `bin`) and project.  With a single chunk the bins
+// outlive the call, so a later projection of the same subset passes
+// bin = false.
+template <typename EPI>
+int run_forward_binned(const mbir_geometry *g, const float *vp, const float *values,
+                       long long P, int band, const int64_t *pix, const FwdBins &b, bool bin,
+                       const EPI &epi, cudaStream_t st, const char *what) {
+  const int V = g->num_views;
+  for (int v0 = 0; v0 < V; v0 += b.views) {
+    const int nv = std::min(b.views, V - v0);
+    int rc;
+    if (bin || b.views < V) {
+      rc = launch_bin(g, vp, v0, nv, pix, P, b, st);
+      if (rc) return rc;
+    }
+    rc = launch_binned(g, v0, nv, values, P, band, b, epi, st, what);
+    if (rc) return rc;
+  }
   return MBIR_OK;
 }
 
@@ -340,13 +429,15 @@ struct VcdWs {
   float *grad_part, *delta, *gbuf, *hinv, *gpbuf, *hpbuf, *alpha;
   double *dc_sums, *prior_part, *fwd_part, *sq_part, *l1_part;
   void *ad;
+  FwdBins bins;  // binned cone forward (used when `binned`)
   BackShape bs;
   int dc_chunks, prior_blocks, fwd_blocks, upd_chunks, upd_yblocks;
+  bool binned;
   size_t bytes;
 };
 
-constexpr int kUpdChunk = 32;   // pixels per update tile
-constexpr int kDcChunk = 256;   // pixels per DC-sum chunk
+constexpr int kUpdChunk = 16;   // pixels per update tile (two load batches)
+constexpr int kDcChunk = 32;    // pixels per DC-sum chunk
 
 size_t storage_size(int storage) { return storage == MBIR_F32 ? 4 : 2; }
 
@@ -374,6 +465,16 @@ VcdWs vcd_layout(const mbir_geometry *g, long long Ps, const mbir_vcd_params *pr
   w.l1_part = c.take<double>((size_t)w.upd_chunks * w.upd_yblocks);
   w.alpha = c.take<float>(4);
   w.ad = c.take<char>((size_t)V * g->num_det_channels * g->num_det_rows * storage_size(prm->storage));
+  w.binned = use_cone_rt(g);
+  w.bins = FwdBins{nullptr, nullptr, nullptr, nullptr, 0};
+  if (w.binned) {
+    const int vc = bin_views(g, Ps);
+    w.bins.views = vc;
+    w.bins.recs = c.take<ConeFwdRec>((size_t)vc * Ps);
+    w.bins.list = c.take<int>((size_t)vc * 2 * Ps);
+    w.bins.offs = c.take<int>((size_t)vc * (fwd_nblk(g) + 1));
+    w.bins.touched = c.take<unsigned char>((size_t)V * fwd_nblk(g));
+  }
   w.bytes = c.used;
   return w;
 }
@@ -388,15 +489,23 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   const VcdScalars sc = make_scalars(*prm);
   const bool DCon = dc != nullptr;
   int rc;
+  // 0. the subset's (view, pixel) records, binned by channel block; when one
+  //    chunk holds every view the gradient reads them too.
+  const bool shared_bins = w.binned && w.bins.views >= V && g->psf_radius == 1;
+  if (shared_bins) {
+    rc = launch_bin(g, vp, 0, V, pix, Ps, w.bins, st);
+    if (rc) return rc;
+  }
+  const ConeFwdRec *recs = shared_bins ? w.bins.recs : nullptr;
   // 1. gradient partials of A^T (w e), one slab per view chunk
   if (wts) {
     ReadWeighted<T> rd{err, es, wts, wsc, C, R};
     rc = run_back(g, vp, 0, V, rd, pix, Ps, 1, 0, S, w.grad_part, w.bs, w.grad_part, st, false,
-                  "vcd gradient (back projection)");
+                  "vcd gradient (back projection)", recs);
   } else {
     ReadScaled<T> rd{err, es, C, R};
     rc = run_back(g, vp, 0, V, rd, pix, Ps, 1, 0, S, w.grad_part, w.bs, w.grad_part, st, false,
-                  "vcd gradient (back projection)");
+                  "vcd gradient (back projection)", recs);
   }
   if (rc) return rc;
   // 2. direction (reduces the chunk slabs in order)
@@ -425,12 +534,15 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   }
   // 3. forward A delta + line-search partials
   LineSearchEpi<T> epi{err, es, wts, wsc, static_cast<T *>(w.ad), C, R, w.fwd_part, 1, 0.0, 0.0};
-  rc = run_forward(g, vp, 0, V, w.delta, Ps, S, 0, pix, epi, st,
-                   "vcd forward + line search");
+  if (w.binned)
+    rc = run_forward_binned(g, vp, w.delta, Ps, S, pix, w.bins, !shared_bins, epi, st,
+                            "vcd forward + line search");
+  else
+    rc = run_forward(g, vp, 0, V, w.delta, Ps, S, 0, pix, epi, st, "vcd forward + line search");
   if (rc) return rc;
   // 4. alpha
   tpre(st);
-  vcd_alpha_kernel<<<1, kThreads, 0, st>>>(w.prior_part, nb, w.fwd_part, w.fwd_blocks, sc.fmc,
+  vcd_alpha_kernel<<<1, kAlphaThreads, 0, st>>>(w.prior_part, nb, w.fwd_part, w.fwd_blocks, sc.fmc,
                                            sc.max_alpha, w.alpha, alpha_user);
   MBIR_CHECK_LAUNCH("vcd alpha");
   if (prm->positivity) {
@@ -439,7 +551,11 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
                                                                         w.alpha, w.delta);
     MBIR_CHECK_LAUNCH("vcd positivity");
     LineSearchEpi<T> epi2{err, es, wts, wsc, static_cast<T *>(w.ad), C, R, nullptr, 0, 0.0, 0.0};
-    rc = run_forward(g, vp, 0, V, w.delta, Ps, S, 0, pix, epi2, st, "vcd forward (positivity)");
+    if (w.binned)
+      rc = run_forward_binned(g, vp, w.delta, Ps, S, pix, w.bins, false, epi2, st,
+                              "vcd forward (positivity)");
+    else
+      rc = run_forward(g, vp, 0, V, w.delta, Ps, S, 0, pix, epi2, st, "vcd forward (positivity)");
     if (rc) return rc;
   }
   // 5. update
@@ -452,6 +568,16 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   vcd_finish_kernel<<<1, kThreads, 0, st>>>(S, w.upd_chunks, w.upd_chunks * w.upd_yblocks,
                                             w.sq_part, w.l1_part, w.alpha, accum);
   MBIR_CHECK_LAUNCH("vcd finish");
+  if (w.binned) {
+    // Only the (view, channel-block) tiles the subset reached: elsewhere
+    // A delta is zero and e is unchanged.
+    const int nblk = fwd_nblk(g);
+    tpre(st);
+    vcd_sino_update_tiles_kernel<T><<<dim3(nblk, V), 256, 0, st>>>(
+        C, R, kFwdCB, w.bins.touched, w.alpha, err, static_cast<const T *>(w.ad));
+    MBIR_CHECK_LAUNCH("vcd sinogram update");
+    return MBIR_OK;
+  }
   const size_t n = (size_t)V * C * R;
   const int blocks = (int)std::min<size_t>((n / 4 + 255) / 256 + 1, 148 * 32);
   tpre(st);

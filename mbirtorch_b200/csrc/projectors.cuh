@@ -89,6 +89,15 @@ struct ConeRec {
   float m0, w_r, hw1r, lmaxr, a0, a1;
 };
 
+// One cone (view, pixel) at psf radius 1, formed once per subset by
+// cone_bin_kernel and read by the register-tiled forward (packed for 16-byte
+// shared loads) and by the VCD gradient's back projection.
+struct __align__(16) ConeFwdRec {
+  float4 a;  // m0, w_r, (w_r + 1) / 2, min(w_r, 1)         (vertical fan)
+  float4 b;  // 1 / w_r, tap weights at centre - 1, centre, centre + 1
+  float4 c;  // a0, a1 (t(k) = a0 + a1 k), centre channel, value row (int bits)
+};
+
 // ── back projection: parallel ─────────────────────────────────────────────
 template <int CP, int SPL, int NT, typename RD>
 __global__ void __launch_bounds__(kThreads)
@@ -175,7 +184,8 @@ template <int CP, int SPL, int NT, typename RD>
 __global__ void __launch_bounds__(kThreads)
 back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc, RD rd,
                  const int64_t *__restrict__ pix, int P, int slice_start, int band,
-                 int slice_chunks, float *__restrict__ out) {
+                 int slice_chunks, float *__restrict__ out,
+                 const ConeFwdRec *__restrict__ recs) {
   extern __shared__ float smem[];
   constexpr int MT = MBIR_TAPS(NT);
   const int RT = NT ? (NT - 1) / 2 : g.psf, nt = 2 * RT + 1;
@@ -207,7 +217,22 @@ back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, 
   for (int vg = vb; vg < ve; vg += 32) {
     const int nv = min(32, ve - vg);
     __syncwarp();
-    if (lane < nv) {
+    if (CP == 1 && MT == 3 && recs != nullptr && lane < nv) {
+      // The same values cone_bin_kernel formed for this (view, slot).
+      const ConeFwdRec fr = recs[(size_t)(vg + lane) * P + p];
+      ConeRec r;
+      r.ctr = __float_as_int(fr.c.z);
+      r.w[0] = fr.b.y;
+      r.w[1] = fr.b.z;
+      r.w[2] = fr.b.w;
+      r.m0 = fr.a.x;
+      r.w_r = fr.a.y;
+      r.hw1r = fr.a.z;
+      r.lmaxr = fr.a.w;
+      r.a0 = fr.c.x;
+      r.a1 = fr.c.y;
+      tab[lane] = r;
+    } else if (lane < nv) {
       const int gv = v_start + vg + lane;
       const float ang = vp[2 * gv];
       const float z_off = __fsub_rn(g.rso, vp[2 * gv + 1]);
@@ -247,13 +272,30 @@ back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, 
       const float lo = fmaxf(floorf(fminf(ma, mb)) - (float)(RT + 1), 0.f);
       const float hi = fminf(ceilf(fmaxf(ma, mb)) + (float)(RT + 1), (float)(g.R - 1));
       if (lo <= hi) {
+        // Column rows in batches of HB per lane, every load of a batch in
+        // flight before the first use.
+        constexpr int HB = NT == 3 ? 8 : 2;
         const int m_lo = (int)lo, m_hi = (int)hi;
-        for (int m = m_lo + lane; m <= m_hi; m += 32) {
-          float s = 0.f;
+        for (int mb = m_lo + lane; mb <= m_hi; mb += 32 * HB) {
+          float col[HB][MT];
 #pragma unroll
-          for (int t = 0; t < MT; ++t)
-            if (MBIR_TAP_ON(NT, t, nt)) s = fmaf(w[t], rd.get(base[t] + m), s);
-          h[m] = __fmul_rn(s, scl);
+          for (int u = 0; u < HB; ++u) {
+            const int m = mb + 32 * u;
+#pragma unroll
+            for (int t = 0; t < MT; ++t)
+              col[u][t] = (MBIR_TAP_ON(NT, t, nt) && m <= m_hi) ? rd.get(base[t] + m) : 0.f;
+          }
+#pragma unroll
+          for (int u = 0; u < HB; ++u) {
+            const int m = mb + 32 * u;
+            if (m <= m_hi) {
+              float s = 0.f;
+#pragma unroll
+              for (int t = 0; t < MT; ++t)
+                if (MBIR_TAP_ON(NT, t, nt)) s = fmaf(w[t], col[u][t], s);
+              h[m] = __fmul_rn(s, scl);
+            }
+          }
         }
       }
       __syncwarp();
@@ -323,12 +365,18 @@ struct StoreSino {
   float *out;
   int layout, C, R;
   __device__ __forceinline__ bool channel_fastest() const { return layout == MBIR_LAYOUT_VRC; }
-  __device__ __forceinline__ void begin() {}
+  __device__ __forceinline__ void begin(int) {}
   __device__ __forceinline__ void cell(int v, int c, int m, float val) {
     if (layout == MBIR_LAYOUT_VCR)
       out[((size_t)v * C + c) * R + m] = val;
     else
       out[((size_t)v * R + m) * C + c] = val;
+  }
+  template <int N>
+  __device__ __forceinline__ void cells(int v, int c0, int ncb, int m, const float (&acc)[N]) {
+#pragma unroll
+    for (int j = 0; j < N; ++j)
+      if (j < ncb) cell(v, c0 + j, m, acc[j]);
   }
   __device__ __forceinline__ void end(int) {}
 };
@@ -482,7 +530,7 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
   }
   __syncthreads();
   // Epilogue: sum the groups' tiles in group order and hand each cell over.
-  epi.begin();
+  epi.begin(vl);
   const int cells = ncb * rows;
   if (epi.channel_fastest()) {
     for (int i = tid; i < cells; i += kThreads) {
@@ -518,10 +566,36 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
 constexpr int kFwdCB = 16;   // channels per CTA
 constexpr int kFwdEB = 16;   // pixels staged per batch
 constexpr int kFwdVPad = 8;  // zero slices either side of a staged cylinder (>= 2 bp + 1)
-constexpr int kFwdRec = 12;  // record words per pixel
 
 // Record capacity of one compaction round: at least one scan chunk.
 __host__ __device__ inline int fwd_cap(int nthr) { return nthr > 512 ? nthr : 512; }
+
+__device__ __forceinline__ ConeFwdRec cone_fwd_record(const Geo &g, float ang, float z_off,
+                                                      const ConeCenter &cc, int row) {
+  const ConeVP q = cone_finish(g, ang, z_off, cc);
+  float a0, a1;
+  cone_tcoef(g, q.mag, z_off, a0, a1);
+  ConeFwdRec r;
+  r.a = make_float4(q.m0, q.w_r, __fdiv_rn(__fadd_rn(q.w_r, 1.f), 2.f), fminf(q.w_r, 1.f));
+  r.b = make_float4(1.f / q.w_r,
+                    tap_weight(cc.n_p, cc.ctr - 1, q.half_w1, q.lmax, q.ws, g.C),
+                    tap_weight(cc.n_p, cc.ctr, q.half_w1, q.lmax, q.ws, g.C),
+                    tap_weight(cc.n_p, cc.ctr + 1, q.half_w1, q.lmax, q.ws, g.C));
+  r.c = make_float4(a0, a1, __int_as_float(cc.ctr), __int_as_float(row));
+  return r;
+}
+
+// Channel blocks [b_lo, b_hi] reached by a pixel whose taps are the
+// channels ctr - 1 .. ctr + 1 clipped to the detector (-1 when none).
+__device__ __forceinline__ void fwd_block_range(int ctr, int C, int &b_lo, int &b_hi) {
+  const int lo = max(ctr - 1, 0), hi = min(ctr + 1, C - 1);
+  if (lo > hi) {
+    b_lo = b_hi = -1;
+  } else {
+    b_lo = lo / kFwdCB;
+    b_hi = hi / kFwdCB;
+  }
+}
 
 template <int J>
 __device__ __forceinline__ void fwd_taps(float (&acc)[kFwdCB], float w0, float w1, float w2,
@@ -536,19 +610,109 @@ __device__ __forceinline__ void fwd_taps(float (&acc)[kFwdCB], float w0, float w
       fmaf(w2, det, acc[(J >= 0 && J < kFwdCB) ? J : 0]);
 }
 
+// The batches of one round: n records in shared memory, processed kFwdEB at
+// a time.  Staging writes the batch's cylinders, scaled by 1 / cos(phi) per
+// slice, into the zero-padded stage; then thread m forms detector row m's
+// vertical fan for every pixel of the batch and adds its three channel taps.
+// Every batch ends with all threads past a barrier.
+__device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec, int n, int c0,
+                                             float *__restrict__ stage, int SP,
+                                             const float *__restrict__ values, int band,
+                                             int slice_start, float kc_lo, float kc_hi, int bp,
+                                             int R, float (&acc)[kFwdCB]) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const float mf = (float)tid;
+  for (int b0 = 0; b0 < n; b0 += kFwdEB) {
+    const int nb = min(kFwdEB, n - b0);
+    if (2 * band >= nthr) {
+      // slice-major: thread t stages slice t (+ nthr ...) of every pixel of
+      // the batch, with all kFwdEB loads in flight before the first use.
+      for (int k = tid; k < band; k += nthr) {
+        float val[kFwdEB];
+#pragma unroll
+        for (int e = 0; e < kFwdEB; ++e)
+          val[e] = e < nb ? __ldg(values + (size_t)__float_as_int(rec[b0 + e].c.w) * band + k)
+                          : 0.f;
+        const float kf = (float)(slice_start + k);
+#pragma unroll
+        for (int e = 0; e < kFwdEB; ++e) {
+          if (e < nb) {
+            const float4 c = rec[b0 + e].c;
+            stage[e * SP + kFwdVPad + k] = val[e] * inv_cos_from_t(fmaf(c.y, kf, c.x));
+          }
+        }
+      }
+    } else {
+      for (int i = tid; i < nb * band; i += nthr) {
+        const int e = i / band, k = i - e * band;
+        const float4 c = rec[b0 + e].c;
+        stage[e * SP + kFwdVPad + k] =
+            __ldg(values + (size_t)__float_as_int(c.w) * band + k) *
+            inv_cos_from_t(fmaf(c.y, (float)(slice_start + k), c.x));
+      }
+    }
+    __syncthreads();
+    if (tid < R) {
+      for (int e = 0; e < nb; ++e) {
+        const ConeFwdRec *r = rec + b0 + e;
+        const float4 ra = r->a, rb = r->b;
+        const int j = __float_as_int(r->c.z) - c0 + 1;  // in [0, kFwdCB + 1]
+        const float m0 = ra.x, w_r = ra.y, hw1r = ra.z, lmaxr = ra.w;
+        const float k_m = (mf - m0) * rb.x;
+        const float kc = fminf(fmaxf(rintf(k_m), kc_lo), kc_hi);
+        const float d = w_r * (kc - k_m);
+        const float *st = stage + e * SP + kFwdVPad + ((int)kc - slice_start);
+        float det;
+        if (bp == 1) {
+          const float am = fminf(fmaxf(hw1r - fabsf(d - w_r), 0.f), lmaxr);
+          const float a0 = fminf(fmaxf(hw1r - fabsf(d), 0.f), lmaxr);
+          const float ap = fminf(fmaxf(hw1r - fabsf(d + w_r), 0.f), lmaxr);
+          det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
+        } else {
+          det = 0.f;
+          for (int ko = -bp; ko <= bp; ++ko) {
+            const float a = fminf(fmaxf(hw1r - fabsf(fmaf(w_r, (float)ko, d)), 0.f), lmaxr);
+            det = fmaf(a, st[ko], det);
+          }
+        }
+        const float w0 = rb.y, w1 = rb.z, w2 = rb.w;
+        switch (j) {
+          case 0: fwd_taps<0>(acc, w0, w1, w2, det); break;
+          case 1: fwd_taps<1>(acc, w0, w1, w2, det); break;
+          case 2: fwd_taps<2>(acc, w0, w1, w2, det); break;
+          case 3: fwd_taps<3>(acc, w0, w1, w2, det); break;
+          case 4: fwd_taps<4>(acc, w0, w1, w2, det); break;
+          case 5: fwd_taps<5>(acc, w0, w1, w2, det); break;
+          case 6: fwd_taps<6>(acc, w0, w1, w2, det); break;
+          case 7: fwd_taps<7>(acc, w0, w1, w2, det); break;
+          case 8: fwd_taps<8>(acc, w0, w1, w2, det); break;
+          case 9: fwd_taps<9>(acc, w0, w1, w2, det); break;
+          case 10: fwd_taps<10>(acc, w0, w1, w2, det); break;
+          case 11: fwd_taps<11>(acc, w0, w1, w2, det); break;
+          case 12: fwd_taps<12>(acc, w0, w1, w2, det); break;
+          case 13: fwd_taps<13>(acc, w0, w1, w2, det); break;
+          case 14: fwd_taps<14>(acc, w0, w1, w2, det); break;
+          case 15: fwd_taps<15>(acc, w0, w1, w2, det); break;
+          case 16: fwd_taps<16>(acc, w0, w1, w2, det); break;
+          default: fwd_taps<17>(acc, w0, w1, w2, det); break;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <typename EPI>
 __global__ void __launch_bounds__(1024)
 forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
                        const float *__restrict__ values, int P, int band, int slice_start,
                        const int64_t *__restrict__ pix, int by_pixel, EPI epi) {
-  extern __shared__ float sm[];
+  extern __shared__ float4 sm4[];
   const int nthr = blockDim.x;
-  const int kFwdCap = fwd_cap(nthr);
-  const int SP = band + 2 * kFwdVPad;                 // staged cylinder pitch
-  float *stage = sm;                                  // kFwdEB x SP
-  int *r_ctr = (int *)(stage + kFwdEB * SP);          // kFwdCap
-  int *r_row = r_ctr + kFwdCap;                       // kFwdCap
-  float *r_f = (float *)(r_row + kFwdCap);            // 10 x kFwdCap
+  const int cap = fwd_cap(nthr);
+  const int SP = band + 2 * kFwdVPad;                     // staged cylinder pitch
+  ConeFwdRec *rec = reinterpret_cast<ConeFwdRec *>(sm4);  // cap records
+  float *stage = reinterpret_cast<float *>(rec + cap);    // kFwdEB x SP
   __shared__ int s_wcount[32];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
@@ -559,15 +723,12 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
   const float ang = vp[2 * v];
   const float cs = cosf(ang), sn = sinf(ang);
   const float z_off = __fsub_rn(g.rso, vp[2 * v + 1]);
-  const int m = tid;
-  const float mf = (float)m;
   const int bp = g.bp;
   // Clamp of the centre slice: a centre outside [ss - bp - 1, ss + band + bp]
   // has no tap inside the band, and the clamped one only meets zero padding
   // (kFwdVPad >= 2 bp + 1).
   const float kc_lo = (float)(slice_start - bp - 1),
               kc_hi = (float)(slice_start + band + bp);
-  const int R = g.R;
 
   for (int i = tid; i < kFwdEB * SP; i += nthr) stage[i] = 0.f;
   float acc[kFwdCB];
@@ -578,7 +739,7 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
   while (pos < P) {
     int n = 0;
     __syncthreads();
-    while (pos < P && n + nthr <= kFwdCap) {
+    while (pos < P && n + nthr <= cap) {
       const int p = pos + tid;
       bool keep = false;
       ConeCenter cc;
@@ -597,97 +758,161 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
         if (w < warp) off += c;
         tot += c;
       }
-      if (keep) {
-        const int s = off + __popc(bal & ((1u << lane) - 1u));
-        const ConeVP q = cone_finish(g, ang, z_off, cc);
-        float a0, a1;
-        cone_tcoef(g, q.mag, z_off, a0, a1);
-        r_ctr[s] = cc.ctr - c0 + 1;  // switch case: centre channel + 1, in [0, kFwdCB + 1]
-        r_row[s] = by_pixel ? (int)pix[p] : p;
-        r_f[0 * kFwdCap + s] = tap_weight(cc.n_p, cc.ctr - 1, q.half_w1, q.lmax, q.ws, g.C);
-        r_f[1 * kFwdCap + s] = tap_weight(cc.n_p, cc.ctr, q.half_w1, q.lmax, q.ws, g.C);
-        r_f[2 * kFwdCap + s] = tap_weight(cc.n_p, cc.ctr + 1, q.half_w1, q.lmax, q.ws, g.C);
-        r_f[3 * kFwdCap + s] = q.m0;
-        r_f[4 * kFwdCap + s] = q.w_r;
-        r_f[5 * kFwdCap + s] = __fdiv_rn(__fadd_rn(q.w_r, 1.f), 2.f);
-        r_f[6 * kFwdCap + s] = fminf(q.w_r, 1.f);
-        r_f[7 * kFwdCap + s] = 1.f / q.w_r;
-        r_f[8 * kFwdCap + s] = a0;
-        r_f[9 * kFwdCap + s] = a1;
-      }
+      if (keep)
+        rec[off + __popc(bal & ((1u << lane) - 1u))] =
+            cone_fwd_record(g, ang, z_off, cc, by_pixel ? (int)pix[p] : p);
       n += tot;
       pos += nthr;
       __syncthreads();
     }
-    for (int b0 = 0; b0 < n; b0 += kFwdEB) {
-      const int nb = min(kFwdEB, n - b0);
-      // Stage the batch's scaled cylinders.
-      for (int i = tid; i < nb * band; i += nthr) {
-        const int e = i / band, k = i - e * band;
-        const int r = b0 + e;
-        const float tk = fmaf(r_f[9 * kFwdCap + r], (float)(slice_start + k), r_f[8 * kFwdCap + r]);
-        stage[e * SP + kFwdVPad + k] =
-            __ldg(values + (size_t)r_row[r] * band + k) * inv_cos_from_t(tk);
-      }
-      __syncthreads();
-      if (m < R) {
-        for (int e = 0; e < nb; ++e) {
-          const int r = b0 + e;
-          const float m0 = r_f[3 * kFwdCap + r], w_r = r_f[4 * kFwdCap + r];
-          const float hw1r = r_f[5 * kFwdCap + r], lmaxr = r_f[6 * kFwdCap + r];
-          const float inv_wr = r_f[7 * kFwdCap + r];
-          const float k_m = (mf - m0) * inv_wr;
-          const float kc = fminf(fmaxf(rintf(k_m), kc_lo), kc_hi);
-          const float d = w_r * (kc - k_m);
-          const float *st = stage + e * SP + kFwdVPad + ((int)kc - slice_start);
-          float det;
-          if (bp == 1) {
-            const float am = fminf(fmaxf(hw1r - fabsf(d - w_r), 0.f), lmaxr);
-            const float a0 = fminf(fmaxf(hw1r - fabsf(d), 0.f), lmaxr);
-            const float ap = fminf(fmaxf(hw1r - fabsf(d + w_r), 0.f), lmaxr);
-            det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
-          } else {
-            det = 0.f;
-            for (int ko = -bp; ko <= bp; ++ko) {
-              const float a = fminf(fmaxf(hw1r - fabsf(fmaf(w_r, (float)ko, d)), 0.f), lmaxr);
-              det = fmaf(a, st[ko], det);
-            }
-          }
-          const float w0 = r_f[0 * kFwdCap + r], w1 = r_f[1 * kFwdCap + r];
-          const float w2 = r_f[2 * kFwdCap + r];
-          switch (r_ctr[r]) {
-            case 0: fwd_taps<0>(acc, w0, w1, w2, det); break;
-            case 1: fwd_taps<1>(acc, w0, w1, w2, det); break;
-            case 2: fwd_taps<2>(acc, w0, w1, w2, det); break;
-            case 3: fwd_taps<3>(acc, w0, w1, w2, det); break;
-            case 4: fwd_taps<4>(acc, w0, w1, w2, det); break;
-            case 5: fwd_taps<5>(acc, w0, w1, w2, det); break;
-            case 6: fwd_taps<6>(acc, w0, w1, w2, det); break;
-            case 7: fwd_taps<7>(acc, w0, w1, w2, det); break;
-            case 8: fwd_taps<8>(acc, w0, w1, w2, det); break;
-            case 9: fwd_taps<9>(acc, w0, w1, w2, det); break;
-            case 10: fwd_taps<10>(acc, w0, w1, w2, det); break;
-            case 11: fwd_taps<11>(acc, w0, w1, w2, det); break;
-            case 12: fwd_taps<12>(acc, w0, w1, w2, det); break;
-            case 13: fwd_taps<13>(acc, w0, w1, w2, det); break;
-            case 14: fwd_taps<14>(acc, w0, w1, w2, det); break;
-            case 15: fwd_taps<15>(acc, w0, w1, w2, det); break;
-            case 16: fwd_taps<16>(acc, w0, w1, w2, det); break;
-            default: fwd_taps<17>(acc, w0, w1, w2, det); break;
-          }
-        }
-      }
-      __syncthreads();
-    }
+    fwd_rt_round(rec, n, c0, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, acc);
   }
-  // Epilogue: thread m hands over its row's cells, channel by channel.
-  epi.begin();
-  if (m < R) {
-#pragma unroll
-    for (int j = 0; j < kFwdCB; ++j)
-      if (j < ncb) epi.cell(vl, c0 + j, m, acc[j]);
-  }
+  // Epilogue: thread m hands over its row's cells.
+  epi.begin(vl);
+  if (tid < g.R) epi.cells(vl, c0, ncb, tid, acc);
   epi.end(blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// ── forward projection, cone, binned ───────────────────────────────────────
+// For a pixel subset that several launches use (the VCD gradient, forward
+// and positivity re-projection), the (view, pixel) records are formed once by
+// cone_bin_kernel and bucketed by channel block, so that each forward CTA
+// reads exactly its pixels instead of scanning the subset and re-forming
+// every pixel's geometry (atan2, sin/cos, divisions) in each of the
+// C / kFwdCB blocks of a view.
+//
+// cone_bin_kernel: one CTA per view of the chunk [v_start, v_start + gridDim.x).
+//   recs[vl * P + p]                 record of subset slot p
+//   list[vl * 2P + ...]              slots per channel block, in increasing slot order
+//   offs[vl * (nblk + 1) + b .. b + 1]   block b's range of list
+// Slots are placed by a deterministic prefix over (chunk, warp, tap side,
+// lane): no atomics decide an order.
+__global__ void __launch_bounds__(256)
+cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
+                const int64_t *__restrict__ pix, int P, int by_pixel, int nblk,
+                ConeFwdRec *__restrict__ recs, int *__restrict__ list, int *__restrict__ offs) {
+  extern __shared__ int bsm[];
+  const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nvw = 2 * (nthr >> 5);  // virtual warps: (warp, tap side)
+  int *cursor = bsm;                // nblk
+  int *wc = bsm + nblk;             // nvw x nblk
+  const int vl = blockIdx.x, v = v_start + vl;
+  const float ang = vp[2 * v];
+  const float cs = cosf(ang), sn = sinf(ang);
+  const float z_off = __fsub_rn(g.rso, vp[2 * v + 1]);
+  ConeFwdRec *vrec = recs + (size_t)vl * P;
+  int *vlist = list + (size_t)vl * 2 * P;
+  int *voffs = offs + (size_t)vl * (nblk + 1);
+
+  for (int b = tid; b < nblk; b += nthr) cursor[b] = 0;
+  __syncthreads();
+  // Pass 1: records and per-block counts (the counts do not depend on the
+  // order of the shared-memory increments).
+  for (int p = tid; p < P; p += nthr) {
+    float xt, yt;
+    pixel_xy(g, (int)pix[p], xt, yt);
+    const ConeCenter cc = cone_center(g, cs, sn, xt, yt);
+    vrec[p] = cone_fwd_record(g, ang, z_off, cc, by_pixel ? (int)pix[p] : p);
+    int b_lo, b_hi;
+    fwd_block_range(cc.ctr, g.C, b_lo, b_hi);
+    if (b_lo >= 0) atomicAdd(&cursor[b_lo], 1);
+    if (b_hi > b_lo) atomicAdd(&cursor[b_hi], 1);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int s = 0;
+    for (int b = 0; b < nblk; ++b) {
+      const int c = cursor[b];
+      cursor[b] = s;
+      voffs[b] = s;
+      s += c;
+    }
+    voffs[nblk] = s;
+  }
+  __syncthreads();
+  // Pass 2: stable placement, one chunk of nthr slots at a time (a thread
+  // reads back the records it wrote itself in pass 1).
+  const unsigned lt = (1u << lane) - 1u;
+  for (int base = 0; base < P; base += nthr) {
+    const int p = base + tid;
+    int b0 = -1, b1 = -1;
+    if (p < P) {
+      fwd_block_range(__float_as_int(vrec[p].c.z), g.C, b0, b1);
+      if (b1 == b0) b1 = -1;
+    }
+    for (int i = tid; i < nvw * nblk; i += nthr) wc[i] = 0;
+    __syncthreads();
+    const unsigned peers0 = __match_any_sync(0xffffffffu, b0);
+    const unsigned peers1 = __match_any_sync(0xffffffffu, b1);
+    if (b0 >= 0 && (peers0 & lt) == 0) wc[(2 * warp) * nblk + b0] = __popc(peers0);
+    if (b1 >= 0 && (peers1 & lt) == 0) wc[(2 * warp + 1) * nblk + b1] = __popc(peers1);
+    __syncthreads();
+    for (int b = tid; b < nblk; b += nthr) {
+      int s = cursor[b];
+      for (int j = 0; j < nvw; ++j) {
+        const int c = wc[j * nblk + b];
+        wc[j * nblk + b] = s;
+        s += c;
+      }
+      cursor[b] = s;
+    }
+    __syncthreads();
+    if (b0 >= 0) vlist[wc[(2 * warp) * nblk + b0] + __popc(peers0 & lt)] = p;
+    if (b1 >= 0) vlist[wc[(2 * warp + 1) * nblk + b1] + __popc(peers1 & lt)] = p;
+    __syncthreads();
+  }
+}
+
+// Forward CTA (channel block, view of the chunk) over its bucket.  The
+// epilogue sees the absolute view v_start + vl and partial slot
+// (v_start + vl) * nblk + block; touched[view * nblk + block] records
+// whether any pixel reached the tile.
+template <typename EPI>
+__global__ void __launch_bounds__(1024)
+forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values, int P, int band,
+                           int slice_start, const ConeFwdRec *__restrict__ recs,
+                           const int *__restrict__ list, const int *__restrict__ offs,
+                           unsigned char *__restrict__ touched, EPI epi) {
+  extern __shared__ float4 sm4[];
+  const int nthr = blockDim.x, tid = threadIdx.x;
+  const int cap = fwd_cap(nthr);
+  const int SP = band + 2 * kFwdVPad;
+  ConeFwdRec *rec = reinterpret_cast<ConeFwdRec *>(sm4);
+  float *stage = reinterpret_cast<float *>(rec + cap);
+  const int nblk = gridDim.x, blk = blockIdx.x, vl = blockIdx.y;
+  const int c0 = blk * kFwdCB;
+  const int ncb = min(kFwdCB, g.C - c0);
+  const int bp = g.bp;
+  const float kc_lo = (float)(slice_start - bp - 1),
+              kc_hi = (float)(slice_start + band + bp);
+  const ConeFwdRec *vrec = recs + (size_t)vl * P;
+  const int *vlist = list + (size_t)vl * 2 * P;
+  const int start = offs[(size_t)vl * (nblk + 1) + blk];
+  const int end = offs[(size_t)vl * (nblk + 1) + blk + 1];
+  const int v = v_start + vl;
+  if (tid == 0) touched[(size_t)v * nblk + blk] = end > start;
+  if (end == start) {
+    // No pixel reaches the tile: its A x is zero and is not stored (readers
+    // consult `touched`); the epilogue's partials are zero.
+    epi.begin(v);
+    epi.end(v * nblk + blk);
+    return;
+  }
+
+  for (int i = tid; i < kFwdEB * SP; i += nthr) stage[i] = 0.f;
+  float acc[kFwdCB];
+#pragma unroll
+  for (int j = 0; j < kFwdCB; ++j) acc[j] = 0.f;
+  for (int base = start; base < end; base += cap) {
+    const int n = min(cap, end - base);
+    __syncthreads();
+    for (int i = tid; i < n; i += nthr) rec[i] = vrec[vlist[base + i]];
+    __syncthreads();
+    fwd_rt_round(rec, n, c0, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, acc);
+  }
+  epi.begin(v);
+  if (tid < g.R) epi.cells(v, c0, ncb, tid, acc);
+  epi.end(v * nblk + blk);
 }
 
 }  // namespace mbir

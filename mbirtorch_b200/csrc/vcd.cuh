@@ -110,6 +110,7 @@ vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int 
   if (i < n) {
     const int p = (int)(i / S), l = (int)(i - (size_t)p * S);
     float bp = 0.f;
+#pragma unroll 8
     for (int c = 0; c < nchunks; ++c) bp += part[(size_t)c * n + i];
     const int pixel = (int)pix[p];
     const float g_f = __fmul_rn(-sc.fmc, bp);
@@ -166,6 +167,7 @@ __global__ void vcd_dc_sums_kernel(int P, int S, int pchunk, const float *__rest
   if (l >= S) return;
   const int p0 = chunk * pchunk, p1 = min(P, p0 + pchunk);
   double num = 0.0, den = 0.0;
+#pragma unroll 8
   for (int p = p0; p < p1; ++p) {
     const size_t i = (size_t)p * S + l;
     const float hi = hinv[i];
@@ -189,6 +191,7 @@ vcd_dc_direction_kernel(int P, int S, int nchunks, const double *__restrict__ su
   if (i < n) {
     const int l = (int)(i % S);
     double num = 0.0, den = 0.0;
+#pragma unroll 8
     for (int c = 0; c < nchunks; ++c) {
       num += sums[((size_t)c * S + l) * 2];
       den += sums[((size_t)c * S + l) * 2 + 1];
@@ -209,6 +212,8 @@ vcd_dc_direction_kernel(int P, int S, int nchunks, const double *__restrict__ su
 }
 
 // ── 3. forward epilogue: line search + Ad store ───────────────────────────
+// The per-view scale is a power of two, so Ad / scale is formed exactly as
+// Ad * (1 / scale).
 template <typename T>
 struct LineSearchEpi {
   const T *e;
@@ -220,26 +225,65 @@ struct LineSearchEpi {
   double *partials;
   int with_sums;
   double fl, fq;
+  float scale, inv_scale, wscale;
   __device__ __forceinline__ bool channel_fastest() const { return false; }
-  __device__ __forceinline__ void begin() {
+  __device__ __forceinline__ void begin(int v) {
     fl = 0.0;
     fq = 0.0;
+    scale = __ldg(es + v);
+    inv_scale = 1.f / scale;
+    wscale = w != nullptr ? __ldg(wsc + v) : 1.f;
   }
   __device__ __forceinline__ void cell(int v, int c, int m, float val) {
     const size_t i = ((size_t)v * C + c) * R + m;
-    const float scale = __ldg(es + v);
-    const T stored = from_f32<T>(__fdiv_rn(val, scale));
+    const T stored = from_f32<T>(__fmul_rn(val, inv_scale));
     ad[i] = stored;
     if (!with_sums) return;
     const float adv = __fmul_rn(to_f32(stored), scale);
     const float ev = __fmul_rn(to_f32(e[i]), scale);
     if (w != nullptr) {
-      const float wv = __fmul_rn(to_f32(w[i]), __ldg(wsc + v));
+      const float wv = __fmul_rn(to_f32(w[i]), wscale);
       fl += (double)__fmul_rn(__fmul_rn(wv, ev), adv);
       fq += (double)__fmul_rn(__fmul_rn(adv, adv), wv);
     } else {
       fl += (double)__fmul_rn(ev, adv);
       fq += (double)__fmul_rn(adv, adv);
+    }
+  }
+  // A row's cells at channels c0 .. c0 + ncb - 1 at once: every load of e
+  // and w goes out before the first store of Ad, which the compiler could
+  // not otherwise move past (the pointers may alias as far as it knows).
+  template <int N>
+  __device__ __forceinline__ void cells(int v, int c0, int ncb, int m, const float (&acc)[N]) {
+    const size_t i0 = ((size_t)v * C + c0) * R + m;
+    float ev[N], wv[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      ev[j] = 0.f;
+      wv[j] = 0.f;
+      if (with_sums && j < ncb) {
+        ev[j] = to_f32(e[i0 + (size_t)j * R]);
+        if (w != nullptr) wv[j] = to_f32(w[i0 + (size_t)j * R]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      if (j < ncb) {
+        const T stored = from_f32<T>(__fmul_rn(acc[j], inv_scale));
+        ad[i0 + (size_t)j * R] = stored;
+        if (with_sums) {
+          const float adv = __fmul_rn(to_f32(stored), scale);
+          const float evs = __fmul_rn(ev[j], scale);
+          if (w != nullptr) {
+            const float wvs = __fmul_rn(wv[j], wscale);
+            fl += (double)__fmul_rn(__fmul_rn(wvs, evs), adv);
+            fq += (double)__fmul_rn(__fmul_rn(adv, adv), wvs);
+          } else {
+            fl += (double)__fmul_rn(evs, adv);
+            fq += (double)__fmul_rn(adv, adv);
+          }
+        }
+      }
     }
   }
   __device__ __forceinline__ void end(int slot) {
@@ -261,29 +305,49 @@ struct RefreshEpi {
   T *e;
   const float *es;
   int C, R;
+  float inv_scale;
   __device__ __forceinline__ bool channel_fastest() const { return false; }
-  __device__ __forceinline__ void begin() {}
+  __device__ __forceinline__ void begin(int v) { inv_scale = 1.f / __ldg(es + v); }
   __device__ __forceinline__ void cell(int v, int c, int m, float val) {
     const size_t i = ((size_t)v * C + c) * R + m;
-    e[i] = from_f32<T>(__fdiv_rn(__fsub_rn(__ldg(y + i), val), __ldg(es + v)));
+    e[i] = from_f32<T>(__fmul_rn(__fsub_rn(__ldg(y + i), val), inv_scale));
+  }
+  template <int N>
+  __device__ __forceinline__ void cells(int v, int c0, int ncb, int m, const float (&acc)[N]) {
+    const size_t i0 = ((size_t)v * C + c0) * R + m;
+    float yv[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) yv[j] = j < ncb ? __ldg(y + i0 + (size_t)j * R) : 0.f;
+#pragma unroll
+    for (int j = 0; j < N; ++j)
+      if (j < ncb)
+        e[i0 + (size_t)j * R] = from_f32<T>(__fmul_rn(__fsub_rn(yv[j], acc[j]), inv_scale));
   }
   __device__ __forceinline__ void end(int) {}
 };
 
 // ── 4. alpha ─────────────────────────────────────────────────────────────
-// One CTA.  prior: np pairs (pl, pq); fwd: nf pairs (fl, fq).
-__global__ void __launch_bounds__(kThreads)
+// One CTA of kAlphaThreads.  prior: np pairs (pl, pq); fwd: nf pairs (fl, fq).
+constexpr int kAlphaThreads = 1024;
+
+__global__ void __launch_bounds__(kAlphaThreads)
 vcd_alpha_kernel(const double *__restrict__ prior, int np, const double *__restrict__ fwd, int nf,
                  float fmc, float max_alpha, float *__restrict__ alpha_out,
                  float *__restrict__ alpha_user) {
   double pl = 0.0, pq = 0.0, fl = 0.0, fq = 0.0;
-  for (int i = threadIdx.x; i < np; i += kThreads) {
-    pl += prior[2 * i];
-    pq += prior[2 * i + 1];
+  const double2 *pr2 = reinterpret_cast<const double2 *>(prior);
+  const double2 *fw2 = reinterpret_cast<const double2 *>(fwd);
+#pragma unroll 4
+  for (int i = threadIdx.x; i < np; i += kAlphaThreads) {
+    const double2 v = pr2[i];
+    pl += v.x;
+    pq += v.y;
   }
-  for (int i = threadIdx.x; i < nf; i += kThreads) {
-    fl += fwd[2 * i];
-    fq += fwd[2 * i + 1];
+#pragma unroll 4
+  for (int i = threadIdx.x; i < nf; i += kAlphaThreads) {
+    const double2 v = fw2[i];
+    fl += v.x;
+    fq += v.y;
   }
   block_sum2(pl, pq);
   block_sum2(fl, fq);
@@ -312,6 +376,7 @@ __global__ void vcd_positivity_kernel(int P, int S, const int64_t *__restrict__ 
 }
 
 // ── 5. update ────────────────────────────────────────────────────────────
+constexpr int kUpdPix = 8;  // pixels per load batch of the recon update
 // Recon scatter-add over a (pixel chunk, slice block) tile; per-slice sum of
 // squares and ell1 partials.
 __global__ void __launch_bounds__(kThreads)
@@ -325,12 +390,26 @@ vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pi
   const float a = alpha[0];
   double sq = 0.0, l1 = 0.0;
   if (l < S) {
-    for (int p = p0; p < p1; ++p) {
-      const float ds = __fmul_rn(a, delta[(size_t)p * S + l]);
-      float *x = flat + (size_t)pix[p] * S + l;
-      *x = __fadd_rn(*x, ds);
-      sq += (double)__fmul_rn(ds, ds);
-      l1 += (double)fabsf(ds);
+    // The pixels of a subset are distinct, so all kUpdPix loads of the
+    // cylinders' voxels go out before the first store.
+    for (int pb = p0; pb < p1; pb += kUpdPix) {
+      float ds[kUpdPix], xv[kUpdPix];
+      float *xp[kUpdPix];
+#pragma unroll
+      for (int u = 0; u < kUpdPix; ++u) {
+        const int p = min(pb + u, P - 1);
+        ds[u] = __fmul_rn(a, delta[(size_t)p * S + l]);
+        xp[u] = flat + (size_t)pix[p] * S + l;
+        xv[u] = *xp[u];
+      }
+#pragma unroll
+      for (int u = 0; u < kUpdPix; ++u) {
+        if (pb + u < p1) {
+          *xp[u] = __fadd_rn(xv[u], ds[u]);
+          sq += (double)__fmul_rn(ds[u], ds[u]);
+          l1 += (double)fabsf(ds[u]);
+        }
+      }
     }
     sq_part[(size_t)chunk * S + l] = sq;
   }
@@ -346,10 +425,12 @@ vcd_finish_kernel(int S, int nchunks, int nl1, const double *__restrict__ sq_par
                   double *__restrict__ accum) {
   for (int l = threadIdx.x; l < S; l += kThreads) {
     double s = 0.0;
+#pragma unroll 8
     for (int c = 0; c < nchunks; ++c) s += sq_part[(size_t)c * S + l];
     accum[2 + l] += s;
   }
   double l1 = 0.0, dummy = 0.0;
+#pragma unroll 4
   for (int i = threadIdx.x; i < nl1; i += kThreads) l1 += l1_part[i];
   block_sum2(l1, dummy);
   if (threadIdx.x == 0) {
@@ -393,6 +474,39 @@ __global__ void vcd_sino_update_kernel<float>(size_t n, const float *__restrict_
   for (size_t i = n4 * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
     e[i] = __fsub_rn(e[i], __fmul_rn(a, ad[i]));
+}
+
+// The same update over the (view, channel-block) tiles a binned forward
+// marked as reached (grid: blocks x views).  A tile is CB consecutive
+// channels of one view, i.e. one contiguous run of CB * R cells.
+template <typename T>
+__global__ void __launch_bounds__(256)
+vcd_sino_update_tiles_kernel(int C, int R, int CB, const unsigned char *__restrict__ touched,
+                             const float *__restrict__ alpha, T *__restrict__ e,
+                             const T *__restrict__ ad) {
+  const int b = blockIdx.x, v = blockIdx.y;
+  if (!touched[(size_t)v * gridDim.x + b]) return;
+  const float a = alpha[0];
+  const int c0 = b * CB;
+  const int n = min(CB, C - c0) * R;
+  const size_t base = ((size_t)v * C + c0) * R;
+  T *et = e + base;
+  const T *dt = ad + base;
+  constexpr int U = 4;
+  for (int i0 = threadIdx.x; i0 < n; i0 += 256 * U) {
+    float ev[U], dv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + 256 * u;
+      ev[u] = i < n ? to_f32(et[i]) : 0.f;
+      dv[u] = i < n ? to_f32(dt[i]) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + 256 * u;
+      if (i < n) et[i] = from_f32<T>(__fsub_rn(ev[u], __fmul_rn(a, dv[u])));
+    }
+  }
 }
 
 // ── iteration statistics / init / conversion ─────────────────────────────
@@ -506,7 +620,8 @@ __global__ void fill_kernel(int n, float v, float *__restrict__ out) {
   if (i < n) out[i] = v;
 }
 
-// Per-view max |value| of an f32 VRC sinogram -> scale (f16 storage).
+// Per-view max |value| of an f32 VRC sinogram -> power-of-two scale (16-bit
+// storage).
 __global__ void __launch_bounds__(kThreads)
 view_scale_kernel(int RC, const float *__restrict__ src, float target, float *__restrict__ scale) {
   const int v = blockIdx.x;
@@ -519,7 +634,15 @@ view_scale_kernel(int RC, const float *__restrict__ src, float target, float *__
   if (threadIdx.x == 0) {
     float t = 0.f;
     for (int w = 0; w < kThreads / 32; ++w) t = fmaxf(t, sm[w]);
-    scale[v] = t > 0.f ? t / target : 1.f;
+    // The smallest power of two s with t / s <= target, so that scaling
+    // and unscaling are exact.
+    float s = 1.f;
+    if (t > 0.f) {
+      int ex;
+      const float mant = frexpf(t / target, &ex);
+      s = ldexpf(1.f, mant == 0.5f ? ex - 1 : ex);
+    }
+    scale[v] = s;
   }
 }
 

@@ -131,6 +131,7 @@ class ReconServer:
         self.completed = []
         self._next_id = 0
         self.max_concurrent = 0
+        self.deferred = 0   # admissions put off because the ledger was full
         self.t0 = None
 
     # ── requests ───────────────────────────────────────────────────────────
@@ -147,8 +148,27 @@ class ReconServer:
         return r
 
     # ── scheduling ─────────────────────────────────────────────────────────
+    def job_charge(self, model, weighted, max_iterations):
+        """(peak, resident) ledger bytes of a job on ``model``.  Subsets are
+        equal sized, ceil(ROR pixels / subsets), so the largest one in the
+        partition sequence is known before any partition is drawn."""
+        rs, gran, ror = model.get_params(['recon_shape', 'granularity', 'use_ror_mask'])
+        n_pix = int(vcd_utils.get_2d_ror_mask(rs, use_ror_mask=ror).sum()) \
+            if ror is not False else rs[0] * rs[1]
+        seq = vcd_utils.gen_partition_sequence(model.get_params('partition_sequence'),
+                                               max_iterations)
+        max_ps = max((-(-n_pix // min(int(gran[int(i)]), n_pix)) for i in seq), default=1)
+        return MemoryLedger.job_bytes(model, self.storage_dtype, weighted, max_ps)
+
     def _admit(self, r):
         m = r.model
+        peak, resident = self.job_charge(m, r.weights is not None, r.max_iterations)
+        if not self.ledger.fits(peak):
+            if self.active:
+                self.deferred += 1
+                return False
+            raise MemoryError(f'request {r.id} needs {peak} bytes; the ledger budget is '
+                              f'{self.ledger.budget}')
         m.storage_dtype = self.storage_dtype
         m.configure_devices(devices=[self.device])
         m.setup_logger(logfile_path=None, print_logs=False)
@@ -157,11 +177,6 @@ class ReconServer:
         parts = [vcd_utils.gen_pixel_partition(rs, n, use_ror_mask=ror, rng=rng) for n in gran]
         seq = vcd_utils.gen_partition_sequence(m.get_params('partition_sequence'),
                                                r.max_iterations)
-        max_ps = max((int(parts[int(i)].shape[1]) for i in seq), default=1)
-        peak, resident = MemoryLedger.job_bytes(m, self.storage_dtype, r.weights is not None,
-                                                max_ps)
-        if not self.ledger.fits(peak) and self.active:
-            return False
         m.auto_set_regularization_params(r.sinogram, weights=r.weights)
         r._stream = torch.cuda.Stream(self.device)
         r._run = VcdRun(m, r.sinogram, parts, seq, r.stop_pct, weights=r.weights, rng=rng,

@@ -13,7 +13,7 @@ import pytest
 import torch
 
 import mbirtorch_b200 as mb
-from mbirtorch_b200.serving import MemoryLedger, ReconServer
+from mbirtorch_b200.serving import ReconServer
 
 pytestmark = pytest.mark.gpu
 
@@ -98,13 +98,13 @@ def test_server_equals_model_recon_with_same_seed():
 
 def test_admission_respects_ledger_and_failures_are_isolated():
     jobs = _jobs()
-    # A budget that holds one job at a time (the largest job's peak).
-    peaks = []
-    for make, _ in jobs:
-        m = make()
-        peaks.append(MemoryLedger.job_bytes(m, 'float16', False, 4096)[0])
-    srv = ReconServer(storage_dtype='float16', max_active=8,
-                      memory_budget_bytes=int(max(peaks) * 1.05))
+    # A budget one byte short of all jobs resident at once: some admissions
+    # must wait for a finished job's release.
+    srv = ReconServer(storage_dtype='float16', max_active=8, memory_budget_bytes=1)
+    charges = [srv.job_charge(make(), False, 2) for make, _ in jobs]
+    budget = sum(res for _, res in charges) - 1
+    assert max(peak for peak, _ in charges) <= budget
+    srv = ReconServer(storage_dtype='float16', max_active=8, memory_budget_bytes=budget)
     reqs = []
     for i, (make, sino) in enumerate(jobs):
         m = make()
@@ -115,7 +115,7 @@ def test_admission_respects_ledger_and_failures_are_isolated():
     reqs.append(srv.submit(bad, np.zeros((3, 3, 3), np.float32), max_iterations=2))
     srv.run_until_idle(timeout_s=300)
     assert srv.ledger.high_water <= srv.ledger.budget
-    assert srv.max_concurrent < len(jobs)
+    assert srv.max_concurrent < len(jobs) and srv.deferred > 0
     assert all(r.error is None for r in reqs[:-1])
     assert isinstance(reqs[-1].error, ValueError)
     st = srv.stats()

@@ -191,3 +191,59 @@ def test_recon_simple_parallel_equals_model_path():
                                                           endpoint=False))
     r2, _ = m.recon(d['sino'], max_iterations=2)
     assert rel_l2(r1, r2) <= 1e-6
+
+
+def test_cone_subset_step_binned_view_chunks_weights_positivity():
+    """A whole-image cone subset (65536 pixels x 40 views) splits the binned
+    forward into view chunks; weighted, with positivity: one step against
+    the FP64 oracle."""
+    from oracle import vcd as ovcd
+    V = 40
+    m = mb.ConeBeamModel((V, 8, 320), np.linspace(0, 2 * np.pi, V, endpoint=False),
+                         2048.0, 1024.0)
+    m.set_params(no_warning=True, verbose=0, delta_det_channel=2.0, delta_det_row=2.0)
+    m.auto_set_recon_geometry(no_warning=True)
+    m.set_params(no_warning=True, recon_shape=(256, 256, 4), positivity_flag=True)
+    rs = m.get_params('recon_shape')
+    rng = np.random.default_rng(11)
+    x_true = rng.random(rs).astype(np.float32)
+    sino = m.forward_project(x_true)
+    w = (0.5 + rng.random(sino.shape)).astype(np.float32)
+    m.auto_set_regularization_params(sino, weights=w)
+    x0 = (0.05 * rng.standard_normal(rs)).astype(np.float32)
+    e0 = sino - m.forward_project(x0)
+    H = m.compute_hessian_diagonal(weights=w)
+    upd = m.create_vcd_subset_updater(H, weights=torch.as_tensor(w, device='cuda'))
+    idx = np.arange(rs[0] * rs[1], dtype=np.int64)
+    flat = torch.as_tensor(x0.reshape(-1, rs[2]), device='cuda').clone()
+    err = torch.as_tensor(e0, device='cuda').clone()
+    flat, err, ell1, alpha, sumsq = upd(flat, err, torch.as_tensor(idx, device='cuda'))
+    prob = _oracle_problem(m)
+    sy, sx = m.get_params(['sigma_y', 'sigma_x'])
+    ou = ovcd.SubsetUpdater(prob, H.reshape(-1, rs[2]), w, sy, sx, positivity=True,
+                            dc_profile=ovcd.dc_damping_profile(prob))
+    oflat = x0.reshape(-1, rs[2]).astype(np.float64)
+    oerr = e0.astype(np.float64)
+    _, oalpha, _ = ou(oflat, oerr, idx)
+    assert abs(float(alpha) - oalpha) / oalpha <= 1e-4
+    assert rel_l2(flat.cpu().numpy(), oflat) <= 1e-5
+    assert rel_l2(err.cpu().numpy(), oerr) <= 1e-5
+
+
+def test_sixteen_bit_view_scales_are_powers_of_two():
+    from mbirtorch_b200.vcd_engine import ResidentSinogram
+    rng = np.random.default_rng(2)
+    s = torch.as_tensor((rng.standard_normal((7, 5, 6)) * 10 ** rng.uniform(-3, 3, (7, 1, 1)))
+                        .astype(np.float32), device='cuda')
+    s[3] = 0
+    vmax = s.abs().amax(dim=(1, 2)).cpu().numpy()
+    # float16: max |e_v| / scale in (128, 256]; bfloat16 keeps f32's exponent
+    # range and a unit scale.
+    r = ResidentSinogram.from_vrc(s, 2)
+    sc = r.scale.cpu().numpy().astype(np.float64)
+    assert np.array_equal(np.exp2(np.round(np.log2(sc))), sc)
+    assert np.all(vmax / sc <= 256) and np.all((vmax == 0) | (vmax / sc > 128))
+    assert rel_l2(r.to_vrc().cpu().numpy(), s.cpu().numpy()) <= 1e-3
+    r = ResidentSinogram.from_vrc(s, 1)
+    assert np.all(r.scale.cpu().numpy() == 1)
+    assert rel_l2(r.to_vrc().cpu().numpy(), s.cpu().numpy()) <= 4e-3

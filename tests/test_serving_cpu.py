@@ -33,3 +33,18 @@ def test_job_charge_grows_with_size_and_shrinks_with_precision():
     # but halves the error and delta sinograms; weights add one array.
     assert rw - r16 == 2 * V * R * C
     assert r16 > 0
+
+
+def test_job_charge_matches_drawn_partitions():
+    from mbirtorch_b200 import vcd_utils
+    from mbirtorch_b200.serving import ReconServer
+    m = _cone((40, 12, 24))
+    srv = ReconServer(device='cuda:0', memory_budget_bytes=1 << 30, storage_dtype='float16')
+    rs, gran, ror = m.get_params(['recon_shape', 'granularity', 'use_ror_mask'])
+    rng = np.random.RandomState(5)
+    parts = [vcd_utils.gen_pixel_partition(rs, n, use_ror_mask=ror, rng=rng) for n in gran]
+    for iters in (1, 3, 20):
+        seq = vcd_utils.gen_partition_sequence(m.get_params('partition_sequence'), iters)
+        max_ps = max(int(parts[int(i)].shape[1]) for i in seq)
+        assert srv.job_charge(m, False, iters) == \
+            MemoryLedger.job_bytes(m, 'float16', False, max_ps)
