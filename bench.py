@@ -70,13 +70,13 @@ def profile_case(case, m, mb, torch, y):
         m.recon(y, max_iterations=ITERS, stop_threshold_change_pct=0, logfile_path=None,
                 print_logs=False, output_sharded=True)
     elif case == "subset":
-        from mbirtorch_b200.vcd_engine import ResidentSinogram
+        from mbirtorch_b200.vcd_engine import ResidentSinogram, storage_code
         m.auto_set_regularization_params(y)
         H = m.compute_hessian_diagonal(output_sharded=True)
         upd = m.create_vcd_subset_updater(H, weights=1)
         rs = m.get_params('recon_shape')
         flat = torch.zeros(rs[0] * rs[1], rs[2], device=y.device)
-        err = ResidentSinogram.from_vrc(y)
+        err = ResidentSinogram.from_vrc(y, storage_code(m.storage_dtype))
         np.random.seed(0)
         parts = torch.as_tensor(mb.gen_pixel_partition(rs, 128), device=y.device)
         for i in range(3):

@@ -87,7 +87,7 @@ class VcdRun:
         sino = None if self.init_error_sinogram is not None else m._sino_device(self.sinogram)
         refresh = m.error_refresh_interval
         if refresh is None:
-            refresh = 0 if self.storage == _lib.MBIR_F32 else 1
+            refresh = {_lib.MBIR_F32: 0, _lib.MBIR_F16: 5, _lib.MBIR_BF16: 1}[self.storage]
         self.refresh = refresh
         self.y_vcr = None
         if refresh and sino is not None:
