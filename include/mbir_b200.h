@@ -118,6 +118,15 @@ typedef struct mbir_vcd_params {
     int32_t positivity;  /* clip so that recon + alpha * delta >= 0 */
     int32_t storage;     /* MBIR_F32 / MBIR_BF16 / MBIR_F16 for the error
                             sinogram, the weights and the delta sinogram */
+    /* Proximal-map prior (prox_map, tomography_model.py:3251-3373, with the
+     * gradient of qggmrf.py:186-206 and the scalar Hessian of
+     * tomography_model.py:2530-2537).  prox_input == NULL selects the
+     * qGGMRF prior and the two fields below are ignored; otherwise the
+     * prior's gradient is prox_constant * (x - prox_input) and its Hessian
+     * prox_constant. */
+    float prox_constant;          /* 1 / sigma_prox^2, > 0 */
+    int32_t reserved;             /* zero */
+    const float *prox_input;      /* (N*N, S) f32 device array, like flat_recon */
 } mbir_vcd_params;
 
 /* Version of this ABI (major * 10000 + minor * 100 + patch). */

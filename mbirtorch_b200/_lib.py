@@ -68,6 +68,9 @@ class VcdParams(ctypes.Structure):
         ("max_alpha", ctypes.c_float),
         ("positivity", ctypes.c_int32),
         ("storage", ctypes.c_int32),
+        ("prox_constant", ctypes.c_float),
+        ("reserved", ctypes.c_int32),
+        ("prox_input", ctypes.c_void_p),
     ]
 
 

@@ -599,6 +599,8 @@ int validate_vcd(const mbir_geometry *g, const mbir_vcd_params *prm, const void 
   if (Ps <= 0) return fail(MBIR_ERR_INVALID, "subset must have at least one pixel");
   if (!(prm->sigma_x > 0.f) || !(prm->fm_constant > 0.f) || !(prm->T > 0.f))
     return fail(MBIR_ERR_INVALID, "sigma_x, T and fm_constant must be positive");
+  if (prm->prox_input != nullptr && !(prm->prox_constant > 0.f))
+    return fail(MBIR_ERR_INVALID, "prox_constant (1 / sigma_prox^2) must be positive");
   return MBIR_OK;
 }
 
@@ -606,7 +608,7 @@ int validate_vcd(const mbir_geometry *g, const mbir_vcd_params *prm, const void 
 
 extern "C" {
 
-int32_t mbir_abi_version(void) { return 10000; }
+int32_t mbir_abi_version(void) { return 10100; }
 
 const char *mbir_last_error(void) { return g_last_error.c_str(); }
 

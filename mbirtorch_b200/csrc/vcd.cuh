@@ -37,6 +37,8 @@ struct VcdScalars {
   float two_b[6];   // 2 * b[j]  (get_2_b_tilde's b_for_delta * 2.0)
   float b[6];
   float max_alpha;
+  float prox_c;        // 1 / sigma_prox^2 (proximal-map prior)
+  const float *prox;   // proximal-map prior mean, (N*N, S); NULL: qGGMRF prior
 };
 
 inline VcdScalars make_scalars(const mbir_vcd_params &p) {
@@ -53,6 +55,8 @@ inline VcdScalars make_scalars(const mbir_vcd_params &p) {
     s.two_b[j] = (float)((double)p.b[j] * 2.0);
   }
   s.max_alpha = p.max_alpha;
+  s.prox_c = p.prox_constant;
+  s.prox = p.prox_input;
   return s;
 }
 
@@ -115,27 +119,35 @@ vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int 
     const int pixel = (int)pix[p];
     const float g_f = __fmul_rn(-sc.fmc, bp);
     const float h_f = __fmul_rn(sc.fmc, H[(size_t)pixel * S + l]);
-    // qGGMRF surrogate (qggmrf.py:117-183): slice term with reflected ends,
-    // then the 4 clamped in-plane neighbours.
     const float *cyl = flat + (size_t)pixel * S;
     const float xs = cyl[l];
-    const float dp = (l + 1 < S) ? __fsub_rn(cyl[l + 1], xs) : 0.f;  // delta[l+1]
-    const float dm = (l > 0) ? __fsub_rn(xs, cyl[l - 1]) : 0.f;      // delta[l]
-    const float bt_p = __fmul_rn(2.f, b_tilde(dp, sc));
-    const float bt_m = __fmul_rn(2.f, b_tilde(dm, sc));
-    float g_p = __fadd_rn(__fmul_rn(-sc.b[4], __fmul_rn(bt_p, dp)),
-                          __fmul_rn(sc.b[5], __fmul_rn(bt_m, dm)));
-    float h_p = __fadd_rn(__fmul_rn(sc.b[4], bt_p), __fmul_rn(sc.b[5], bt_m));
-    const int row = pixel / NC, col = pixel - (pixel / NC) * NC;
-    const int dr[4] = {1, -1, 0, 0}, dc[4] = {0, 0, 1, -1};
+    float g_p, h_p;
+    if (sc.prox != nullptr) {
+      // Proximal-map prior (qggmrf.py:186-206): gradient (x - v) / sigma^2,
+      // Hessian 1 / sigma^2.
+      g_p = __fmul_rn(sc.prox_c, __fsub_rn(xs, sc.prox[(size_t)pixel * S + l]));
+      h_p = sc.prox_c;
+    } else {
+      // qGGMRF surrogate (qggmrf.py:117-183): slice term with reflected
+      // ends, then the 4 clamped in-plane neighbours.
+      const float dp = (l + 1 < S) ? __fsub_rn(cyl[l + 1], xs) : 0.f;  // delta[l+1]
+      const float dm = (l > 0) ? __fsub_rn(xs, cyl[l - 1]) : 0.f;      // delta[l]
+      const float bt_p = __fmul_rn(2.f, b_tilde(dp, sc));
+      const float bt_m = __fmul_rn(2.f, b_tilde(dm, sc));
+      g_p = __fadd_rn(__fmul_rn(-sc.b[4], __fmul_rn(bt_p, dp)),
+                      __fmul_rn(sc.b[5], __fmul_rn(bt_m, dm)));
+      h_p = __fadd_rn(__fmul_rn(sc.b[4], bt_p), __fmul_rn(sc.b[5], bt_m));
+      const int row = pixel / NC, col = pixel - (pixel / NC) * NC;
+      const int dr[4] = {1, -1, 0, 0}, dc[4] = {0, 0, 1, -1};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int rr = min(max(row + dr[k], 0), NR - 1);
-      const int cc = min(max(col + dc[k], 0), NC - 1);
-      const float d = __fsub_rn(xs, flat[((size_t)rr * NC + cc) * S + l]);
-      const float w = __fmul_rn(sc.two_b[k], b_tilde(d, sc));
-      g_p = __fadd_rn(g_p, __fmul_rn(w, d));
-      h_p = __fadd_rn(h_p, w);
+      for (int k = 0; k < 4; ++k) {
+        const int rr = min(max(row + dr[k], 0), NR - 1);
+        const int cc = min(max(col + dc[k], 0), NC - 1);
+        const float d = __fsub_rn(xs, flat[((size_t)rr * NC + cc) * S + l]);
+        const float w = __fmul_rn(sc.two_b[k], b_tilde(d, sc));
+        g_p = __fadd_rn(g_p, __fmul_rn(w, d));
+        h_p = __fadd_rn(h_p, w);
+      }
     }
     if (!DC) {
       const float dl = -__fdiv_rn(__fadd_rn(g_f, g_p), __fadd_rn(h_f, h_p));

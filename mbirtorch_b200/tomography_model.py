@@ -373,20 +373,44 @@ class TomographyModel(ParameterHandler):
         return (1.0 / (2 * sigma_y ** 2)) * torch.sum((error_sinogram * error_sinogram) * weights)
 
     # ── the VCD engine seam ─────────────────────────────────────────────────
-    def _vcd_params(self, storage):
+    def _vcd_params(self, storage, prox_flat=None):
         nbr, sigma_x, p, q, T = self.get_params(['qggmrf_nbr_wts', 'sigma_x', 'p', 'q', 'T'])
         b = _qggmrf.get_b_from_nbr_wts(nbr)
         fm_constant = 1.0 / (self.get_params('sigma_y') ** 2.0)
+        prox_constant, prox_ptr = 0.0, None
+        if prox_flat is not None:
+            # 1 / sigma_prox^2 in double precision, rounded once to float32 as
+            # the reference's python-scalar * float32-tensor product does.
+            prox_constant = 1.0 / (self.get_params('sigma_prox') ** 2.0)
+            prox_ptr = prox_flat.data_ptr()
         return make_vcd_params(fm_constant, sigma_x, p, q, T, b, self.get_params('max_alpha'),
-                               self.get_params('positivity_flag') is True, storage)
+                               self.get_params('positivity_flag') is True, storage,
+                               prox_constant, prox_ptr)
 
-    def _make_engine(self, fm_hessian_flat, weights_res, storage, max_subset_pixels=1):
+    def _prox_flat(self, prox_input):
+        """The proximal-map input as a contiguous (N*N, S) float32 device
+        array (tomography_model.py:2842-2860: shape checked before
+        flattening)."""
+        if prox_input is None:
+            return None
+        recon_shape = tuple(self.get_params('recon_shape'))
+        if tuple(prox_input.shape) != recon_shape:
+            raise ValueError('prox_input does not have the correct size. \n'
+                             f'Expected {recon_shape}, got shape '
+                             f'{tuple(prox_input.shape)} for prox_input shape.')
+        return self._recon_device(prox_input).reshape(-1, recon_shape[2]).contiguous()
+
+    def _make_engine(self, fm_hessian_flat, weights_res, storage, max_subset_pixels=1,
+                     prox_flat=None):
         dc = self._dc_damping_profile()
         dc_t = None if dc is None else torch.as_tensor(dc, dtype=torch.float32,
                                                        device=self.torch_device)
-        return VcdEngine(self._geometry(), self.projector.view_params, self._vcd_params(storage),
-                         fm_hessian_flat, weights=weights_res, dc_profile=dc_t,
-                         max_subset_pixels=max_subset_pixels)
+        engine = VcdEngine(self._geometry(), self.projector.view_params,
+                           self._vcd_params(storage, prox_flat), fm_hessian_flat,
+                           weights=weights_res, dc_profile=dc_t,
+                           max_subset_pixels=max_subset_pixels)
+        engine.prox_flat = prox_flat  # the parameters point at it
+        return engine
 
     def create_vcd_subset_updater(self, fm_hessian, weights, prox_input=None):
         """The subset updater of tomography_model.py:2434-2660: returns
@@ -395,10 +419,9 @@ class TomographyModel(ParameterHandler):
         ``(flat_recon, error_sinogram, ell1, alpha, delta_sumsq)`` as device
         values.  ``error_sinogram`` may be the resident form
         (:class:`ResidentSinogram`) or a (V, R, C) float32 CUDA tensor
-        (converted in and out around the update)."""
-        if prox_input is not None:
-            raise NotImplementedError('the proximal-map prior is not implemented on the '
-                                      'sm_100a path yet')
+        (converted in and out around the update).  With ``prox_input``
+        (the recon's shape) the prior is the proximal map's instead of
+        qGGMRF."""
         const_weights = not torch.is_tensor(weights) and not isinstance(weights,
                                                                        ResidentSinogram)
         if const_weights and abs(weights - 1) > 1e-5:
@@ -410,7 +433,7 @@ class TomographyModel(ParameterHandler):
         if not const_weights:
             w_res = (weights if isinstance(weights, ResidentSinogram)
                      else ResidentSinogram.from_vrc(self._sino_device(weights), storage))
-        engine = self._make_engine(H, w_res, storage)
+        engine = self._make_engine(H, w_res, storage, prox_flat=self._prox_flat(prox_input))
 
         def vcd_subset_updater(flat_recon, error_sinogram, pixel_indices):
             plain = torch.is_tensor(error_sinogram)
@@ -518,17 +541,63 @@ class TomographyModel(ParameterHandler):
         """The device VCD loop (tomography_model.py:2699-3013).  The loop
         state -- recon, resident error sinogram, Hessian -- stays on the
         device; one host synchronization per iteration reads the stats."""
-        if prox_input is not None:
-            raise NotImplementedError('the proximal-map prior is not implemented on the '
-                                      'sm_100a path yet')
         from .vcd_run import VcdRun
         run = VcdRun(self, sinogram, partitions, partition_sequence, stop_threshold_change_pct,
                      weights=weights, init_recon=init_recon,
                      init_error_sinogram=init_error_sinogram, fm_hessian=fm_hessian,
-                     first_iteration=first_iteration).run()
+                     first_iteration=first_iteration, prox_input=prox_input).run()
         if return_checkpoint:
             return run.recon3d(), run.losses(), run.checkpoint()
         return run.recon3d(), run.losses()
+
+    def prox_map(self, prox_input, sinogram, sigma_prox=None, weights=None, init_recon=None,
+                 do_initialization=True, stop_threshold_change_pct=0.2, max_iterations=3,
+                 first_iteration=0, logfile_path='~/.mbirtorch/logs/prox.log', print_logs=True,
+                 output_sharded=False):
+        """Proximal map for Plug-and-Play (tomography_model.py:3251-3373): a
+        reconstruction whose prior is Gaussian with mean ``prox_input`` and
+        standard deviation ``sigma_prox`` (automatic from the sinogram when
+        None).  ``do_initialization=False`` reuses the partitions and
+        regularization of the previous call on this model.  The pixel
+        partitions are drawn from numpy's global random generator.  Returns
+        (recon, recon_dict)."""
+        if do_initialization or self.prox_data is None:
+            (sinogram, weights, init_recon, partitions, seq, granularity,
+             reg) = self.initialize_recon(sinogram, weights, init_recon, max_iterations,
+                                          first_iteration, logfile_path=logfile_path,
+                                          print_logs=print_logs)
+            self.prox_data = (partitions, seq, granularity, reg)
+        else:
+            partitions, seq, granularity, reg = self.prox_data
+            if self.log_buffer is None:
+                self.setup_logger(logfile_path=logfile_path, print_logs=print_logs)
+        own_sigma_prox = self.get_params('sigma_prox')
+        if sigma_prox is not None:
+            reg = dict(reg, sigma_prox=sigma_prox)
+            self.set_params(no_warning=True, sigma_prox=sigma_prox,
+                            auto_regularize_flag=self.get_params('auto_regularize_flag'))
+        try:
+            with torch.no_grad():
+                recon, losses = self._vcd_recon(sinogram, partitions, seq,
+                                                stop_threshold_change_pct, weights=weights,
+                                                init_recon=init_recon, prox_input=prox_input,
+                                                first_iteration=first_iteration)
+        finally:
+            self.set_params(no_warning=True, sigma_prox=own_sigma_prox)
+        fm_rmse = [float(v) for v in losses[0]]
+        recon_params = dict(zip(recon_param_names, [
+            len(fm_rmse), granularity, [int(v) for v in seq], fm_rmse, [0], reg,
+            [100 * float(v) for v in losses[2]], [float(v) for v in losses[3]],
+            [[float(x) for x in row] for row in losses[4]]]))
+        if logfile_path:
+            self.logger.info('Logs written to {}'.format(
+                os.path.abspath(os.path.expanduser(logfile_path))))
+        for h in list(self.logger.handlers):
+            h.flush()
+        self.close_log_file()
+        notes = 'Proximal map completed: {}\n\n'.format(datetime.datetime.now())
+        recon_dict = self.get_recon_dict(recon_params, notes=notes)
+        return self._out(recon, output_sharded), recon_dict
 
     # ── model description ───────────────────────────────────────────────────
     def get_recon_dict(self, recon_params=None, notes=None, save_log=True, save_model=True,

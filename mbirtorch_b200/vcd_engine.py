@@ -77,7 +77,10 @@ class ResidentSinogram:
         return self.data.numel() * self.data.element_size() + self.scale.numel() * 4
 
 
-def make_vcd_params(fm_constant, sigma_x, p, q, T, b, max_alpha, positivity, storage):
+def make_vcd_params(fm_constant, sigma_x, p, q, T, b, max_alpha, positivity, storage,
+                    prox_constant=0.0, prox_input_ptr=None):
+    """``mbir_vcd_params``; a proximal-map prior is given by the device
+    pointer of its (N*N, S) float32 mean and 1 / sigma_prox^2."""
     prm = VcdParams()
     prm.fm_constant = float(fm_constant)
     prm.sigma_x = float(sigma_x)
@@ -87,6 +90,9 @@ def make_vcd_params(fm_constant, sigma_x, p, q, T, b, max_alpha, positivity, sto
     prm.max_alpha = float(max_alpha)
     prm.positivity = int(bool(positivity))
     prm.storage = int(storage)
+    prm.prox_constant = float(prox_constant)
+    prm.reserved = 0
+    prm.prox_input = prox_input_ptr
     return prm
 
 

@@ -35,7 +35,7 @@ class VcdRun:
     def __init__(self, model, sinogram, partitions, partition_sequence,
                  stop_threshold_change_pct, weights=None, init_recon=None,
                  init_error_sinogram=None, fm_hessian=None, rng=None, first_iteration=0,
-                 stream=None):
+                 stream=None, prox_input=None):
         model.verify_valid_params()
         model._require_cuda()
         self.model = model
@@ -52,6 +52,7 @@ class VcdRun:
         self.init_recon = init_recon
         self.init_error_sinogram = init_error_sinogram
         self.fm_hessian = fm_hessian
+        self.prox_input = prox_input
         self.partitions = partitions
         self.seq = np.asarray(partition_sequence)
         self.stop_pct = stop_threshold_change_pct
@@ -137,7 +138,9 @@ class VcdRun:
         self.parts_dev = [torch.as_tensor(np.ascontiguousarray(p), dtype=torch.int64, device=dev)
                           for p in self.partitions]
         max_ps = max((int(self.partitions[int(i)].shape[1]) for i in self.seq), default=1)
-        self.engine = m._make_engine(H, self.w_res, self.storage, max_subset_pixels=max_ps)
+        self.prox_flat = m._prox_flat(self.prox_input)
+        self.engine = m._make_engine(H, self.w_res, self.storage, max_subset_pixels=max_ps,
+                                     prox_flat=self.prox_flat)
         self.host = torch.empty(2 + self.recon_shape[2] + 4, dtype=torch.float64,
                                 pin_memory=True)
         log.info('Starting VCD iterations')

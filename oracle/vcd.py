@@ -173,8 +173,13 @@ class SubsetUpdater:
 
     def __init__(self, prob, fm_hessian_flat, weights, sigma_y, sigma_x,
                  p=2.0, q=1.2, T=1.0, nbr_wts=(1.0, 1.0, 1.0), max_alpha=1.5,
-                 positivity=False, dc_profile=None):
+                 positivity=False, dc_profile=None, prox_input=None, sigma_prox=None):
+        """With ``prox_input`` ((N*N, S)) the prior is the proximal map's:
+        gradient (x - v) / sigma_prox^2 and Hessian 1 / sigma_prox^2
+        (qggmrf.py:186-206, tomography_model.py:2525-2537)."""
         self.prob = prob
+        self.prox = None if prox_input is None else np.asarray(prox_input, np.float64)
+        self.prox_c = None if prox_input is None else 1.0 / sigma_prox ** 2
         self.H = np.asarray(fm_hessian_flat, dtype=np.float64)
         self.w = None if weights is None else np.asarray(weights, np.float64)
         self.fm_c = 1.0 / sigma_y ** 2
@@ -194,9 +199,13 @@ class SubsetUpdater:
 
     def __call__(self, flat_recon, error, idx):
         prob, fm_c = self.prob, self.fm_c
-        g_p, h_p = gradient_and_hessian(flat_recon, prob.recon_shape, idx,
-                                        self.b, self.sigma_x, self.p, self.q,
-                                        self.T)
+        if self.prox is not None:
+            g_p = self.prox_c * (flat_recon[idx] - self.prox[idx])
+            h_p = self.prox_c
+        else:
+            g_p, h_p = gradient_and_hessian(flat_recon, prob.recon_shape, idx,
+                                            self.b, self.sigma_x, self.p, self.q,
+                                            self.T)
         ew = error if self.w is None else self.w * error
         g_f = -fm_c * prob.back(ew, idx)
         h_f = fm_c * self.H[idx]
@@ -246,7 +255,7 @@ def hessian_diagonal(prob, weights, sino_shape):
 
 def recon(prob, sino, sigma_y, sigma_x, partitions, seq, weights=None,
           init_recon=None, dc_profile=None, max_alpha=1.5, positivity=False,
-          p=2.0, q=1.2, T=1.0, nbr_wts=(1.0, 1.0, 1.0)):
+          p=2.0, q=1.2, T=1.0, nbr_wts=(1.0, 1.0, 1.0), prox_input=None, sigma_prox=None):
     """FP64 VCD recon.  ``partitions`` must be drawn by the caller, and the
     global np.random state must be where the reference leaves it after the
     partitions: each iteration draws one subset permutation from it.
@@ -259,9 +268,12 @@ def recon(prob, sino, sigma_y, sigma_x, partitions, seq, weights=None,
         init_recon = direct_recon(prob, sino)
     error, flat = initial_state(prob, sino, init_recon, weights, scale)
     H = hessian_diagonal(prob, weights, sino.shape)
+    prox_flat = None if prox_input is None else \
+        np.asarray(prox_input, np.float64).reshape(-1, prob.recon_shape[2])
     upd = SubsetUpdater(prob, H, weights, sigma_y, sigma_x, p=p, q=q, T=T,
                         nbr_wts=nbr_wts, max_alpha=max_alpha,
-                        positivity=positivity, dc_profile=dc_profile)
+                        positivity=positivity, dc_profile=dc_profile,
+                        prox_input=prox_flat, sigma_prox=sigma_prox)
     N = sino.size
     avg_w = 1.0 if weights is None else float(np.mean(weights))
     stats = {'fm_rmse': [], 'nmae': [], 'alpha': []}

@@ -20,6 +20,11 @@ Cases
   autoreg.npz       auto_set_regularization_params on phantom sinograms
   direct.npz        recon_direct (FBP, FDK, helical FDK)
   recon_*.npz       seeded VCD recon traces (parallel, cone, weighted)
+  prox_*.npz        seeded prox_map (proximal-map prior) traces, parallel
+                    (automatic sigma_prox) and cone (given sigma_prox)
+
+Pass case-function names to regenerate only those, e.g.
+    PYTHONPATH=/root/reference python tests/golden/make_golden.py prox_cases
 """
 
 import json
@@ -323,9 +328,39 @@ def recon_cases():
     print('wrote recons')
 
 
+def prox_cases():
+    # prox_map on a smoothed, perturbed phantom as the proximal input.
+    m, ang, ph, sino = _parallel_data(41)
+    rng = np.random.default_rng(43)
+    v = (ph + rng.normal(0, 0.05, ph.shape)).astype(np.float32)
+    np.random.seed(11)
+    rec, d = m.prox_map(v, sino, max_iterations=3, stop_threshold_change_pct=0,
+                        logfile_path=None, print_logs=False)
+    rp = d['recon_params']
+    np.savez_compressed(os.path.join(HERE, 'prox_parallel.npz'), sino=sino, angles=ang,
+                        prox_input=v, recon=rec, fm_rmse=np.array(rp['fm_rmse']),
+                        alpha=np.array(rp['alpha_values']),
+                        reg=np.array([rp['regularization_params'][k]
+                                      for k in ('sigma_y', 'sigma_x', 'sigma_prox')]),
+                        sigma_prox=np.array(np.nan), seed=np.array(11), max_iterations=np.array(3))
+    mc, ang, zsh, ph, s = _cone_data(42)
+    v = (ph + rng.normal(0, 0.05, ph.shape)).astype(np.float32)
+    np.random.seed(12)
+    rec, d = mc.prox_map(v, s, sigma_prox=0.05, max_iterations=3, stop_threshold_change_pct=0,
+                         logfile_path=None, print_logs=False)
+    rp = d['recon_params']
+    np.savez_compressed(os.path.join(HERE, 'prox_cone.npz'), sino=s, angles=ang,
+                        z_shifts=np.zeros_like(ang), prox_input=v, recon=rec,
+                        fm_rmse=np.array(rp['fm_rmse']), alpha=np.array(rp['alpha_values']),
+                        reg=np.array([rp['regularization_params'][k]
+                                      for k in ('sigma_y', 'sigma_x', 'sigma_prox')]),
+                        sigma_prox=np.array(0.05), seed=np.array(12), max_iterations=np.array(3))
+    print('wrote prox')
+
+
+CASES = ['projector_cases', 'qggmrf_case', 'partition_case', 'autoreg_and_direct_cases',
+         'recon_cases', 'prox_cases']
+
 if __name__ == '__main__':
-    projector_cases()
-    qggmrf_case()
-    partition_case()
-    autoreg_and_direct_cases()
-    recon_cases()
+    for name in (sys.argv[1:] or CASES):
+        globals()[name]()

@@ -24,7 +24,7 @@ def _declared_functions():
 
 def test_library_builds_and_loads():
     lib = _lib.load()
-    assert lib.mbir_abi_version() == 10000
+    assert lib.mbir_abi_version() == 10100
     assert os.path.exists(_lib.library_path())
 
 
@@ -39,7 +39,7 @@ def test_every_declared_symbol_is_exported_and_bound():
 
 def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.Geometry) == 10 * 4 + 10 * 4
-    assert ctypes.sizeof(_lib.VcdParams) == 12 * 4 + 2 * 4
+    assert ctypes.sizeof(_lib.VcdParams) == 12 * 4 + 2 * 4 + 2 * 4 + 8
 
 
 def _geom(**kw):

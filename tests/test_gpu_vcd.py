@@ -247,3 +247,45 @@ def test_sixteen_bit_view_scales_are_powers_of_two():
     r = ResidentSinogram.from_vrc(s, 1)
     assert np.all(r.scale.cpu().numpy() == 1)
     assert rel_l2(r.to_vrc().cpu().numpy(), s.cpu().numpy()) <= 4e-3
+
+
+@pytest.mark.parametrize("name", ["prox_parallel", "prox_cone"])
+def test_prox_map_matches_reference_and_oracle(name):
+    """prox_map (proximal-map prior) against the reference's seeded run and
+    the FP64 oracle."""
+    from oracle import vcd as ovcd
+    d = load_golden(f'{name}.npz')
+    V = d['sino'].shape[0]
+    if name == 'prox_parallel':
+        m = mb.ParallelBeamModel(d['sino'].shape, np.linspace(0, np.pi, V, endpoint=False))
+        sigma_prox = None
+    else:
+        m = mb.ConeBeamModel(d['sino'].shape, np.linspace(0, 2 * np.pi, V, endpoint=False),
+                             64.0, 32.0)
+        sigma_prox = float(d['sigma_prox'])
+    m.set_params(no_warning=True, verbose=0)
+    np.random.seed(int(d['seed']))
+    rec, rd = m.prox_map(d['prox_input'], d['sino'], sigma_prox=sigma_prox,
+                         max_iterations=int(d['max_iterations']), stop_threshold_change_pct=0,
+                         logfile_path=None, print_logs=False)
+    rp = rd['recon_params']
+    assert rel_l2(rec, d['recon']) <= 1e-4
+    np.testing.assert_allclose(rp['fm_rmse'], d['fm_rmse'], rtol=1e-4)
+    np.testing.assert_allclose(rp['alpha_values'], d['alpha'], rtol=1e-4)
+    np.testing.assert_allclose(rp['regularization_params']['sigma_prox'], d['reg'][2],
+                               rtol=1e-6)
+    prob = _oracle_problem(m)
+    np.random.seed(int(d['seed']))
+    parts = [ovcd.pixel_partition(prob.recon_shape, n) for n in GRANULARITY]
+    seq = ovcd.partition_sequence(SEQUENCE, int(d['max_iterations']))
+    dc = ovcd.dc_damping_profile(prob) if name == 'prox_cone' else None
+    orec, _ = ovcd.recon(prob, d['sino'], d['reg'][0], d['reg'][1], parts, seq, dc_profile=dc,
+                         prox_input=d['prox_input'], sigma_prox=float(d['reg'][2]))
+    assert rel_l2(rec, orec) <= 1e-4
+    # a second call reusing the first call's partitions and regularization
+    rec2, _ = m.prox_map(rec, d['sino'], sigma_prox=sigma_prox, do_initialization=False,
+                         max_iterations=1, logfile_path=None, print_logs=False)
+    assert np.isfinite(rec2).all() and rec2.shape == rec.shape
+    with pytest.raises(ValueError, match='prox_input'):
+        m.prox_map(d['prox_input'][:, :, :2], d['sino'], max_iterations=1, logfile_path=None,
+                   print_logs=False)

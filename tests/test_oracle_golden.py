@@ -158,3 +158,24 @@ def test_cone_recon_matches_reference(name, tag):
     assert rel_l2(rec, d['recon']) < 1e-4
     np.testing.assert_allclose(st['fm_rmse'], d['fm_rmse'], rtol=1e-4)
     np.testing.assert_allclose(st['alpha'], d['alpha'], rtol=1e-4)
+
+
+@pytest.mark.parametrize("name", ["prox_parallel", "prox_cone"])
+def test_prox_map_matches_reference(name):
+    """prox_map's proximal-map prior: the reference's seeded run (automatic
+    sigma_prox for parallel, a given one for cone) against the oracle."""
+    d = load_golden(f'{name}.npz')
+    sino = d['sino']
+    if name == 'prox_parallel':
+        prob, dc = _parallel_problem(sino, d['angles']), None
+    else:
+        prob = _cone_problem(load_golden('direct.npz'), 'cone', sino, d['angles'], d['z_shifts'])
+        dc = vcd.dc_damping_profile(prob)
+    np.random.seed(int(d['seed']))
+    parts = [vcd.pixel_partition(prob.recon_shape, n) for n in GRANULARITY]
+    seq = vcd.partition_sequence(SEQUENCE, int(d['max_iterations']))
+    rec, st = vcd.recon(prob, sino, d['reg'][0], d['reg'][1], parts, seq, dc_profile=dc,
+                        prox_input=d['prox_input'], sigma_prox=float(d['reg'][2]))
+    assert rel_l2(rec, d['recon']) < 1e-4
+    np.testing.assert_allclose(st['fm_rmse'], d['fm_rmse'], rtol=1e-4)
+    np.testing.assert_allclose(st['alpha'], d['alpha'], rtol=1e-4)
