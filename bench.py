@@ -438,6 +438,7 @@ def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd):
     m.set_storage_precision(args.storage)
     res["mixed_precision"] = mp
     res["serving"] = serving_extra(mb, torch, y_host, rec_ref)
+    res["serving_mix"] = serving_mix_extra(mb, torch)
     res["fm_rmse_final"] = rd["recon_params"]["fm_rmse"][-1]
     # ── CPU baseline ──
     try:
@@ -475,6 +476,103 @@ def serving_extra(mb, torch, y_host, rec_ref, jobs=4):
                 "rel_l2_job0_vs_f32_recon": float((r0 - ref).norm() / ref.norm()),
                 "failed": st["failed"]})
     return out
+
+
+def mix_jobs(mb, torch, n_jobs=16, seed=7):
+    """A seeded sample of the serving mix, scaled to run in seconds: 40%
+    parallel, 40% cone, 20% helical cone (2 turns); slices in {16, 64},
+    in-plane size in {128, 256}, views in {180, 360}, channels 1.5x the
+    in-plane size, rows = slices; ellipsoid phantoms with Poisson noise
+    at I0 = 1e4 (largest line integral scaled to 3).  Returns
+    [(model factory, sinogram, seed)]."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(n_jobs):
+        kind = rng.choice(["parallel", "cone", "helical"], p=[0.4, 0.4, 0.2])
+        S, N, Vj = int(rng.choice([16, 64])), int(rng.choice([128, 256])), int(rng.choice([180, 360]))
+        Cj = int(1.5 * N)
+
+        def make(kind=kind, S=S, N=N, Vj=Vj, Cj=Cj):
+            if kind == "parallel":
+                mj = mb.ParallelBeamModel((Vj, S, Cj), np.linspace(0, np.pi, Vj, endpoint=False))
+            else:
+                turns = 2 if kind == "helical" else 1
+                ang = np.linspace(0, 2 * np.pi * turns, Vj, endpoint=False)
+                zs = np.linspace(-S / 4, S / 4, Vj) if kind == "helical" else None
+                mj = mb.ConeBeamModel((Vj, S, Cj), ang, source_detector_dist=4.0 * N,
+                                      source_iso_dist=2.0 * N, helical_z_shifts=zs)
+                mj.set_params(no_warning=True, delta_det_channel=2.0, delta_det_row=2.0)
+                mj.auto_set_recon_geometry(no_warning=True)
+            mj.set_params(no_warning=True, verbose=0, recon_shape=(N, N, S))
+            return mj
+
+        mj = make()
+        rs = mj.get_params("recon_shape")
+        g = np.linspace(-1, 1, N, dtype=np.float32)
+        X, Y = np.meshgrid(g, g)
+        z = np.linspace(-1, 1, S, dtype=np.float32)
+        vol = np.zeros(rs, np.float32)
+        for _ in range(6):
+            c, a = rng.uniform(-0.4, 0.4, 3), rng.uniform(0.1, 0.4, 3)
+            inside = ((X - c[0]) / a[0]) ** 2 + ((Y - c[1]) / a[1]) ** 2
+            vol += np.float32(rng.uniform(0.2, 1.0)) * (
+                (inside[:, :, None] + ((z - c[2]) / a[2]) ** 2) <= 1)
+        clean = mj.forward_project(vol)
+        mu = 3.0 / max(float(clean.max()), 1e-6)
+        counts = rng.poisson(I0 * np.exp(-mu * clean))
+        sino = (-np.log(np.maximum(counts, 1) / I0) / mu).astype(np.float32)
+        jobs.append((make, sino, 1000 + j))
+    return jobs
+
+
+def serving_mix_extra(mb, torch, n_jobs=16):
+    """The north-star comparison on a sample of the serving mix: the plain
+    form (each job alone, FP32, one after another through model.recon) vs
+    the served form (all jobs submitted at once to a ReconServer with
+    float16 storage: resident, admitted against the memory ledger, advancing
+    concurrently).  Both with 10 VCD iterations and the same per-job seeds,
+    so each served result is compared with its own plain result."""
+    from mbirtorch_b200.serving import ReconServer
+    jobs = mix_jobs(mb, torch, n_jobs)
+    iters = 10
+
+    def plain():
+        out = []
+        t0 = time.perf_counter()
+        for make, sino, seed in jobs:
+            mj = make()
+            np.random.seed(seed)
+            r, _ = mj.recon(sino, max_iterations=iters, stop_threshold_change_pct=0,
+                            logfile_path=None, print_logs=False)
+            out.append(r)
+        return out, time.perf_counter() - t0
+
+    def served():
+        srv = ReconServer(storage_dtype="float16", max_active=8)
+        t0 = time.perf_counter()
+        reqs = [srv.submit(make(), sino, max_iterations=iters, seed=seed, arrival=t0)
+                for make, sino, seed in jobs]
+        srv.run_until_idle(timeout_s=600)
+        return reqs, time.perf_counter() - t0, srv.stats()
+
+    plain()        # warm-up (library load, allocator)
+    served()
+    ref, t_plain = plain()
+    reqs, t_srv, st = served()
+    rel = [float(np.linalg.norm(r.recon.astype(np.float64) - p) / np.linalg.norm(p))
+           for r, p in zip(reqs, ref)]
+    kinds = {}
+    for make, _, _ in jobs:
+        k = type(make()).__name__
+        kinds[k] = kinds.get(k, 0) + 1
+    return {"jobs": n_jobs, "iterations": iters, "models": kinds,
+            "plain_f32_recons_per_s": n_jobs / t_plain,
+            "served_f16_recons_per_s": n_jobs / t_srv,
+            "served_over_plain": t_plain / t_srv,
+            "served_p50_latency_s": st["p50_latency_s"],
+            "served_p99_latency_s": st["p99_latency_s"],
+            "max_concurrent": st["max_concurrent"], "failed": st["failed"],
+            "max_rel_l2_served_vs_plain": max(rel)}
 
 
 def main_reference(args, rank, world):

@@ -427,6 +427,7 @@ int fwd_blocks(const mbir_geometry *g, int band, int v_count) {
 // ── VCD workspace ─────────────────────────────────────────────────────────
 struct VcdWs {
   float *grad_part, *delta, *gbuf, *hinv, *gpbuf, *hpbuf, *alpha;
+  unsigned int *counters;  // [0] spare, [1] recon-update CTAs (last-CTA election)
   double *dc_sums, *prior_part, *fwd_part, *sq_part, *l1_part;
   void *ad;
   FwdBins bins;  // binned cone forward (used when `binned`)
@@ -464,6 +465,7 @@ VcdWs vcd_layout(const mbir_geometry *g, long long Ps, const mbir_vcd_params *pr
   w.sq_part = c.take<double>((size_t)w.upd_chunks * S);
   w.l1_part = c.take<double>((size_t)w.upd_chunks * w.upd_yblocks);
   w.alpha = c.take<float>(4);
+  w.counters = c.take<unsigned int>(2);
   w.ad = c.take<char>((size_t)V * g->num_det_channels * g->num_det_rows * storage_size(prm->storage));
   w.binned = use_cone_rt(g);
   w.bins = FwdBins{nullptr, nullptr, nullptr, nullptr, 0};
@@ -533,6 +535,7 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
     MBIR_CHECK_LAUNCH("vcd DC direction");
   }
   // 3. forward A delta + line-search partials
+  // 3. forward A delta + line-search partials
   LineSearchEpi<T> epi{err, es, wts, wsc, static_cast<T *>(w.ad), C, R, w.fwd_part, 1, 0.0, 0.0};
   if (w.binned)
     rc = run_forward_binned(g, vp, w.delta, Ps, S, pix, w.bins, !shared_bins, epi, st,
@@ -562,12 +565,9 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   dim3 gu(w.upd_chunks, w.upd_yblocks);
   tpre(st);
   vcd_pixel_update_kernel<<<gu, kThreads, 0, st>>>((int)Ps, S, kUpdChunk, pix, w.delta, w.alpha,
-                                                   flat, w.sq_part, w.l1_part);
+                                                   flat, w.sq_part, w.l1_part, w.counters + 1,
+                                                   accum);
   MBIR_CHECK_LAUNCH("vcd pixel update");
-  tpre(st);
-  vcd_finish_kernel<<<1, kThreads, 0, st>>>(S, w.upd_chunks, w.upd_chunks * w.upd_yblocks,
-                                            w.sq_part, w.l1_part, w.alpha, accum);
-  MBIR_CHECK_LAUNCH("vcd finish");
   if (w.binned) {
     // Only the (view, channel-block) tiles the subset reached: elsewhere
     // A delta is zero and e is unchanged.
@@ -902,13 +902,16 @@ size_t mbir_vcd_workspace_size(const mbir_geometry *geom, int64_t max_subset_pix
   return vcd_layout(geom, max_subset_pixels, params, nullptr).bytes;
 }
 
-int32_t mbir_vcd_subset_update(const mbir_geometry *geom, const float *view_params,
-                               const mbir_vcd_params *params, float *flat_recon, void *error_sino,
-                               const float *err_scale, const void *weights,
-                               const float *w_scale, const float *fm_hessian,
-                               const float *dc_profile, const int64_t *pixel_indices,
-                               int64_t num_pixels, double *accum, float *alpha_out,
-                               void *workspace, size_t workspace_bytes, void *stream) {
+namespace {
+// One subset update; `fresh` zeroes the workspace's last-CTA counters first
+// (the elected CTAs leave them at zero, so a partition pass zeroes them once).
+int32_t subset_update(const mbir_geometry *geom, const float *view_params,
+                      const mbir_vcd_params *params, float *flat_recon, void *error_sino,
+                      const float *err_scale, const void *weights, const float *w_scale,
+                      const float *fm_hessian, const float *dc_profile,
+                      const int64_t *pixel_indices, int64_t num_pixels, double *accum,
+                      float *alpha_out, void *workspace, size_t workspace_bytes, void *stream,
+                      bool fresh) {
   int rc = validate_vcd(geom, params, flat_recon, error_sino, err_scale, weights, w_scale,
                         fm_hessian, num_pixels);
   if (rc) return rc;
@@ -918,6 +921,11 @@ int32_t mbir_vcd_subset_update(const mbir_geometry *geom, const float *view_para
     return fail(MBIR_ERR_WORKSPACE, "VCD workspace of %zu bytes < %zu needed", workspace_bytes,
                 w.bytes);
   cudaStream_t st = as_stream(stream);
+  if (fresh) {
+    const cudaError_t e = cudaMemsetAsync(w.counters, 0, 2 * sizeof(unsigned int), st);
+    if (e != cudaSuccess)
+      return fail(MBIR_ERR_CUDA, "VCD counter reset failed: %s", cudaGetErrorString(e));
+  }
   switch (params->storage) {
     case MBIR_F32:
       return vcd_subset_t<float>(geom, view_params, params, flat_recon,
@@ -937,6 +945,19 @@ int32_t mbir_vcd_subset_update(const mbir_geometry *geom, const float *view_para
                                   dc_profile, pixel_indices, num_pixels, accum, alpha_out, w, st);
   }
 }
+}  // namespace
+
+int32_t mbir_vcd_subset_update(const mbir_geometry *geom, const float *view_params,
+                               const mbir_vcd_params *params, float *flat_recon, void *error_sino,
+                               const float *err_scale, const void *weights,
+                               const float *w_scale, const float *fm_hessian,
+                               const float *dc_profile, const int64_t *pixel_indices,
+                               int64_t num_pixels, double *accum, float *alpha_out,
+                               void *workspace, size_t workspace_bytes, void *stream) {
+  return subset_update(geom, view_params, params, flat_recon, error_sino, err_scale, weights,
+                       w_scale, fm_hessian, dc_profile, pixel_indices, num_pixels, accum,
+                       alpha_out, workspace, workspace_bytes, stream, true);
+}
 
 int32_t mbir_vcd_partition_pass(const mbir_geometry *geom, const float *view_params,
                                 const mbir_vcd_params *params, float *flat_recon, void *error_sino,
@@ -951,10 +972,10 @@ int32_t mbir_vcd_partition_pass(const mbir_geometry *geom, const float *view_par
     if (order[i] < 0 || order[i] >= num_subsets)
       return fail(MBIR_ERR_INVALID, "order[%d] = %d outside [0, %d)", i, order[i], num_subsets);
   for (int i = 0; i < num_subsets; ++i) {
-    const int rc = mbir_vcd_subset_update(
+    const int rc = subset_update(
         geom, view_params, params, flat_recon, error_sino, err_scale, weights, w_scale,
         fm_hessian, dc_profile, partition + (size_t)order[i] * subset_pixels, subset_pixels, accum,
-        nullptr, workspace, workspace_bytes, stream);
+        nullptr, workspace, workspace_bytes, stream, i == 0);
     if (rc) return rc;
   }
   return MBIR_OK;

@@ -15,7 +15,8 @@
 //   4. alpha         one CTA: FP64 reduction of all partials, the clamped
 //                    step (tomography_model.py:2612-2617)
 //   5. update        recon += alpha delta with per-slice sum of squares and
-//                    ell1, then e -= alpha Ad
+//                    ell1 (the last CTA folds them into the accumulators),
+//                    then e -= alpha Ad
 // Every reduction is a fixed-order tree over per-CTA partials, so a subset
 // update is bit-reproducible run to run.
 #pragma once
@@ -223,6 +224,24 @@ vcd_dc_direction_kernel(int P, int S, int nchunks, const double *__restrict__ su
   }
 }
 
+// Grid-wide "last CTA" election: every CTA calls it once after writing its
+// partials; it returns true in exactly one CTA (the last to arrive), which
+// then sees every other CTA's writes.  The counter counts `total` arrivals
+// (possibly over several launches in stream order) and the elected CTA
+// resets it to zero.
+__device__ __forceinline__ bool last_cta(unsigned int *counter, unsigned int total) {
+  __shared__ bool s_last;
+  __threadfence();  // this thread's partial writes, before the arrival
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == total - 1u;
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last;
+}
+
 // ── 3. forward epilogue: line search + Ad store ───────────────────────────
 // The per-view scale is a power of two, so Ad / scale is formed exactly as
 // Ad * (1 / scale).
@@ -395,7 +414,8 @@ __global__ void __launch_bounds__(kThreads)
 vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pix,
                         const float *__restrict__ delta, const float *__restrict__ alpha,
                         float *__restrict__ flat, double *__restrict__ sq_part,
-                        double *__restrict__ l1_part) {
+                        double *__restrict__ l1_part, unsigned int *__restrict__ counter,
+                        double *__restrict__ accum) {
   const int l = blockIdx.y * kThreads + threadIdx.x;
   const int chunk = blockIdx.x;
   const int p0 = chunk * pchunk, p1 = min(P, p0 + pchunk);
@@ -428,26 +448,25 @@ vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pi
   double dummy = 0.0;
   block_sum2(l1, dummy);
   if (threadIdx.x == 0) l1_part[(size_t)blockIdx.y * gridDim.x + chunk] = l1;
-}
-
-// accum[0] += ell1, accum[1] += alpha, accum[2 + l] += sum_p ds^2.
-__global__ void __launch_bounds__(kThreads)
-vcd_finish_kernel(int S, int nchunks, int nl1, const double *__restrict__ sq_part,
-                  const double *__restrict__ l1_part, const float *__restrict__ alpha,
-                  double *__restrict__ accum) {
-  for (int l = threadIdx.x; l < S; l += kThreads) {
-    double s = 0.0;
+  // The last CTA folds all partials into the accumulators (fixed order):
+  // accum[0] += ell1, accum[1] += alpha, accum[2 + l] += sum_p ds^2.
+  if (last_cta(counter, gridDim.x * gridDim.y)) {
+    const int nchunks = gridDim.x, nl1 = gridDim.x * gridDim.y;
+    for (int ls = threadIdx.x; ls < S; ls += blockDim.x) {
+      double s2 = 0.0;
 #pragma unroll 8
-    for (int c = 0; c < nchunks; ++c) s += sq_part[(size_t)c * S + l];
-    accum[2 + l] += s;
-  }
-  double l1 = 0.0, dummy = 0.0;
+      for (int c = 0; c < nchunks; ++c) s2 += __ldcg(sq_part + (size_t)c * S + ls);
+      accum[2 + ls] += s2;
+    }
+    double t1 = 0.0, t2 = 0.0;
 #pragma unroll 4
-  for (int i = threadIdx.x; i < nl1; i += kThreads) l1 += l1_part[i];
-  block_sum2(l1, dummy);
-  if (threadIdx.x == 0) {
-    accum[0] += l1;
-    accum[1] += (double)alpha[0];
+    for (int i = threadIdx.x; i < nl1; i += blockDim.x) t1 += __ldcg(l1_part + i);
+    block_sum2(t1, t2);
+    if (threadIdx.x == 0) {
+      accum[0] += t1;
+      accum[1] += (double)alpha[0];
+      *counter = 0u;
+    }
   }
 }
 

@@ -132,6 +132,10 @@ class ReconServer:
         self._next_id = 0
         self.max_concurrent = 0
         self.deferred = 0   # admissions put off because the ledger was full
+        # Streams are reused from job to job: the caching allocator keeps its
+        # freed blocks per stream, so a fresh stream per job would grow the
+        # pool (synchronizing cudaMalloc calls) instead of reusing it.
+        self._streams = []
         self.t0 = None
 
     # ── requests ───────────────────────────────────────────────────────────
@@ -178,7 +182,7 @@ class ReconServer:
         seq = vcd_utils.gen_partition_sequence(m.get_params('partition_sequence'),
                                                r.max_iterations)
         m.auto_set_regularization_params(r.sinogram, weights=r.weights)
-        r._stream = torch.cuda.Stream(self.device)
+        r._stream = self._streams.pop() if self._streams else torch.cuda.Stream(self.device)
         r._run = VcdRun(m, r.sinogram, parts, seq, r.stop_pct, weights=r.weights, rng=rng,
                         stream=r._stream)
         self.ledger.take(peak)
@@ -215,6 +219,8 @@ class ReconServer:
                     r.recon = r._out.numpy().reshape(rs)
                     r.finished = time.perf_counter()
                     r._run = None
+                    self._streams.append(r._stream)
+                    r._stream = None
                     self.ledger.release(r._charge)
                     r._charge = 0
                     self.active.remove(r)
@@ -236,6 +242,10 @@ class ReconServer:
             except Exception as exc:  # a failing job frees its slot, others go on
                 r.error = exc
                 r.finished = time.perf_counter()
+                r._run = None
+                if r._stream is not None:
+                    self._streams.append(r._stream)
+                    r._stream = None
                 if r._charge:
                     self.ledger.release(r._charge)
                     r._charge = 0
