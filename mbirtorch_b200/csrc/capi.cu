@@ -292,7 +292,7 @@ int cone_rt_threads(const mbir_geometry *g) { return (g->num_det_rows + 31) / 32
 size_t cone_rt_smem(const mbir_geometry *g, int band) {
   const int nthr = cone_rt_threads(g);
   return sizeof(ConeFwdRec) * (size_t)fwd_cap(nthr) +
-         sizeof(float) * (size_t)kFwdEB * (band + 2 * kFwdVPad);
+         sizeof(float) * ((size_t)kFwdEB * (band + 2 * kFwdVPad) + (size_t)(kFwdCB + 4) * nthr);
 }
 
 template <typename EPI>

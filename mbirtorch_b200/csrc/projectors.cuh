@@ -551,24 +551,25 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
   epi.end(blockIdx.y * gridDim.x + blockIdx.x);
 }
 
-// ── forward projection, cone, register-tiled ───────────────────────────────
+// ── forward projection, cone, row-tiled ────────────────────────────────────
 // The cone forward for psf radius 1 and up to 1024 detector rows.  A CTA
-// owns one view and kFwdCB channels; thread m owns detector row m and keeps
-// the row's kFwdCB channel sums in registers.  Pixels reaching the block are
-// compacted as in forward_kernel, then processed in batches of kFwdEB: the
-// batch's cylinders, scaled by 1 / cos(phi) per slice, are staged in
-// zero-padded shared memory (one rsqrt per voxel), and every thread forms
-// its row's detector-side vertical fan from them (cone_beam.py:203-226)
-// and adds the three channel taps into registers.  The tap -> register map
-// depends on the pixel's centre channel, which is the same for all threads,
-// so it is a warp-uniform switch over compile-time register indices: no
-// shared-memory read-modify-write chains, no atomics, fixed summation order.
+// owns one view and kFwdCB channels; thread m owns detector row m and its
+// kFwdCB channel sums, held in a thread-private column of shared memory
+// (kFwdCB + 4 rows so that the three taps of any reaching pixel land
+// without a bounds test or a branch on the pixel's channel).  Pixels
+// reaching the block are compacted as in forward_kernel, then processed in
+// batches of kFwdEB: the batch's cylinders, scaled by 1 / cos(phi) per
+// slice, are staged in zero-padded shared memory (one rsqrt per voxel), and
+// every thread forms its row's detector-side vertical fan from them
+// (cone_beam.py:203-226) and adds the three channel taps.  No atomics; each
+// channel's sum is a fixed sequence of FMAs in pixel order.
 constexpr int kFwdCB = 16;   // channels per CTA
 constexpr int kFwdEB = 16;   // pixels staged per batch
 constexpr int kFwdVPad = 8;  // zero slices either side of a staged cylinder (>= 2 bp + 1)
 
-// Record capacity of one compaction round: at least one scan chunk.
-__host__ __device__ inline int fwd_cap(int nthr) { return nthr > 512 ? nthr : 512; }
+// Record capacity of one round (at least one scan chunk); the shared memory
+// also holds the stage and (kFwdCB + 4) accumulator rows per thread.
+__host__ __device__ inline int fwd_cap(int nthr) { return nthr > 256 ? nthr : 256; }
 
 __device__ __forceinline__ ConeFwdRec cone_fwd_record(const Geo &g, float ang, float z_off,
                                                       const ConeCenter &cc, int row) {
@@ -597,29 +598,17 @@ __device__ __forceinline__ void fwd_block_range(int ctr, int C, int &b_lo, int &
   }
 }
 
-template <int J>
-__device__ __forceinline__ void fwd_taps(float (&acc)[kFwdCB], float w0, float w1, float w2,
-                                         float det) {
-  // Case J: the pixel's centre channel is c0 + J - 1, so tap t lands on
-  // block channel J - 2 + t.
-  if (J - 2 >= 0 && J - 2 < kFwdCB) acc[(J - 2 >= 0 && J - 2 < kFwdCB) ? J - 2 : 0] =
-      fmaf(w0, det, acc[(J - 2 >= 0 && J - 2 < kFwdCB) ? J - 2 : 0]);
-  if (J - 1 >= 0 && J - 1 < kFwdCB) acc[(J - 1 >= 0 && J - 1 < kFwdCB) ? J - 1 : 0] =
-      fmaf(w1, det, acc[(J - 1 >= 0 && J - 1 < kFwdCB) ? J - 1 : 0]);
-  if (J >= 0 && J < kFwdCB) acc[(J >= 0 && J < kFwdCB) ? J : 0] =
-      fmaf(w2, det, acc[(J >= 0 && J < kFwdCB) ? J : 0]);
-}
-
 // The batches of one round: n records in shared memory, processed kFwdEB at
 // a time.  Staging writes the batch's cylinders, scaled by 1 / cos(phi) per
 // slice, into the zero-padded stage; then thread m forms detector row m's
-// vertical fan for every pixel of the batch and adds its three channel taps.
+// vertical fan for every pixel of the batch and adds its three channel taps
+// into its accumulator column acc_s[r * nthr + m], r = 0 .. kFwdCB + 3.
 // Every batch ends with all threads past a barrier.
-__device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec, int n, int c0,
+__device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec, int n,
                                              float *__restrict__ stage, int SP,
                                              const float *__restrict__ values, int band,
                                              int slice_start, float kc_lo, float kc_hi, int bp,
-                                             int R, float (&acc)[kFwdCB]) {
+                                             int R, int c0, float *__restrict__ acc_s) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   const float mf = (float)tid;
   for (int b0 = 0; b0 < n; b0 += kFwdEB) {
@@ -675,27 +664,14 @@ __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec,
             det = fmaf(a, st[ko], det);
           }
         }
-        const float w0 = rb.y, w1 = rb.z, w2 = rb.w;
-        switch (j) {
-          case 0: fwd_taps<0>(acc, w0, w1, w2, det); break;
-          case 1: fwd_taps<1>(acc, w0, w1, w2, det); break;
-          case 2: fwd_taps<2>(acc, w0, w1, w2, det); break;
-          case 3: fwd_taps<3>(acc, w0, w1, w2, det); break;
-          case 4: fwd_taps<4>(acc, w0, w1, w2, det); break;
-          case 5: fwd_taps<5>(acc, w0, w1, w2, det); break;
-          case 6: fwd_taps<6>(acc, w0, w1, w2, det); break;
-          case 7: fwd_taps<7>(acc, w0, w1, w2, det); break;
-          case 8: fwd_taps<8>(acc, w0, w1, w2, det); break;
-          case 9: fwd_taps<9>(acc, w0, w1, w2, det); break;
-          case 10: fwd_taps<10>(acc, w0, w1, w2, det); break;
-          case 11: fwd_taps<11>(acc, w0, w1, w2, det); break;
-          case 12: fwd_taps<12>(acc, w0, w1, w2, det); break;
-          case 13: fwd_taps<13>(acc, w0, w1, w2, det); break;
-          case 14: fwd_taps<14>(acc, w0, w1, w2, det); break;
-          case 15: fwd_taps<15>(acc, w0, w1, w2, det); break;
-          case 16: fwd_taps<16>(acc, w0, w1, w2, det); break;
-          default: fwd_taps<17>(acc, w0, w1, w2, det); break;
-        }
+        // Thread-private accumulator column in shared memory: row r holds
+        // channel c0 + r - 2, so tap t of centre slot j lands on row j + t
+        // (the same FMA sequence per channel as register accumulators, with
+        // no branch on the pixel's channel).
+        float *a = acc_s + j * nthr + tid;
+        a[0] = fmaf(rb.y, det, a[0]);
+        a[nthr] = fmaf(rb.z, det, a[nthr]);
+        a[2 * nthr] = fmaf(rb.w, det, a[2 * nthr]);
       }
     }
     __syncthreads();
@@ -713,6 +689,7 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
   const int SP = band + 2 * kFwdVPad;                     // staged cylinder pitch
   ConeFwdRec *rec = reinterpret_cast<ConeFwdRec *>(sm4);  // cap records
   float *stage = reinterpret_cast<float *>(rec + cap);    // kFwdEB x SP
+  float *acc_s = stage + kFwdEB * SP;                     // (kFwdCB + 4) x nthr
   __shared__ int s_wcount[32];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
@@ -731,9 +708,8 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
               kc_hi = (float)(slice_start + band + bp);
 
   for (int i = tid; i < kFwdEB * SP; i += nthr) stage[i] = 0.f;
-  float acc[kFwdCB];
 #pragma unroll
-  for (int j = 0; j < kFwdCB; ++j) acc[j] = 0.f;
+  for (int r = 0; r < kFwdCB + 4; ++r) acc_s[r * nthr + tid] = 0.f;
 
   int pos = 0;
   while (pos < P) {
@@ -765,9 +741,12 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
       pos += nthr;
       __syncthreads();
     }
-    fwd_rt_round(rec, n, c0, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, acc);
+    fwd_rt_round(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, c0, acc_s);
   }
   // Epilogue: thread m hands over its row's cells.
+  float acc[kFwdCB];
+#pragma unroll
+  for (int j = 0; j < kFwdCB; ++j) acc[j] = acc_s[(j + 2) * nthr + tid];
   epi.begin(vl);
   if (tid < g.R) epi.cells(vl, c0, ncb, tid, acc);
   epi.end(blockIdx.y * gridDim.x + blockIdx.x);
@@ -879,6 +858,7 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
   const int SP = band + 2 * kFwdVPad;
   ConeFwdRec *rec = reinterpret_cast<ConeFwdRec *>(sm4);
   float *stage = reinterpret_cast<float *>(rec + cap);
+  float *acc_s = stage + kFwdEB * SP;  // (kFwdCB + 4) x nthr
   const int nblk = gridDim.x, blk = blockIdx.x, vl = blockIdx.y;
   const int c0 = blk * kFwdCB;
   const int ncb = min(kFwdCB, g.C - c0);
@@ -900,16 +880,18 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
   }
 
   for (int i = tid; i < kFwdEB * SP; i += nthr) stage[i] = 0.f;
-  float acc[kFwdCB];
 #pragma unroll
-  for (int j = 0; j < kFwdCB; ++j) acc[j] = 0.f;
+  for (int r = 0; r < kFwdCB + 4; ++r) acc_s[r * nthr + tid] = 0.f;
   for (int base = start; base < end; base += cap) {
     const int n = min(cap, end - base);
     __syncthreads();
     for (int i = tid; i < n; i += nthr) rec[i] = vrec[vlist[base + i]];
     __syncthreads();
-    fwd_rt_round(rec, n, c0, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, acc);
+    fwd_rt_round(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, c0, acc_s);
   }
+  float acc[kFwdCB];
+#pragma unroll
+  for (int j = 0; j < kFwdCB; ++j) acc[j] = acc_s[(j + 2) * nthr + tid];
   epi.begin(v);
   if (tid < g.R) epi.cells(v, c0, ncb, tid, acc);
   epi.end(v * nblk + blk);
