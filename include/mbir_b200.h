@@ -282,6 +282,28 @@ int32_t mbir_vcd_partition_pass(const mbir_geometry *geom,
                                 double *accum, void *workspace,
                                 size_t workspace_bytes, void *stream);
 
+/* Workspace bytes for mbir_denoise_pass with subsets of subset_pixels
+ * pixels of an image with num_slices slices. */
+size_t mbir_denoise_workspace_size(int32_t num_slices, int64_t subset_pixels);
+
+/* One QGGMRF-denoiser iteration (QGGMRFDenoiser.denoise's inner loop and
+ * vcd_subset_denoiser, denoising.py:35-83 and :390-425): the identity
+ * forward model, so the residual image plays the error sinogram.  The
+ * subsets of `partition` (num_subsets, subset_pixels) int64 are updated in
+ * their stored order (the denoiser never reshuffles).
+ *   flat_image, flat_error   (num_rows * num_cols, num_slices) f32, updated
+ *                            in place (error = noisy image - image)
+ *   params                   fm_constant = 1 / sigma_noise^2, the qGGMRF
+ *                            scalars and max_alpha; storage, positivity and
+ *                            the proximal fields are ignored
+ *   accum                    device f64 [2], ADDED to: sum |alpha delta|,
+ *                            sum alpha over the subsets */
+int32_t mbir_denoise_pass(int32_t num_rows, int32_t num_cols, int32_t num_slices,
+                          const mbir_vcd_params *params, float *flat_image,
+                          float *flat_error, const int64_t *partition,
+                          int32_t num_subsets, int64_t subset_pixels, double *accum,
+                          void *workspace, size_t workspace_bytes, void *stream);
+
 /* Re-form the resident error sinogram from the measured one:
  * error = (y - A x) / err_scale[v] in `storage`, with y the FP32 sinogram
  * in the (V, C, R) layout and x the flat (N*N, S) recon at pixel_indices.

@@ -14,6 +14,7 @@ __version__ = "0.1.0"
 from .autograd import (TorchProjector, back_project_differentiable,  # noqa: F401
                        forward_project_differentiable, weighted_residual_loss)
 from .cone_beam import ConeBeamModel, recon_simple_cone  # noqa: F401
+from .denoising import QGGMRFDenoiser  # noqa: F401
 from .parallel_beam import ParallelBeamModel, recon_simple_parallel  # noqa: F401
 from .qggmrf import get_b_from_nbr_wts, qggmrf_loss  # noqa: F401
 from .tomography_model import TomographyModel  # noqa: F401
@@ -21,7 +22,8 @@ from .vcd_utils import (gen_full_indices, gen_partition_sequence, gen_pixel_part
                         gen_set_of_pixel_partitions, gen_weights, get_2d_ror_mask)
 
 __all__ = [
-    "ParallelBeamModel", "ConeBeamModel", "TomographyModel", "recon_simple_parallel",
+    "ParallelBeamModel", "ConeBeamModel", "TomographyModel", "QGGMRFDenoiser",
+    "recon_simple_parallel",
     "recon_simple_cone", "TorchProjector", "forward_project_differentiable",
     "back_project_differentiable", "weighted_residual_loss", "gen_weights",
     "gen_full_indices", "gen_pixel_partition", "gen_set_of_pixel_partitions",

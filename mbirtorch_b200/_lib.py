@@ -107,6 +107,9 @@ SIGNATURES = {
     "mbir_iteration_stats": (_i32, [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _i32, _vp, _i64,
                                     _vp, _vp, _sz, _vp]),
     "mbir_iteration_stats_workspace_size": (_sz, []),
+    "mbir_denoise_workspace_size": (_sz, [_i32, _i64]),
+    "mbir_denoise_pass": (_i32, [_i32, _i32, _i32, _PP, _vp, _vp, _vp, _i32, _i64, _vp, _vp,
+                                 _sz, _vp]),
 }
 
 _lib = None

@@ -981,6 +981,78 @@ int32_t mbir_vcd_partition_pass(const mbir_geometry *geom, const float *view_par
   return MBIR_OK;
 }
 
+namespace {
+struct DenoiseWs {
+  float *delta, *alpha;
+  double *prior, *fwd, *l1;
+  unsigned int *counter;
+  int blocks;
+  size_t bytes;
+};
+
+DenoiseWs denoise_layout(int S, long long Ps, void *base) {
+  DenoiseWs w;
+  const size_t n = (size_t)Ps * S;
+  w.blocks = (int)((n + kThreads - 1) / kThreads);
+  Carver c(base);
+  w.delta = c.take<float>(n);
+  w.prior = c.take<double>((size_t)w.blocks * 2);
+  w.fwd = c.take<double>((size_t)w.blocks * 2);
+  w.l1 = c.take<double>((size_t)w.blocks);
+  w.alpha = c.take<float>(4);
+  w.counter = c.take<unsigned int>(1);
+  w.bytes = c.used;
+  return w;
+}
+}  // namespace
+
+size_t mbir_denoise_workspace_size(int32_t num_slices, int64_t subset_pixels) {
+  if (num_slices <= 0 || subset_pixels <= 0) return 0;
+  return denoise_layout(num_slices, subset_pixels, nullptr).bytes;
+}
+
+int32_t mbir_denoise_pass(int32_t num_rows, int32_t num_cols, int32_t num_slices,
+                          const mbir_vcd_params *params, float *flat_image, float *flat_error,
+                          const int64_t *partition, int32_t num_subsets, int64_t subset_pixels,
+                          double *accum, void *workspace, size_t workspace_bytes,
+                          void *stream) {
+  if (num_rows <= 0 || num_cols <= 0 || num_slices <= 0)
+    return fail(MBIR_ERR_INVALID, "image sizes must be positive");
+  if (!params || !flat_image || !flat_error || !partition || !accum)
+    return fail(MBIR_ERR_INVALID, "NULL argument");
+  if (num_subsets <= 0 || subset_pixels <= 0)
+    return fail(MBIR_ERR_INVALID, "denoiser pass needs at least one non-empty subset");
+  if (!(params->sigma_x > 0.f) || !(params->fm_constant > 0.f) || !(params->T > 0.f))
+    return fail(MBIR_ERR_INVALID, "sigma_x, T and fm_constant must be positive");
+  const DenoiseWs w = denoise_layout(num_slices, subset_pixels, workspace);
+  if (!workspace || workspace_bytes < w.bytes)
+    return fail(MBIR_ERR_WORKSPACE, "denoiser workspace of %zu bytes < %zu needed",
+                workspace_bytes, w.bytes);
+  cudaStream_t st = as_stream(stream);
+  cudaError_t e = cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), st);
+  if (e != cudaSuccess)
+    return fail(MBIR_ERR_CUDA, "denoiser counter reset failed: %s", cudaGetErrorString(e));
+  const VcdScalars sc = make_scalars(*params);
+  for (int k = 0; k < num_subsets; ++k) {
+    const int64_t *pix = partition + (size_t)k * subset_pixels;
+    tpre(st);
+    denoise_direction_kernel<<<w.blocks, kThreads, 0, st>>>(
+        (int)subset_pixels, num_slices, pix, num_rows, num_cols, flat_image, flat_error, sc,
+        w.delta, w.prior, w.fwd);
+    MBIR_CHECK_LAUNCH("denoise direction");
+    tpre(st);
+    vcd_alpha_kernel<<<1, kAlphaThreads, 0, st>>>(w.prior, w.blocks, w.fwd, w.blocks, sc.fmc,
+                                                 sc.max_alpha, w.alpha, nullptr);
+    MBIR_CHECK_LAUNCH("denoise alpha");
+    tpre(st);
+    denoise_update_kernel<<<w.blocks, kThreads, 0, st>>>((int)subset_pixels, num_slices, pix,
+                                                         w.delta, w.alpha, flat_image,
+                                                         flat_error, w.l1, w.counter, accum);
+    MBIR_CHECK_LAUNCH("denoise update");
+  }
+  return MBIR_OK;
+}
+
 size_t mbir_iteration_stats_workspace_size(void) {
   return align_up(sizeof(double) * 3 * 148 * 4) + align_up(sizeof(double) * 148 * 4);
 }

@@ -98,6 +98,34 @@ __device__ __forceinline__ void block_sum2(double &a, double &b) {
   }
 }
 
+// qGGMRF surrogate gradient and Hessian of voxel (pixel, l) (qggmrf.py:
+// 117-183): the slice term with reflected ends, then the 4 clamped in-plane
+// neighbours.
+__device__ __forceinline__ void qggmrf_terms(const float *__restrict__ flat, int pixel, int l,
+                                             int S, int NR, int NC, const VcdScalars &sc,
+                                             float &g_p, float &h_p) {
+  const float *cyl = flat + (size_t)pixel * S;
+  const float xs = cyl[l];
+  const float dp = (l + 1 < S) ? __fsub_rn(cyl[l + 1], xs) : 0.f;  // delta[l+1]
+  const float dm = (l > 0) ? __fsub_rn(xs, cyl[l - 1]) : 0.f;      // delta[l]
+  const float bt_p = __fmul_rn(2.f, b_tilde(dp, sc));
+  const float bt_m = __fmul_rn(2.f, b_tilde(dm, sc));
+  g_p = __fadd_rn(__fmul_rn(-sc.b[4], __fmul_rn(bt_p, dp)),
+                  __fmul_rn(sc.b[5], __fmul_rn(bt_m, dm)));
+  h_p = __fadd_rn(__fmul_rn(sc.b[4], bt_p), __fmul_rn(sc.b[5], bt_m));
+  const int row = pixel / NC, col = pixel - (pixel / NC) * NC;
+  const int dr[4] = {1, -1, 0, 0}, dc[4] = {0, 0, 1, -1};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int rr = min(max(row + dr[k], 0), NR - 1);
+    const int cc = min(max(col + dc[k], 0), NC - 1);
+    const float d = __fsub_rn(xs, flat[((size_t)rr * NC + cc) * S + l]);
+    const float w = __fmul_rn(sc.two_b[k], b_tilde(d, sc));
+    g_p = __fadd_rn(g_p, __fmul_rn(w, d));
+    h_p = __fadd_rn(h_p, w);
+  }
+}
+
 // ── 2. direction ─────────────────────────────────────────────────────────
 // Thread per (pixel p, slice l).  DC = 0: writes delta and the prior
 // line-term partials.  DC = 1: writes g, 1/h, g_p, h_p for the damping pass.
@@ -129,26 +157,7 @@ vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int 
       g_p = __fmul_rn(sc.prox_c, __fsub_rn(xs, sc.prox[(size_t)pixel * S + l]));
       h_p = sc.prox_c;
     } else {
-      // qGGMRF surrogate (qggmrf.py:117-183): slice term with reflected
-      // ends, then the 4 clamped in-plane neighbours.
-      const float dp = (l + 1 < S) ? __fsub_rn(cyl[l + 1], xs) : 0.f;  // delta[l+1]
-      const float dm = (l > 0) ? __fsub_rn(xs, cyl[l - 1]) : 0.f;      // delta[l]
-      const float bt_p = __fmul_rn(2.f, b_tilde(dp, sc));
-      const float bt_m = __fmul_rn(2.f, b_tilde(dm, sc));
-      g_p = __fadd_rn(__fmul_rn(-sc.b[4], __fmul_rn(bt_p, dp)),
-                      __fmul_rn(sc.b[5], __fmul_rn(bt_m, dm)));
-      h_p = __fadd_rn(__fmul_rn(sc.b[4], bt_p), __fmul_rn(sc.b[5], bt_m));
-      const int row = pixel / NC, col = pixel - (pixel / NC) * NC;
-      const int dr[4] = {1, -1, 0, 0}, dc[4] = {0, 0, 1, -1};
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int rr = min(max(row + dr[k], 0), NR - 1);
-        const int cc = min(max(col + dc[k], 0), NC - 1);
-        const float d = __fsub_rn(xs, flat[((size_t)rr * NC + cc) * S + l]);
-        const float w = __fmul_rn(sc.two_b[k], b_tilde(d, sc));
-        g_p = __fadd_rn(g_p, __fmul_rn(w, d));
-        h_p = __fadd_rn(h_p, w);
-      }
+      qggmrf_terms(flat, pixel, l, S, NR, NC, sc, g_p, h_p);
     }
     if (!DC) {
       const float dl = -__fdiv_rn(__fadd_rn(g_f, g_p), __fadd_rn(h_f, h_p));
@@ -536,6 +545,77 @@ vcd_sino_update_tiles_kernel(int C, int R, int CB, const unsigned char *__restri
     for (int u = 0; u < U; ++u) {
       const int i = i0 + 256 * u;
       if (i < n) et[i] = from_f32<T>(__fsub_rn(ev[u], __fmul_rn(a, dv[u])));
+    }
+  }
+}
+
+// ── QGGMRF denoiser (identity forward model; denoising.py:35-83) ──────────
+// Direction at the subset's voxels: the qGGMRF prior terms, the forward
+// gradient -fmc * e and forward Hessian 1, and the four line-search sums
+// per CTA: (sum g_p d, sum h_p d^2) into prior, (sum e d, sum d^2) into fwd.
+__global__ void __launch_bounds__(kThreads)
+denoise_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int NC,
+                         const float *__restrict__ flat, const float *__restrict__ err,
+                         VcdScalars sc, float *__restrict__ delta, double *__restrict__ prior,
+                         double *__restrict__ fwd) {
+  const size_t n = (size_t)P * S;
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  double pl = 0.0, pq = 0.0, fl = 0.0, fq = 0.0;
+  if (i < n) {
+    const int p = (int)(i / S), l = (int)(i - (size_t)p * S);
+    const int pixel = (int)pix[p];
+    float g_p, h_p;
+    qggmrf_terms(flat, pixel, l, S, NR, NC, sc, g_p, h_p);
+    const float e = err[(size_t)pixel * S + l];
+    const float g_f = __fmul_rn(-sc.fmc, e);
+    const float dl = -__fdiv_rn(__fadd_rn(g_f, g_p), __fadd_rn(1.f, h_p));
+    delta[i] = dl;
+    pl = (double)__fmul_rn(g_p, dl);
+    pq = (double)__fmul_rn(h_p, __fmul_rn(dl, dl));
+    fl = (double)__fmul_rn(e, dl);
+    fq = (double)__fmul_rn(dl, dl);
+  }
+  block_sum2(pl, pq);
+  block_sum2(fl, fq);
+  if (threadIdx.x == 0) {
+    prior[2 * blockIdx.x] = pl;
+    prior[2 * blockIdx.x + 1] = pq;
+    fwd[2 * blockIdx.x] = fl;
+    fwd[2 * blockIdx.x + 1] = fq;
+  }
+}
+
+// image += alpha d and error -= alpha d at the subset's voxels; the last CTA
+// folds ell1 and alpha into accum[0], accum[1] (fixed order).
+__global__ void __launch_bounds__(kThreads)
+denoise_update_kernel(int P, int S, const int64_t *__restrict__ pix,
+                      const float *__restrict__ delta, const float *__restrict__ alpha,
+                      float *__restrict__ flat, float *__restrict__ err,
+                      double *__restrict__ l1_part, unsigned int *__restrict__ counter,
+                      double *__restrict__ accum) {
+  const size_t n = (size_t)P * S;
+  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
+  const float a = alpha[0];
+  double l1 = 0.0, dummy = 0.0;
+  if (i < n) {
+    const int p = (int)(i / S), l = (int)(i - (size_t)p * S);
+    const size_t v = (size_t)pix[p] * S + l;
+    const float ds = __fmul_rn(a, delta[i]);
+    flat[v] = __fadd_rn(flat[v], ds);
+    err[v] = __fsub_rn(err[v], ds);
+    l1 = (double)fabsf(ds);
+  }
+  block_sum2(l1, dummy);
+  if (threadIdx.x == 0) l1_part[blockIdx.x] = l1;
+  if (last_cta(counter, gridDim.x)) {
+    double t1 = 0.0, t2 = 0.0;
+#pragma unroll 4
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) t1 += __ldcg(l1_part + k);
+    block_sum2(t1, t2);
+    if (threadIdx.x == 0) {
+      accum[0] += t1;
+      accum[1] += (double)a;
+      *counter = 0u;
     }
   }
 }

@@ -22,6 +22,8 @@ Cases
   recon_*.npz       seeded VCD recon traces (parallel, cone, weighted)
   prox_*.npz        seeded prox_map (proximal-map prior) traces, parallel
                     (automatic sigma_prox) and cone (given sigma_prox)
+  denoise.npz       QGGMRFDenoiser: noise estimate and seeded denoise runs
+                    (given and estimated sigma_noise)
 
 Pass case-function names to regenerate only those, e.g.
     PYTHONPATH=/root/reference python tests/golden/make_golden.py prox_cases
@@ -358,8 +360,30 @@ def prox_cases():
     print('wrote prox')
 
 
+def denoise_case():
+    shape = (24, 20, 10)
+    clean = phantom(shape, 51)
+    noisy = (clean + np.random.default_rng(52).normal(0, 0.1, shape)).astype(np.float32)
+    den = mbirtorch.QGGMRFDenoiser(shape, compile_mode='off')
+    den.configure_devices(devices=['cpu'])
+    den.set_params(no_warning=True, verbose=0)
+    out = {'noisy': noisy, 'sigma_est': np.array(den.estimate_image_noise_std(noisy))}
+    for tag, sigma in (('given', 0.1), ('auto', None)):
+        np.random.seed(13)
+        d, dd = den.denoise(noisy, sigma_noise=sigma, max_iterations=4,
+                            stop_threshold_change_pct=0.0, logfile_path=None, print_logs=False)
+        rp = dd['recon_params']
+        out[f'{tag}_out'] = d
+        out[f'{tag}_alpha'] = np.array(rp['alpha_values'])
+        out[f'{tag}_nmae_pct'] = np.array(rp['stop_threshold_change_pct'])
+        out[f'{tag}_reg'] = np.array([rp['regularization_params'][k]
+                                      for k in ('sigma_y', 'sigma_x', 'sigma_prox')])
+    np.savez_compressed(os.path.join(HERE, 'denoise.npz'), **out)
+    print('wrote denoise')
+
+
 CASES = ['projector_cases', 'qggmrf_case', 'partition_case', 'autoreg_and_direct_cases',
-         'recon_cases', 'prox_cases']
+         'recon_cases', 'prox_cases', 'denoise_case']
 
 if __name__ == '__main__':
     for name in (sys.argv[1:] or CASES):

@@ -127,3 +127,24 @@ def test_storage_precision_names():
         m.set_storage_precision(s)
     with pytest.raises(ValueError):
         m.set_storage_precision('int8')
+
+
+def test_denoiser_noise_estimate_and_regularization_match_reference():
+    """The denoiser's host statistics (noise estimate, auto-regularization
+    on the row subsample) against the reference's values."""
+    from conftest import load_golden
+    from mbirtorch_b200.denoising import _subsample_to_host
+    d = load_golden('denoise.npz')
+    noisy = d['noisy']
+    den = mb.QGGMRFDenoiser(noisy.shape)
+    den.set_params(no_warning=True, verbose=0)
+    assert abs(den.estimate_image_noise_std(noisy) - float(d['sigma_est'])) \
+        <= 1e-6 * float(d['sigma_est'])
+    for tag, sigma in (('given', 0.1), ('auto', None)):
+        sigma = den.estimate_image_noise_std(noisy) if sigma is None else sigma
+        den.set_params(no_warning=True, sigma_noise=sigma)
+        rows = den.subsample_views(np.arange(noisy.shape[0]))
+        step = int(rows[1] - rows[0]) if rows.size > 1 else 1
+        reg = den.auto_set_regularization_params(_subsample_to_host(noisy, row_step=step))
+        np.testing.assert_allclose([reg['sigma_y'], reg['sigma_x'], reg['sigma_prox']],
+                                   d[f'{tag}_reg'], rtol=1e-6)

@@ -179,3 +179,19 @@ def test_prox_map_matches_reference(name):
     assert rel_l2(rec, d['recon']) < 1e-4
     np.testing.assert_allclose(st['fm_rmse'], d['fm_rmse'], rtol=1e-4)
     np.testing.assert_allclose(st['alpha'], d['alpha'], rtol=1e-4)
+
+
+@pytest.mark.parametrize("tag", ["given", "auto"])
+def test_denoiser_matches_reference(tag):
+    """QGGMRFDenoiser.denoise: the reference's seeded sweep against the
+    oracle, with the regularization scalars the reference used."""
+    from oracle import denoise as oden
+    d = load_golden('denoise.npz')
+    noisy = d['noisy']
+    np.random.seed(13)
+    part = vcd.pixel_partition(noisy.shape, 16, use_ror_mask=False)
+    sigma_y, sigma_x = d[f'{tag}_reg'][:2]
+    out, alphas, nmaes = oden.denoise(noisy, sigma_y, sigma_x, part, 4)
+    assert rel_l2(out, d[f'{tag}_out']) < 1e-5
+    np.testing.assert_allclose(alphas, d[f'{tag}_alpha'], rtol=1e-4)
+    np.testing.assert_allclose(100 * nmaes, d[f'{tag}_nmae_pct'], rtol=1e-4)
