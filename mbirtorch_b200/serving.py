@@ -90,6 +90,8 @@ class Request:
         self._charge = 0
         self._out = None
         self._out_event = None
+        self._state = None       # a preempted run's state, to resume from
+        self.preempted = False   # taken off the device by ReconServer.preempt
 
     def done(self):
         return self.finished is not None
@@ -164,7 +166,39 @@ class ReconServer:
         max_ps = max((-(-n_pix // min(int(gran[int(i)]), n_pix)) for i in seq), default=1)
         return MemoryLedger.job_bytes(model, self.storage_dtype, weighted, max_ps)
 
+    def _admit_state(self, r):
+        m = r.model
+        m.configure_devices(devices=[self.device])
+        m.setup_logger(logfile_path=None, print_logs=False)
+        state = r._state
+        m.storage_dtype = {_lib.MBIR_F32: 'float32', _lib.MBIR_BF16: 'bfloat16',
+                           _lib.MBIR_F16: 'float16'}[int(state['storage'])]
+        seq = np.asarray(state['seq'])
+        parts = [state[f'partition_{k}'] for k in range(int(state['num_partitions']))]
+        max_ps = max((int(parts[int(i)].shape[1]) for i in seq), default=1)
+        _, resident = MemoryLedger.job_bytes(m, m.storage_dtype, 'w' in state, max_ps)
+        if not self.ledger.fits(resident):
+            if self.active:
+                self.deferred += 1
+                return False
+            raise MemoryError(f'request {r.id} needs {resident} bytes; the ledger budget is '
+                              f'{self.ledger.budget}')
+        r._stream = self._streams.pop() if self._streams else torch.cuda.Stream(self.device)
+        with torch.cuda.device(self.device):
+            r._run = VcdRun.from_state(m, state, stream=r._stream)
+        r._state = None
+        self.ledger.take(resident)
+        r._charge = resident
+        r.admitted = time.perf_counter()
+        if r._run.finished:
+            self._finish(r)
+        else:
+            r._run.enqueue_iteration()
+        return True
+
     def _admit(self, r):
+        if getattr(r, '_state', None) is not None:
+            return self._admit_state(r)
         m = r.model
         peak, resident = self.job_charge(m, r.weights is not None, r.max_iterations)
         if not self.ledger.fits(peak):
@@ -207,6 +241,38 @@ class ReconServer:
         r.recon_params = {'num_iterations': run.done, 'fm_rmse': [float(v) for v in fm],
                           'stop_threshold_change_pct': [100 * float(v) for v in nmae],
                           'alpha_values': [float(v) for v in alphas]}
+
+    # ── preemption ─────────────────────────────────────────────────────────
+    def preempt(self, request):
+        """Take an admitted request off the device between iterations: its
+        resident state comes back as a host dict (:meth:`VcdRun.state_dict`)
+        and its memory and slot are freed.  :meth:`resume` continues it,
+        here or in another server, to the same result it would have reached
+        uninterrupted."""
+        if request not in self.active or request._run is None or request._out_event is not None:
+            raise ValueError(f'request {request.id} is not running')
+        run = request._run
+        if run._event is not None:
+            if run.collect():
+                pass  # finished now; the checkpoint still carries its state
+        state = run.state_dict()
+        state['request_max_iterations'] = np.array(request.max_iterations)
+        self.active.remove(request)
+        self._streams.append(request._stream)
+        request._stream = None
+        request._run = None
+        self.ledger.release(request._charge)
+        request._charge = 0
+        request.preempted = True
+        return state
+
+    def resume(self, model, state, arrival=None):
+        """Queue a preempted request (its model and its :meth:`preempt`
+        state) to continue; returns the new :class:`Request`."""
+        r = self.submit(model, None, max_iterations=int(state['request_max_iterations']),
+                        arrival=arrival)
+        r._state = state
+        return r
 
     def step(self):
         """One scheduler pass; returns True if it did anything."""

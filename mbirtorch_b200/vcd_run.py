@@ -27,6 +27,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._lib import STORAGE_DTYPES
 from .vcd_engine import ResidentSinogram, error_init, iteration_stats, order_array, storage_code
 
 
@@ -223,6 +224,138 @@ class VcdRun:
     def checkpoint(self):
         with torch.cuda.stream(self.stream):
             return {'error_sinogram': self.err.to_vrc(), 'fm_hessian': self.fm_hessian}
+
+    # ── resident-state checkpoint (preemption and restart) ───────────────
+    _TRACES = ('fm_rmse', 'pm_loss', 'nmae', 'alphas', 'dnorm')
+
+    def state_dict(self):
+        """The run's whole resident state on the host, between iterations:
+        the recon, the stored error sinogram (its storage bits and per-view
+        scales), weights, the FP32 measurements kept for the 16-bit refresh,
+        the Hessian diagonal, the partitions and sequence, the traces so far
+        and the position of the run's own RandomState.  A run restored from
+        it (:meth:`from_state`) continues exactly as this one would have:
+        the same subset orders and bit-identical kernels.  Only runs with
+        their own RandomState can be checkpointed (the global numpy
+        generator is not theirs to save)."""
+        if self._event is not None:
+            raise RuntimeError('checkpoint between iterations (collect the pending one first)')
+        if not isinstance(self.rng, np.random.RandomState):
+            raise RuntimeError('only a run with its own RandomState can be checkpointed')
+
+        def raw(t):  # 16-bit storage travels as its raw bits
+            t = t.detach()
+            return (t.view(torch.int16) if t.dtype in (torch.float16, torch.bfloat16)
+                    else t).cpu().numpy()
+
+        with torch.cuda.stream(self.stream):
+            kind, keys, pos, has_gauss, gauss = self.rng.get_state()
+            st = {'version': np.array(1), 'storage': np.array(self.storage),
+                  'refresh': np.array(self.refresh), 'done': np.array(self.done),
+                  'finished': np.array(self.finished), 'seq': np.asarray(self.seq),
+                  'stop_pct': np.array(self.stop_pct),
+                  'first_iteration': np.array(self.first_iteration),
+                  'constant_weights': np.array(self.constant_weights),
+                  'recon_shape': np.array(self.recon_shape),
+                  'sinogram_shape': np.array(self.sinogram_shape),
+                  'flat': raw(self.flat), 'fm_hessian': raw(self.fm_hessian),
+                  'err': raw(self.err.data), 'err_scale': raw(self.err.scale),
+                  'rng_keys': keys, 'rng_pos': np.array(pos),
+                  'rng_gauss': np.array([has_gauss, gauss], dtype=np.float64),
+                  'num_partitions': np.array(len(self.partitions)),
+                  'reg': np.array([self.model.get_params(k) or 0.0
+                                   for k in ('sigma_y', 'sigma_x', 'sigma_prox')],
+                                  dtype=np.float64)}
+            for k, p in enumerate(self.partitions):
+                st[f'partition_{k}'] = np.asarray(p)
+            for name in self._TRACES:
+                st[name] = getattr(self, name)
+            if self.w_res is not None:
+                st['w'], st['w_scale'] = raw(self.w_res.data), raw(self.w_res.scale)
+            if self.y_vcr is not None:
+                st['y_vcr'] = raw(self.y_vcr)
+            if self.prox_flat is not None:
+                st['prox'] = raw(self.prox_flat)
+        return st
+
+    def save_state(self, path):
+        """:meth:`state_dict` written to ``path`` (numpy .npz)."""
+        np.savez(path, **self.state_dict())
+
+    @classmethod
+    def from_state(cls, model, state, stream=None):
+        """A prepared run that continues from ``state`` (a dict from
+        :meth:`state_dict` or the path of a :meth:`save_state` file) on
+        ``model`` (the same geometry and regularization)."""
+        if isinstance(state, (str, bytes)) or hasattr(state, '__fspath__'):
+            with np.load(state) as f:
+                state = {k: f[k] for k in f.files}
+        if int(state['version']) != 1:
+            raise ValueError('unknown checkpoint version {}'.format(int(state['version'])))
+        if tuple(state['recon_shape']) != tuple(model.get_params('recon_shape')) or \
+                tuple(state['sinogram_shape']) != tuple(model.get_params('sinogram_shape')):
+            raise ValueError('the checkpoint was taken on another geometry')
+        storage = int(state['storage'])
+        sy, sx, sp = (float(v) for v in state['reg'])
+        model.set_params(no_warning=True, sigma_y=sy, sigma_x=sx, sigma_prox=sp,
+                         auto_regularize_flag=False)
+        model.storage_dtype = {_lib.MBIR_F32: 'float32', _lib.MBIR_BF16: 'bfloat16',
+                               _lib.MBIR_F16: 'float16'}[storage]
+        parts = [state[f'partition_{k}'] for k in range(int(state['num_partitions']))]
+        rng = np.random.RandomState()
+        rng.set_state(('MT19937', state['rng_keys'], int(state['rng_pos']),
+                       int(state['rng_gauss'][0]), float(state['rng_gauss'][1])))
+        run = cls.__new__(cls)
+        run.model = model
+        run.recon_shape = tuple(int(v) for v in state['recon_shape'])
+        run.sinogram_shape = tuple(int(v) for v in state['sinogram_shape'])
+        run.sinogram = run.weights = run.init_recon = run.init_error_sinogram = None
+        run.prox_input = None
+        run.partitions = parts
+        run.seq = np.asarray(state['seq'])
+        run.stop_pct = float(state['stop_pct'])
+        run.rng = rng
+        run.first_iteration = int(state['first_iteration'])
+        run.storage = storage
+        run.stream = stream if stream is not None else torch.cuda.current_stream(
+            model.torch_device)
+        for name in cls._TRACES:
+            setattr(run, name, np.array(state[name]))
+        run.done = int(state['done'])
+        run.finished = bool(state['finished'])
+        run._event = None
+        run._pending = None
+        run.refresh = int(state['refresh'])
+        run.constant_weights = bool(state['constant_weights'])
+        dev = model.torch_device
+        sdt = STORAGE_DTYPES[storage]
+
+        def cooked(a, dtype):
+            t = torch.as_tensor(a, device=dev)
+            return t.view(dtype) if dtype in (torch.float16, torch.bfloat16) else t
+
+        with torch.cuda.stream(run.stream):
+            run.flat = cooked(state['flat'], torch.float32).contiguous()
+            run.fm_hessian = cooked(state['fm_hessian'], torch.float32)
+            V, R, C = run.sinogram_shape
+            run.err = ResidentSinogram(cooked(state['err'], sdt).contiguous(),
+                                       cooked(state['err_scale'], torch.float32), R, storage)
+            run.w_res = None
+            if 'w' in state:
+                run.w_res = ResidentSinogram(cooked(state['w'], sdt).contiguous(),
+                                             cooked(state['w_scale'], torch.float32), R, storage)
+            run.y_vcr = cooked(state['y_vcr'], torch.float32) if 'y_vcr' in state else None
+            run.prox_flat = cooked(state['prox'], torch.float32) if 'prox' in state else None
+            run.total = float(math.prod(run.sinogram_shape))
+            run.parts_dev = [torch.as_tensor(np.ascontiguousarray(p), dtype=torch.int64,
+                                             device=dev) for p in parts]
+            max_ps = max((int(parts[int(i)].shape[1]) for i in run.seq), default=1)
+            H = run.fm_hessian.reshape(-1, run.fm_hessian.shape[-1]).contiguous()
+            run.engine = model._make_engine(H, run.w_res, storage, max_subset_pixels=max_ps,
+                                            prox_flat=run.prox_flat)
+            run.host = torch.empty(2 + run.recon_shape[2] + 4, dtype=torch.float64,
+                                   pin_memory=True)
+        return run
 
     def device_bytes(self):
         """Bytes this run holds resident on the device."""

@@ -138,3 +138,33 @@ def test_poisson_schedule_overlaps_jobs():
     assert len(done) == len(jobs) and all(r.error is None for r in done)
     assert srv.max_concurrent >= 2
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("storage", ["float32", "float16"])
+def test_preempt_checkpoint_resume_equals_uninterrupted(storage, tmp_path):
+    """A cone job preempted after two of three iterations, its resident state
+    written to disk and resumed in another server, ends bitwise where the
+    uninterrupted job ends."""
+    jobs = _jobs()
+    make, sino = jobs[1]
+    _, alone = _serve(jobs, [1], storage)
+    srv = ReconServer(storage_dtype=storage, max_active=2)
+    m = make()
+    m.set_params(no_warning=True, verbose=0)
+    r = srv.submit(m, sino, max_iterations=3, seed=1001)
+    while r._run is None or r._run.done < 1:
+        srv.step()
+    state = srv.preempt(r)   # collects the iteration in flight: two done
+    assert int(state['done']) == 2 and not bool(state['finished'])
+    assert r.preempted and srv.ledger.used == 0 and not srv.active
+    np.savez(tmp_path / 'job.npz', **state)
+    with np.load(tmp_path / 'job.npz') as f:
+        loaded = {k: f[k] for k in f.files}
+    srv2 = ReconServer(storage_dtype=storage, max_active=2)
+    m2 = make()
+    m2.set_params(no_warning=True, verbose=0)
+    r2 = srv2.resume(m2, loaded)
+    srv2.run_until_idle(timeout_s=300)
+    assert r2.error is None
+    assert np.array_equal(r2.recon, alone[0].recon)
+    assert r2.recon_params['fm_rmse'] == alone[0].recon_params['fm_rmse']
