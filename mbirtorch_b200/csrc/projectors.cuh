@@ -642,6 +642,7 @@ __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec,
     }
     __syncthreads();
     if (tid < R) {
+#pragma unroll 2
       for (int e = 0; e < nb; ++e) {
         const ConeFwdRec *r = rec + b0 + e;
         const float4 ra = r->a, rb = r->b;

@@ -66,7 +66,8 @@ __device__ __forceinline__ float b_tilde(float delta, const VcdScalars &s) {
   const float ad = fmaxf(fabsf(delta), s.a_min);
   const float ds = __fdiv_rn(ad, s.t_sx);
   const float dqp = powf(ds, s.q_minus_p);
-  const float dp2 = powf(ad, s.p_minus_2);
+  // x^0 is exactly 1 for every x, so the default p = 2 skips the call.
+  const float dp2 = s.p_minus_2 == 0.f ? 1.f : powf(ad, s.p_minus_2);
   float num = __fdiv_rn(dp2, s.two_sx_p);
   num = __fmul_rn(__fmul_rn(num, dqp), __fadd_rn(s.q_over_p, dqp));
   const float den = __fadd_rn(1.f, dqp);
