@@ -177,7 +177,51 @@ back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_cou
   }
 }
 
+// Trapezoid tap weight min(max(x, 0), lmax) (cone_beam.py:203-226,
+// 268-299).  With lmax = 1 -- a projected voxel at least one row pitch tall,
+// the common case -- the clamp is one saturating add; the caller picks SAT
+// from lmax for a whole view (the values are the same either way).
+template <bool SAT>
+__device__ __forceinline__ float trap_w(float x, float lmax) {
+  return SAT ? __saturatef(x) : fminf(fmaxf(x, 0.f), lmax);
+}
+
 // ── back projection: cone ─────────────────────────────────────────────────
+// The vertical gather of one view for a lane's SPL slices l, l + 32, ...:
+// taps of the detector column h around the slice's projected row, scaled
+// by 1 / cos(phi) (coefficient power 1) or 1 + t^2 (power 2).
+template <int CP, int SPL, int NT, bool SAT>
+__device__ __forceinline__ void back_cone_slices(float (&acc)[SPL], const float *__restrict__ h,
+                                                 int l1, int band, int slice_start, float w_r,
+                                                 float m0, float hw1r, float lmaxr, float a0,
+                                                 float a1, float mlo_clamp, float mhi_clamp,
+                                                 int RT, int nt) {
+  constexpr int MT = MBIR_TAPS(NT);
+#pragma unroll
+  for (int j = 0; j < SPL; ++j) {
+    const int l = l1 + 32 * j;
+    if (l < band) {
+      const float k = (float)(slice_start + l);
+      const float m_p = fminf(fmaxf(fmaf(w_r, k, m0), mlo_clamp), mhi_clamp);
+      const float mcf = rintf(m_p);
+      const int mc = (int)mcf;
+      const float d = m_p - mcf;
+      float s = 0.f;
+#pragma unroll
+      for (int t = 0; t < MT; ++t) {
+        if (MBIR_TAP_ON(NT, t, nt)) {
+          float a = trap_w<SAT>(hw1r - fabsf(d - (float)(t - RT)), lmaxr);
+          if (CP == 2) a = a * a;
+          s = fmaf(a, h[mc + t - RT], s);
+        }
+      }
+      const float tk = fmaf(a1, k, a0);
+      const float ic = CP == 2 ? fmaf(tk, tk, 1.f) : inv_cos_from_t(tk);
+      acc[j] = fmaf(ic, s, acc[j]);
+    }
+  }
+}
+
 // One warp per (pixel, chunk of 32*SPL slices).  Dynamic shared memory:
 // 8 warps x (R + 2 kPad) floats of column buffer, then 8 x 32 ConeRec.
 template <int CP, int SPL, int NT, typename RD>
@@ -299,29 +343,12 @@ back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, 
         }
       }
       __syncwarp();
-#pragma unroll
-      for (int j = 0; j < SPL; ++j) {
-        const int l = l0 + lane + 32 * j;
-        if (l < band) {
-          const float k = (float)(slice_start + l);
-          const float m_p = fminf(fmaxf(fmaf(w_r, k, m0), mlo_clamp), mhi_clamp);
-          const float mcf = rintf(m_p);
-          const int mc = (int)mcf;
-          const float d = m_p - mcf;
-          float s = 0.f;
-#pragma unroll
-          for (int t = 0; t < MT; ++t) {
-            if (MBIR_TAP_ON(NT, t, nt)) {
-              float a = fminf(fmaxf(hw1r - fabsf(d - (float)(t - RT)), 0.f), lmaxr);
-              if (CP == 2) a = a * a;
-              s = fmaf(a, h[mc + t - RT], s);
-            }
-          }
-          const float tk = fmaf(a1, k, a0);
-          const float ic = CP == 2 ? fmaf(tk, tk, 1.f) : inv_cos_from_t(tk);
-          acc[j] = fmaf(ic, s, acc[j]);
-        }
-      }
+      if (lmaxr == 1.f)
+        back_cone_slices<CP, SPL, NT, true>(acc, h, l0 + lane, band, slice_start, w_r, m0, hw1r,
+                                            lmaxr, a0, a1, mlo_clamp, mhi_clamp, RT, nt);
+      else
+        back_cone_slices<CP, SPL, NT, false>(acc, h, l0 + lane, band, slice_start, w_r, m0, hw1r,
+                                             lmaxr, a0, a1, mlo_clamp, mhi_clamp, RT, nt);
       __syncwarp();
     }
   }
@@ -653,10 +680,15 @@ __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec,
         const float d = w_r * (kc - k_m);
         const float *st = stage + e * SP + kFwdVPad + ((int)kc - slice_start);
         float det;
-        if (bp == 1) {
-          const float am = fminf(fmaxf(hw1r - fabsf(d - w_r), 0.f), lmaxr);
-          const float a0 = fminf(fmaxf(hw1r - fabsf(d), 0.f), lmaxr);
-          const float ap = fminf(fmaxf(hw1r - fabsf(d + w_r), 0.f), lmaxr);
+        if (bp == 1 && lmaxr == 1.f) {
+          const float am = trap_w<true>(hw1r - fabsf(d - w_r), lmaxr);
+          const float a0 = trap_w<true>(hw1r - fabsf(d), lmaxr);
+          const float ap = trap_w<true>(hw1r - fabsf(d + w_r), lmaxr);
+          det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
+        } else if (bp == 1) {
+          const float am = trap_w<false>(hw1r - fabsf(d - w_r), lmaxr);
+          const float a0 = trap_w<false>(hw1r - fabsf(d), lmaxr);
+          const float ap = trap_w<false>(hw1r - fabsf(d + w_r), lmaxr);
           det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
         } else {
           det = 0.f;
