@@ -35,6 +35,14 @@ constexpr int kThreads = 256;
 constexpr int kListCap = 512;  // forward: pixel records per processing round
 constexpr int kPad = 8;        // cone back: zero rows either side of the column buffer
 
+// Cache hints (no architectural effect; every address passed is in bounds).
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+__device__ __forceinline__ void prefetch_l1(const void *p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // ── sinogram readers (resident VCR layout) ─────────────────────────────────
 // value(v, c, m) = scale(v) * get(base(v, c) + m)
 struct ReadF32 {
@@ -393,6 +401,7 @@ struct StoreSino {
   int layout, C, R;
   __device__ __forceinline__ bool channel_fastest() const { return layout == MBIR_LAYOUT_VRC; }
   __device__ __forceinline__ void begin(int) {}
+  __device__ __forceinline__ void prefetch(int, int, int) {}
   __device__ __forceinline__ void cell(int v, int c, int m, float val) {
     if (layout == MBIR_LAYOUT_VCR)
       out[((size_t)v * C + c) * R + m] = val;
@@ -915,11 +924,21 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
   for (int i = tid; i < kFwdEB * SP; i += nthr) stage[i] = 0.f;
 #pragma unroll
   for (int r = 0; r < kFwdCB + 4; ++r) acc_s[r * nthr + tid] = 0.f;
+  // The epilogue's operands (the error sinogram's cells of this tile) are
+  // on their way to L2 while the tile is computed.
+  epi.prefetch(v, c0, ncb);
   for (int base = start; base < end; base += cap) {
     const int n = min(cap, end - base);
     __syncthreads();
     for (int i = tid; i < n; i += nthr) rec[i] = vrec[vlist[base + i]];
     __syncthreads();
+    // The round's cylinders, 128-byte line by line, toward L1 ahead of the
+    // batch staging.
+    const int lines = (band * (int)sizeof(float) + 127) / 128;
+    for (int i = tid; i < n * lines; i += nthr) {
+      const int e = i / lines, ln = i - e * lines;
+      prefetch_l1(values + (size_t)__float_as_int(rec[e].c.w) * band + ln * 32);
+    }
     fwd_rt_round(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, c0, acc_s);
   }
   float acc[kFwdCB];

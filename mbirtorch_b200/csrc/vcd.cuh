@@ -275,6 +275,17 @@ struct LineSearchEpi {
     inv_scale = 1.f / scale;
     wscale = w != nullptr ? __ldg(wsc + v) : 1.f;
   }
+  // Each warp sends the 128-byte lines of its 32 rows x ncb channels of e
+  // (and w) toward L2 (lane j: channel j).
+  __device__ __forceinline__ void prefetch(int v, int c0, int ncb) {
+    if (!with_sums) return;
+    const int lane = threadIdx.x & 31, m0 = threadIdx.x - lane;
+    if (lane < ncb && m0 < R) {
+      const size_t i = ((size_t)v * C + c0 + lane) * R + m0;
+      prefetch_l2(e + i);
+      if (w != nullptr) prefetch_l2(w + i);
+    }
+  }
   __device__ __forceinline__ void cell(int v, int c, int m, float val) {
     const size_t i = ((size_t)v * C + c) * R + m;
     const T stored = from_f32<T>(__fmul_rn(val, inv_scale));
@@ -349,6 +360,7 @@ struct RefreshEpi {
   float inv_scale;
   __device__ __forceinline__ bool channel_fastest() const { return false; }
   __device__ __forceinline__ void begin(int v) { inv_scale = 1.f / __ldg(es + v); }
+  __device__ __forceinline__ void prefetch(int, int, int) {}
   __device__ __forceinline__ void cell(int v, int c, int m, float val) {
     const size_t i = ((size_t)v * C + c) * R + m;
     e[i] = from_f32<T>(__fmul_rn(__fsub_rn(__ldg(y + i), val), inv_scale));
