@@ -324,8 +324,8 @@ int fwd_nblk(const mbir_geometry *g) { return (g->num_det_channels + kFwdCB - 1)
 
 // Views per binning chunk for a subset of P pixels.
 int bin_views(const mbir_geometry *g, long long P) {
-  const size_t per_view = (size_t)P * (sizeof(ConeFwdRec) + 2 * sizeof(int)) +
-                          (size_t)(fwd_nblk(g) + 1) * sizeof(int);
+  const size_t per_view = (size_t)P * (sizeof(ConeFwdRec) + sizeof(int)) +
+                          (size_t)(fwd_nkeys(g->num_det_channels) + 1) * sizeof(int);
   return (int)std::max<size_t>(1, std::min<size_t>(g->num_views, kBinBytes / per_view));
 }
 
@@ -337,7 +337,14 @@ struct FwdBins {
 };
 
 size_t bin_smem(const mbir_geometry *g) {
-  return sizeof(int) * (size_t)fwd_nblk(g) * (1 + 2 * (kThreads / 32));
+  return sizeof(int) * (size_t)fwd_nkeys(g->num_det_channels) * (1 + kThreads / 32);
+}
+
+// The binned forward where the row-tiled one applies and the binning's
+// per-key counters fit in shared memory (up to about 5,700 channels); wider
+// detectors project each subset with the scanning forward.
+bool use_cone_binned(const mbir_geometry *g) {
+  return use_cone_rt(g) && bin_smem(g) <= (size_t)200 * 1024;
 }
 
 int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count,
@@ -352,8 +359,8 @@ int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count
                   smem, cudaGetErrorString(e));
   }
   tpre(st);
-  cone_bin_kernel<<<v_count, kThreads, smem, st>>>(geo, vp, v_start, pix, (int)P, 0, fwd_nblk(g),
-                                                   b.recs, b.list, b.offs);
+  cone_bin_kernel<<<v_count, kThreads, smem, st>>>(geo, vp, v_start, pix, (int)P, 0, b.recs,
+                                                   b.list, b.offs);
   MBIR_CHECK_LAUNCH("vcd forward binning");
   return MBIR_OK;
 }
@@ -467,14 +474,14 @@ VcdWs vcd_layout(const mbir_geometry *g, long long Ps, const mbir_vcd_params *pr
   w.alpha = c.take<float>(4);
   w.counters = c.take<unsigned int>(2);
   w.ad = c.take<char>((size_t)V * g->num_det_channels * g->num_det_rows * storage_size(prm->storage));
-  w.binned = use_cone_rt(g);
+  w.binned = use_cone_binned(g);
   w.bins = FwdBins{nullptr, nullptr, nullptr, nullptr, 0};
   if (w.binned) {
     const int vc = bin_views(g, Ps);
     w.bins.views = vc;
     w.bins.recs = c.take<ConeFwdRec>((size_t)vc * Ps);
-    w.bins.list = c.take<int>((size_t)vc * 2 * Ps);
-    w.bins.offs = c.take<int>((size_t)vc * (fwd_nblk(g) + 1));
+    w.bins.list = c.take<int>((size_t)vc * Ps);
+    w.bins.offs = c.take<int>((size_t)vc * (fwd_nkeys(g->num_det_channels) + 1));
     w.bins.touched = c.take<unsigned char>((size_t)V * fwd_nblk(g));
   }
   w.bytes = c.used;
@@ -491,7 +498,7 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   const VcdScalars sc = make_scalars(*prm);
   const bool DCon = dc != nullptr;
   int rc;
-  // 0. the subset's (view, pixel) records, binned by channel block; when one
+  // 0. the subset's (view, pixel) records, sorted by centre channel; when one
   //    chunk holds every view the gradient reads them too.
   const bool shared_bins = w.binned && w.bins.views >= V && g->psf_radius == 1;
   if (shared_bins) {

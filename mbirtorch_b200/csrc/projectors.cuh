@@ -634,12 +634,86 @@ __device__ __forceinline__ void fwd_block_range(int ctr, int C, int &b_lo, int &
   }
 }
 
+// The pixels of one staged batch for detector row m = threadIdx.x: the
+// row's vertical fan over the staged cylinder of each pixel and its three
+// channel taps (fwd_rt_round describes the accumulators).  BP = 1 is the
+// psf radius 1 with the taps unrolled; BP = 0 takes the radius bp at run
+// time.  A tap weight clamp(x, 0, lmax) is formed as min(sat(x), lmax),
+// the same value for lmax = min(w_r, 1) <= 1, with no branch on lmax.
+template <int BP, bool SORTED>
+__device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec, int nb,
+                                             const float *__restrict__ stage, int SP, float mf,
+                                             float kc_lo, float kc_hi, int slice_start, int bp,
+                                             int c0, float *__restrict__ acc_s, int &cj,
+                                             float &q0, float &q1, float &q2) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+#pragma unroll 1
+  for (int e = 0; e < nb; ++e) {
+    const ConeFwdRec *r = rec + e;
+    const float4 ra = r->a, rb = r->b;
+    const int j = __float_as_int(r->c.z) - c0 + 1;  // in [0, kFwdCB + 1]
+    const float m0 = ra.x, w_r = ra.y, hw1r = ra.z, lmaxr = ra.w;
+    const float k_m = (mf - m0) * rb.x;
+    const float kc = fminf(fmaxf(rintf(k_m), kc_lo), kc_hi);
+    const float d = w_r * (kc - k_m);
+    const float *st = stage + e * SP + kFwdVPad + ((int)kc - slice_start);
+    float det;
+    if (BP == 1) {
+      const float am = fminf(__saturatef(hw1r - fabsf(d - w_r)), lmaxr);
+      const float a0 = fminf(__saturatef(hw1r - fabsf(d)), lmaxr);
+      const float ap = fminf(__saturatef(hw1r - fabsf(d + w_r)), lmaxr);
+      det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
+    } else {
+      det = 0.f;
+      for (int ko = -bp; ko <= bp; ++ko) {
+        const float a = fminf(__saturatef(hw1r - fabsf(fmaf(w_r, (float)ko, d))), lmaxr);
+        det = fmaf(a, st[ko], det);
+      }
+    }
+    // Thread-private accumulator column in shared memory: row r holds
+    // channel c0 + r - 2, so tap t of centre slot j lands on row j + t.
+    if (SORTED) {
+      if (j != cj) {  // uniform over the CTA; j > cj
+        float *a = acc_s + cj * nthr + tid;
+        a[0] += q0;
+        if (j == cj + 1) {
+          q0 = q1;
+          q1 = q2;
+        } else {
+          a[nthr] += q1;
+          if (j == cj + 2) {
+            q0 = q2;
+          } else {
+            a[2 * nthr] += q2;
+            q0 = 0.f;
+          }
+          q1 = 0.f;
+        }
+        q2 = 0.f;
+        cj = j;
+      }
+      q0 = fmaf(rb.y, det, q0);
+      q1 = fmaf(rb.z, det, q1);
+      q2 = fmaf(rb.w, det, q2);
+    } else {
+      float *a = acc_s + j * nthr + tid;
+      a[0] = fmaf(rb.y, det, a[0]);
+      a[nthr] = fmaf(rb.z, det, a[nthr]);
+      a[2 * nthr] = fmaf(rb.w, det, a[2 * nthr]);
+    }
+  }
+}
+
 // The batches of one round: n records in shared memory, processed kFwdEB at
 // a time.  Staging writes the batch's cylinders, scaled by 1 / cos(phi) per
 // slice, into the zero-padded stage; then thread m forms detector row m's
 // vertical fan for every pixel of the batch and adds its three channel taps
 // into its accumulator column acc_s[r * nthr + m], r = 0 .. kFwdCB + 3.
-// Every batch ends with all threads past a barrier.
+// SORTED: the round's records come in nondecreasing centre channel, so the
+// three rows a pixel adds to stay in registers (q0..q2 for rows cj .. cj + 2)
+// until the centre moves on; a row that leaves is added into its column
+// once.  Every batch ends with all threads past a barrier.
+template <bool SORTED>
 __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec, int n,
                                              float *__restrict__ stage, int SP,
                                              const float *__restrict__ values, int band,
@@ -647,24 +721,29 @@ __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec,
                                              int R, int c0, float *__restrict__ acc_s) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   const float mf = (float)tid;
+  int cj = SORTED ? __float_as_int(rec[0].c.z) - c0 + 1 : 0;
+  float q0 = 0.f, q1 = 0.f, q2 = 0.f;
   for (int b0 = 0; b0 < n; b0 += kFwdEB) {
     const int nb = min(kFwdEB, n - b0);
     if (2 * band >= nthr) {
       // slice-major: thread t stages slice t (+ nthr ...) of every pixel of
-      // the batch, with all kFwdEB loads in flight before the first use.
+      // the batch, with the batch's loads in flight before the first use.
+      // A short batch leaves the unrolled loops early (nb is uniform), so it
+      // issues only its own nb slots.
       for (int k = tid; k < band; k += nthr) {
         float val[kFwdEB];
 #pragma unroll
-        for (int e = 0; e < kFwdEB; ++e)
-          val[e] = e < nb ? __ldg(values + (size_t)__float_as_int(rec[b0 + e].c.w) * band + k)
-                          : 0.f;
+        for (int e = 0; e < kFwdEB; ++e) {
+          if (e >= nb) break;
+          val[e] = __ldg(values + (size_t)__float_as_int(rec[b0 + e].c.w) * band + k);
+        }
         const float kf = (float)(slice_start + k);
+        float *sk = stage + kFwdVPad + k;
 #pragma unroll
         for (int e = 0; e < kFwdEB; ++e) {
-          if (e < nb) {
-            const float4 c = rec[b0 + e].c;
-            stage[e * SP + kFwdVPad + k] = val[e] * inv_cos_from_t(fmaf(c.y, kf, c.x));
-          }
+          if (e >= nb) break;
+          const float4 c = rec[b0 + e].c;
+          sk[e * SP] = val[e] * inv_cos_from_t(fmaf(c.y, kf, c.x));
         }
       }
     } else {
@@ -678,45 +757,20 @@ __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec,
     }
     __syncthreads();
     if (tid < R) {
-#pragma unroll 2
-      for (int e = 0; e < nb; ++e) {
-        const ConeFwdRec *r = rec + b0 + e;
-        const float4 ra = r->a, rb = r->b;
-        const int j = __float_as_int(r->c.z) - c0 + 1;  // in [0, kFwdCB + 1]
-        const float m0 = ra.x, w_r = ra.y, hw1r = ra.z, lmaxr = ra.w;
-        const float k_m = (mf - m0) * rb.x;
-        const float kc = fminf(fmaxf(rintf(k_m), kc_lo), kc_hi);
-        const float d = w_r * (kc - k_m);
-        const float *st = stage + e * SP + kFwdVPad + ((int)kc - slice_start);
-        float det;
-        if (bp == 1 && lmaxr == 1.f) {
-          const float am = trap_w<true>(hw1r - fabsf(d - w_r), lmaxr);
-          const float a0 = trap_w<true>(hw1r - fabsf(d), lmaxr);
-          const float ap = trap_w<true>(hw1r - fabsf(d + w_r), lmaxr);
-          det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
-        } else if (bp == 1) {
-          const float am = trap_w<false>(hw1r - fabsf(d - w_r), lmaxr);
-          const float a0 = trap_w<false>(hw1r - fabsf(d), lmaxr);
-          const float ap = trap_w<false>(hw1r - fabsf(d + w_r), lmaxr);
-          det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
-        } else {
-          det = 0.f;
-          for (int ko = -bp; ko <= bp; ++ko) {
-            const float a = fminf(fmaxf(hw1r - fabsf(fmaf(w_r, (float)ko, d)), 0.f), lmaxr);
-            det = fmaf(a, st[ko], det);
-          }
-        }
-        // Thread-private accumulator column in shared memory: row r holds
-        // channel c0 + r - 2, so tap t of centre slot j lands on row j + t
-        // (the same FMA sequence per channel as register accumulators, with
-        // no branch on the pixel's channel).
-        float *a = acc_s + j * nthr + tid;
-        a[0] = fmaf(rb.y, det, a[0]);
-        a[nthr] = fmaf(rb.z, det, a[nthr]);
-        a[2 * nthr] = fmaf(rb.w, det, a[2 * nthr]);
-      }
+      if (bp == 1)
+        fwd_rt_batch<1, SORTED>(rec + b0, nb, stage, SP, mf, kc_lo, kc_hi, slice_start, bp, c0,
+                                acc_s, cj, q0, q1, q2);
+      else
+        fwd_rt_batch<0, SORTED>(rec + b0, nb, stage, SP, mf, kc_lo, kc_hi, slice_start, bp, c0,
+                                acc_s, cj, q0, q1, q2);
     }
     __syncthreads();
+  }
+  if (SORTED && tid < R) {
+    float *a = acc_s + cj * nthr + tid;
+    a[0] += q0;
+    a[nthr] += q1;
+    a[2 * nthr] += q2;
   }
 }
 
@@ -749,7 +803,12 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
   const float kc_lo = (float)(slice_start - bp - 1),
               kc_hi = (float)(slice_start + band + bp);
 
-  for (int i = tid; i < kFwdEB * SP; i += nthr) stage[i] = 0.f;
+  // Zero padding either side of each staged cylinder (the interiors are
+  // written by every batch before they are read).
+  for (int i = tid; i < kFwdEB * 2 * kFwdVPad; i += nthr) {
+    const int e = i / (2 * kFwdVPad), o = i - e * 2 * kFwdVPad;
+    stage[e * SP + (o < kFwdVPad ? o : band + o)] = 0.f;
+  }
 #pragma unroll
   for (int r = 0; r < kFwdCB + 4; ++r) acc_s[r * nthr + tid] = 0.f;
 
@@ -783,7 +842,8 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
       pos += nthr;
       __syncthreads();
     }
-    fwd_rt_round(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, c0, acc_s);
+    fwd_rt_round<false>(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, c0,
+                        acc_s);
   }
   // Epilogue: thread m hands over its row's cells.
   float acc[kFwdCB];
@@ -797,89 +857,121 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
 // ── forward projection, cone, binned ───────────────────────────────────────
 // For a pixel subset that several launches use (the VCD gradient, forward
 // and positivity re-projection), the (view, pixel) records are formed once by
-// cone_bin_kernel and bucketed by channel block, so that each forward CTA
-// reads exactly its pixels instead of scanning the subset and re-forming
-// every pixel's geometry (atan2, sin/cos, divisions) in each of the
-// C / kFwdCB blocks of a view.
+// cone_bin_kernel and sorted by centre channel, so that each forward CTA
+// reads exactly its pixels, in channel order, instead of scanning the subset
+// and re-forming every pixel's geometry (atan2, sin/cos, divisions) in each
+// of the C / kFwdCB blocks of a view.
 //
 // cone_bin_kernel: one CTA per view of the chunk [v_start, v_start + gridDim.x).
-//   recs[vl * P + p]                 record of subset slot p
-//   list[vl * 2P + ...]              slots per channel block, in increasing slot order
-//   offs[vl * (nblk + 1) + b .. b + 1]   block b's range of list
-// Slots are placed by a deterministic prefix over (chunk, warp, tap side,
-// lane): no atomics decide an order.
+//   recs[vl * P + p]                     record of subset slot p
+//   list[vl * P + ...]                   slots by key = ctr + 1 (ctr in [-1, C]),
+//                                        equal keys in increasing slot order
+//   offs[vl * (C + 3) + k .. k + 1]      key k's range of list
+// A pixel whose centre lies outside [-1, C] has no tap on the detector and
+// is in no key.  Channel block b (channels c0 .. c0 + 15) is reached by the
+// centres c0 - 1 .. c0 + 16: the keys c0 .. c0 + 17, one contiguous range.
+// Slots are placed by a deterministic prefix over (chunk, warp, lane): no
+// atomics decide an order.
+__host__ __device__ inline int fwd_nkeys(int C) { return C + 2; }
+
+__device__ __forceinline__ int fwd_key(int ctr, int C) {
+  return (ctr >= -1 && ctr <= C) ? ctr + 1 : -1;
+}
+
+// Exclusive prefix of a[0 .. n) in place (block-wide; every thread calls
+// it); returns the total.  Thread t scans a contiguous run of keys.
+__device__ __forceinline__ int block_exclusive_scan(int *a, int n, int *warp_tot) {
+  const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int per = (n + nthr - 1) / nthr;
+  const int lo = min(n, tid * per), hi = min(n, lo + per);
+  int s = 0;
+  for (int i = lo; i < hi; ++i) s += a[i];
+  int x = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int t = lane < (nthr >> 5) ? warp_tot[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    warp_tot[lane] = t;  // inclusive over warps
+  }
+  __syncthreads();
+  int run = x - s + (warp > 0 ? warp_tot[warp - 1] : 0);
+  const int total = warp_tot[(nthr >> 5) - 1];
+  for (int i = lo; i < hi; ++i) {
+    const int c = a[i];
+    a[i] = run;
+    run += c;
+  }
+  __syncthreads();
+  return total;
+}
+
 __global__ void __launch_bounds__(256)
 cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
-                const int64_t *__restrict__ pix, int P, int by_pixel, int nblk,
+                const int64_t *__restrict__ pix, int P, int by_pixel,
                 ConeFwdRec *__restrict__ recs, int *__restrict__ list, int *__restrict__ offs) {
   extern __shared__ int bsm[];
+  __shared__ int warp_tot[32];
   const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nvw = 2 * (nthr >> 5);  // virtual warps: (warp, tap side)
-  int *cursor = bsm;                // nblk
-  int *wc = bsm + nblk;             // nvw x nblk
+  const int nw = nthr >> 5;
+  const int nkeys = fwd_nkeys(g.C);
+  int *cursor = bsm;        // nkeys
+  int *wc = bsm + nkeys;    // nw x nkeys
   const int vl = blockIdx.x, v = v_start + vl;
   const float ang = vp[2 * v];
   const float cs = cosf(ang), sn = sinf(ang);
   const float z_off = __fsub_rn(g.rso, vp[2 * v + 1]);
   ConeFwdRec *vrec = recs + (size_t)vl * P;
-  int *vlist = list + (size_t)vl * 2 * P;
-  int *voffs = offs + (size_t)vl * (nblk + 1);
+  int *vlist = list + (size_t)vl * P;
+  int *voffs = offs + (size_t)vl * (nkeys + 1);
 
-  for (int b = tid; b < nblk; b += nthr) cursor[b] = 0;
+  for (int k = tid; k < nkeys; k += nthr) cursor[k] = 0;
   __syncthreads();
-  // Pass 1: records and per-block counts (the counts do not depend on the
+  // Pass 1: records and per-key counts (the counts do not depend on the
   // order of the shared-memory increments).
   for (int p = tid; p < P; p += nthr) {
     float xt, yt;
     pixel_xy(g, (int)pix[p], xt, yt);
     const ConeCenter cc = cone_center(g, cs, sn, xt, yt);
     vrec[p] = cone_fwd_record(g, ang, z_off, cc, by_pixel ? (int)pix[p] : p);
-    int b_lo, b_hi;
-    fwd_block_range(cc.ctr, g.C, b_lo, b_hi);
-    if (b_lo >= 0) atomicAdd(&cursor[b_lo], 1);
-    if (b_hi > b_lo) atomicAdd(&cursor[b_hi], 1);
+    const int key = fwd_key(cc.ctr, g.C);
+    if (key >= 0) atomicAdd(&cursor[key], 1);
   }
   __syncthreads();
-  if (tid == 0) {
-    int s = 0;
-    for (int b = 0; b < nblk; ++b) {
-      const int c = cursor[b];
-      cursor[b] = s;
-      voffs[b] = s;
-      s += c;
-    }
-    voffs[nblk] = s;
-  }
-  __syncthreads();
+  const int total = block_exclusive_scan(cursor, nkeys, warp_tot);
+  for (int k = tid; k < nkeys; k += nthr) voffs[k] = cursor[k];
+  if (tid == 0) voffs[nkeys] = total;
   // Pass 2: stable placement, one chunk of nthr slots at a time (a thread
-  // reads back the records it wrote itself in pass 1).
+  // reads back the record it wrote itself in pass 1).
   const unsigned lt = (1u << lane) - 1u;
   for (int base = 0; base < P; base += nthr) {
     const int p = base + tid;
-    int b0 = -1, b1 = -1;
-    if (p < P) {
-      fwd_block_range(__float_as_int(vrec[p].c.z), g.C, b0, b1);
-      if (b1 == b0) b1 = -1;
-    }
-    for (int i = tid; i < nvw * nblk; i += nthr) wc[i] = 0;
+    const int key = p < P ? fwd_key(__float_as_int(vrec[p].c.z), g.C) : -1;
+    for (int i = tid; i < nw * nkeys; i += nthr) wc[i] = 0;
     __syncthreads();
-    const unsigned peers0 = __match_any_sync(0xffffffffu, b0);
-    const unsigned peers1 = __match_any_sync(0xffffffffu, b1);
-    if (b0 >= 0 && (peers0 & lt) == 0) wc[(2 * warp) * nblk + b0] = __popc(peers0);
-    if (b1 >= 0 && (peers1 & lt) == 0) wc[(2 * warp + 1) * nblk + b1] = __popc(peers1);
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (key >= 0 && (peers & lt) == 0) wc[warp * nkeys + key] = __popc(peers);
     __syncthreads();
-    for (int b = tid; b < nblk; b += nthr) {
-      int s = cursor[b];
-      for (int j = 0; j < nvw; ++j) {
-        const int c = wc[j * nblk + b];
-        wc[j * nblk + b] = s;
+    for (int k = tid; k < nkeys; k += nthr) {
+      int s = cursor[k];
+      for (int j = 0; j < nw; ++j) {
+        const int c = wc[j * nkeys + k];
+        wc[j * nkeys + k] = s;
         s += c;
       }
-      cursor[b] = s;
+      cursor[k] = s;
     }
     __syncthreads();
-    if (b0 >= 0) vlist[wc[(2 * warp) * nblk + b0] + __popc(peers0 & lt)] = p;
-    if (b1 >= 0) vlist[wc[(2 * warp + 1) * nblk + b1] + __popc(peers1 & lt)] = p;
+    if (key >= 0) vlist[wc[warp * nkeys + key] + __popc(peers & lt)] = p;
     __syncthreads();
   }
 }
@@ -908,9 +1000,10 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
   const float kc_lo = (float)(slice_start - bp - 1),
               kc_hi = (float)(slice_start + band + bp);
   const ConeFwdRec *vrec = recs + (size_t)vl * P;
-  const int *vlist = list + (size_t)vl * 2 * P;
-  const int start = offs[(size_t)vl * (nblk + 1) + blk];
-  const int end = offs[(size_t)vl * (nblk + 1) + blk + 1];
+  const int *vlist = list + (size_t)vl * P;
+  const int *voffs = offs + (size_t)vl * (fwd_nkeys(g.C) + 1);
+  const int start = voffs[c0];
+  const int end = voffs[min(c0 + kFwdCB + 2, fwd_nkeys(g.C))];
   const int v = v_start + vl;
   if (tid == 0) touched[(size_t)v * nblk + blk] = end > start;
   if (end == start) {
@@ -921,7 +1014,12 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
     return;
   }
 
-  for (int i = tid; i < kFwdEB * SP; i += nthr) stage[i] = 0.f;
+  // Zero padding either side of each staged cylinder (the interiors are
+  // written by every batch before they are read).
+  for (int i = tid; i < kFwdEB * 2 * kFwdVPad; i += nthr) {
+    const int e = i / (2 * kFwdVPad), o = i - e * 2 * kFwdVPad;
+    stage[e * SP + (o < kFwdVPad ? o : band + o)] = 0.f;
+  }
 #pragma unroll
   for (int r = 0; r < kFwdCB + 4; ++r) acc_s[r * nthr + tid] = 0.f;
   // The epilogue's operands (the error sinogram's cells of this tile) are
@@ -934,12 +1032,14 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
     __syncthreads();
     // The round's cylinders, 128-byte line by line, toward L1 ahead of the
     // batch staging.
-    const int lines = (band * (int)sizeof(float) + 127) / 128;
-    for (int i = tid; i < n * lines; i += nthr) {
-      const int e = i / lines, ln = i - e * lines;
-      prefetch_l1(values + (size_t)__float_as_int(rec[e].c.w) * band + ln * 32);
+    {
+      const int lane = tid & 31, lines = (band + 31) / 32;
+      for (int e = tid >> 5; e < n; e += nthr >> 5)
+        for (int ln = lane; ln < lines; ln += 32)
+          prefetch_l1(values + (size_t)__float_as_int(rec[e].c.w) * band + ln * 32);
     }
-    fwd_rt_round(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, c0, acc_s);
+    fwd_rt_round<true>(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R, c0,
+                       acc_s);
   }
   float acc[kFwdCB];
 #pragma unroll
