@@ -492,7 +492,8 @@ template <typename T>
 int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params *prm,
                  float *flat, T *err, const float *es, const T *wts, const float *wsc,
                  const float *H, const float *dc, const int64_t *pix, long long Ps,
-                 double *accum, float *alpha_user, VcdWs &w, cudaStream_t st) {
+                 double *accum, float *alpha_user, VcdWs &w, cudaStream_t st,
+                 const int64_t *next_pix, bool prebinned, bool *binned_next) {
   const int S = g->num_slices, V = g->num_views, C = g->num_det_channels, R = g->num_det_rows;
   const size_t PS = (size_t)Ps * S;
   const VcdScalars sc = make_scalars(*prm);
@@ -500,8 +501,10 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   int rc;
   // 0. the subset's (view, pixel) records, sorted by centre channel; when one
   //    chunk holds every view the gradient reads them too.
+  //    A partition pass may have formed them already in the previous step's
+  //    tail (`prebinned`).
   const bool shared_bins = w.binned && w.bins.views >= V && g->psf_radius == 1;
-  if (shared_bins) {
+  if (shared_bins && !prebinned) {
     rc = launch_bin(g, vp, 0, V, pix, Ps, w.bins, st);
     if (rc) return rc;
   }
@@ -569,22 +572,41 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
     if (rc) return rc;
   }
   // 5. update
+  if (w.binned) {
+    // Recon update and the sinogram's touched tiles (elsewhere A delta is
+    // zero and e is unchanged) in one launch, with the next subset's bins
+    // when the pass has one and they fit one chunk.
+    const int nblk = fwd_nblk(g);
+    const int nbin = (shared_bins && next_pix != nullptr) ? V : 0;
+    const TailBins tb{make_geo(*g), vp, next_pix, (int)Ps, w.bins.recs, w.bins.list,
+                      w.bins.offs};
+    const size_t smem = nbin ? bin_smem(g) : 0;
+    auto k = vcd_tail_kernel<T>;
+    if (smem > 48 * 1024) {
+      const cudaError_t e =
+          cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess)
+        return fail(MBIR_ERR_CUDA, "VCD update: shared memory request of %zu bytes refused: %s",
+                    smem, cudaGetErrorString(e));
+    }
+    const long long ctas = (long long)nbin + (long long)w.upd_chunks * w.upd_yblocks +
+                           (long long)nblk * V;
+    tpre(st);
+    k<<<(unsigned)ctas, 256, smem, st>>>(nbin, tb, (int)Ps, S, kUpdChunk, pix, w.delta, w.alpha,
+                                          flat, w.sq_part, w.l1_part, w.counters + 1, accum,
+                                          w.upd_chunks, w.upd_yblocks, C, R, kFwdCB,
+                                          w.bins.touched, err, static_cast<const T *>(w.ad),
+                                          nblk);
+    MBIR_CHECK_LAUNCH("vcd pixel + sinogram update");
+    if (binned_next) *binned_next = nbin > 0;
+    return MBIR_OK;
+  }
   dim3 gu(w.upd_chunks, w.upd_yblocks);
   tpre(st);
   vcd_pixel_update_kernel<<<gu, kThreads, 0, st>>>((int)Ps, S, kUpdChunk, pix, w.delta, w.alpha,
                                                    flat, w.sq_part, w.l1_part, w.counters + 1,
                                                    accum);
   MBIR_CHECK_LAUNCH("vcd pixel update");
-  if (w.binned) {
-    // Only the (view, channel-block) tiles the subset reached: elsewhere
-    // A delta is zero and e is unchanged.
-    const int nblk = fwd_nblk(g);
-    tpre(st);
-    vcd_sino_update_tiles_kernel<T><<<dim3(nblk, V), 256, 0, st>>>(
-        C, R, kFwdCB, w.bins.touched, w.alpha, err, static_cast<const T *>(w.ad));
-    MBIR_CHECK_LAUNCH("vcd sinogram update");
-    return MBIR_OK;
-  }
   const size_t n = (size_t)V * C * R;
   const int blocks = (int)std::min<size_t>((n / 4 + 255) / 256 + 1, 148 * 32);
   tpre(st);
@@ -918,7 +940,8 @@ int32_t subset_update(const mbir_geometry *geom, const float *view_params,
                       const float *fm_hessian, const float *dc_profile,
                       const int64_t *pixel_indices, int64_t num_pixels, double *accum,
                       float *alpha_out, void *workspace, size_t workspace_bytes, void *stream,
-                      bool fresh) {
+                      bool fresh, const int64_t *next_pix = nullptr, bool prebinned = false,
+                      bool *binned_next = nullptr) {
   int rc = validate_vcd(geom, params, flat_recon, error_sino, err_scale, weights, w_scale,
                         fm_hessian, num_pixels);
   if (rc) return rc;
@@ -938,18 +961,20 @@ int32_t subset_update(const mbir_geometry *geom, const float *view_params,
       return vcd_subset_t<float>(geom, view_params, params, flat_recon,
                                  static_cast<float *>(error_sino), err_scale,
                                  static_cast<const float *>(weights), w_scale, fm_hessian,
-                                 dc_profile, pixel_indices, num_pixels, accum, alpha_out, w, st);
+                                 dc_profile, pixel_indices, num_pixels, accum, alpha_out, w, st,
+                                 next_pix, prebinned, binned_next);
     case MBIR_BF16:
       return vcd_subset_t<__nv_bfloat16>(geom, view_params, params, flat_recon,
                                          static_cast<__nv_bfloat16 *>(error_sino), err_scale,
                                          static_cast<const __nv_bfloat16 *>(weights), w_scale,
                                          fm_hessian, dc_profile, pixel_indices, num_pixels, accum,
-                                         alpha_out, w, st);
+                                         alpha_out, w, st, next_pix, prebinned, binned_next);
     default:
       return vcd_subset_t<__half>(geom, view_params, params, flat_recon,
                                   static_cast<__half *>(error_sino), err_scale,
                                   static_cast<const __half *>(weights), w_scale, fm_hessian,
-                                  dc_profile, pixel_indices, num_pixels, accum, alpha_out, w, st);
+                                  dc_profile, pixel_indices, num_pixels, accum, alpha_out, w, st,
+                                 next_pix, prebinned, binned_next);
   }
 }
 }  // namespace
@@ -978,12 +1003,18 @@ int32_t mbir_vcd_partition_pass(const mbir_geometry *geom, const float *view_par
   for (int i = 0; i < num_subsets; ++i)
     if (order[i] < 0 || order[i] >= num_subsets)
       return fail(MBIR_ERR_INVALID, "order[%d] = %d outside [0, %d)", i, order[i], num_subsets);
+  // Each step's tail bins the next subset when the bins allow it.
+  bool prebinned = false;
   for (int i = 0; i < num_subsets; ++i) {
+    const int64_t *next =
+        i + 1 < num_subsets ? partition + (size_t)order[i + 1] * subset_pixels : nullptr;
+    bool binned_next = false;
     const int rc = subset_update(
         geom, view_params, params, flat_recon, error_sino, err_scale, weights, w_scale,
         fm_hessian, dc_profile, partition + (size_t)order[i] * subset_pixels, subset_pixels, accum,
-        nullptr, workspace, workspace_bytes, stream, i == 0);
+        nullptr, workspace, workspace_bytes, stream, i == 0, next, prebinned, &binned_next);
     if (rc) return rc;
+    prebinned = binned_next;
   }
   return MBIR_OK;
 }

@@ -915,18 +915,21 @@ __device__ __forceinline__ int block_exclusive_scan(int *a, int n, int *warp_tot
   return total;
 }
 
-__global__ void __launch_bounds__(256)
-cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
-                const int64_t *__restrict__ pix, int P, int by_pixel,
-                ConeFwdRec *__restrict__ recs, int *__restrict__ list, int *__restrict__ offs) {
-  extern __shared__ int bsm[];
+// One CTA's work of cone_bin_kernel: view vl of the chunk, with bsm the
+// (1 + warps) x (C + 2) ints of dynamic shared memory.
+__device__ __forceinline__ void cone_bin_view(const Geo &g, const float *__restrict__ vp,
+                                              int v_start, int vl,
+                                              const int64_t *__restrict__ pix, int P,
+                                              int by_pixel, ConeFwdRec *__restrict__ recs,
+                                              int *__restrict__ list, int *__restrict__ offs,
+                                              int *bsm) {
   __shared__ int warp_tot[32];
   const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nw = nthr >> 5;
   const int nkeys = fwd_nkeys(g.C);
   int *cursor = bsm;        // nkeys
   int *wc = bsm + nkeys;    // nw x nkeys
-  const int vl = blockIdx.x, v = v_start + vl;
+  const int v = v_start + vl;
   const float ang = vp[2 * v];
   const float cs = cosf(ang), sn = sinf(ang);
   const float z_off = __fsub_rn(g.rso, vp[2 * v + 1]);
@@ -974,6 +977,14 @@ cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
     if (key >= 0) vlist[wc[warp * nkeys + key] + __popc(peers & lt)] = p;
     __syncthreads();
   }
+}
+
+__global__ void __launch_bounds__(256)
+cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
+                const int64_t *__restrict__ pix, int P, int by_pixel,
+                ConeFwdRec *__restrict__ recs, int *__restrict__ list, int *__restrict__ offs) {
+  extern __shared__ int bsm[];
+  cone_bin_view(g, vp, v_start, blockIdx.x, pix, P, by_pixel, recs, list, offs, bsm);
 }
 
 // Forward CTA (channel block, view of the chunk) over its bucket.  The

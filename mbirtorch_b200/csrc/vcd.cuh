@@ -430,16 +430,22 @@ __global__ void vcd_positivity_kernel(int P, int S, const int64_t *__restrict__ 
 
 // ── 5. update ────────────────────────────────────────────────────────────
 constexpr int kUpdPix = 8;  // pixels per load batch of the recon update
-// Recon scatter-add over a (pixel chunk, slice block) tile; per-slice sum of
-// squares and ell1 partials.
-__global__ void __launch_bounds__(kThreads)
-vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pix,
-                        const float *__restrict__ delta, const float *__restrict__ alpha,
-                        float *__restrict__ flat, double *__restrict__ sq_part,
-                        double *__restrict__ l1_part, unsigned int *__restrict__ counter,
-                        double *__restrict__ accum) {
-  const int l = blockIdx.y * kThreads + threadIdx.x;
-  const int chunk = blockIdx.x;
+
+// One CTA (bx, by) of the pixel update over a (gx, gy) grid: x += alpha
+// delta at the subset's voxels, the per-slice sums of squares and the l1
+// partials; the last CTA to arrive folds them into accum.
+__device__ __forceinline__ void pixel_update_cta(int P, int S, int pchunk,
+                                                 const int64_t *__restrict__ pix,
+                                                 const float *__restrict__ delta,
+                                                 const float *__restrict__ alpha,
+                                                 float *__restrict__ flat,
+                                                 double *__restrict__ sq_part,
+                                                 double *__restrict__ l1_part,
+                                                 unsigned int *__restrict__ counter,
+                                                 double *__restrict__ accum, int bx, int by,
+                                                 int gx, int gy) {
+  const int l = by * kThreads + threadIdx.x;
+  const int chunk = bx;
   const int p0 = chunk * pchunk, p1 = min(P, p0 + pchunk);
   const float a = alpha[0];
   double sq = 0.0, l1 = 0.0;
@@ -469,11 +475,11 @@ vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pi
   }
   double dummy = 0.0;
   block_sum2(l1, dummy);
-  if (threadIdx.x == 0) l1_part[(size_t)blockIdx.y * gridDim.x + chunk] = l1;
+  if (threadIdx.x == 0) l1_part[(size_t)by * gx + chunk] = l1;
   // The last CTA folds all partials into the accumulators (fixed order):
   // accum[0] += ell1, accum[1] += alpha, accum[2 + l] += sum_p ds^2.
-  if (last_cta(counter, gridDim.x * gridDim.y)) {
-    const int nchunks = gridDim.x, nl1 = gridDim.x * gridDim.y;
+  if (last_cta(counter, gx * gy)) {
+    const int nchunks = gx, nl1 = gx * gy;
     for (int ls = threadIdx.x; ls < S; ls += blockDim.x) {
       double s2 = 0.0;
 #pragma unroll 8
@@ -490,6 +496,18 @@ vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pi
       *counter = 0u;
     }
   }
+}
+
+// Recon scatter-add over a (pixel chunk, slice block) tile; per-slice sum of
+// squares and ell1 partials.
+__global__ void __launch_bounds__(kThreads)
+vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pix,
+                        const float *__restrict__ delta, const float *__restrict__ alpha,
+                        float *__restrict__ flat, double *__restrict__ sq_part,
+                        double *__restrict__ l1_part, unsigned int *__restrict__ counter,
+                        double *__restrict__ accum) {
+  pixel_update_cta(P, S, pchunk, pix, delta, alpha, flat, sq_part, l1_part, counter, accum,
+                   blockIdx.x, blockIdx.y, gridDim.x, gridDim.y);
 }
 
 // e -= alpha * Ad over the whole resident sinogram (both share the per-view
@@ -529,16 +547,13 @@ __global__ void vcd_sino_update_kernel<float>(size_t n, const float *__restrict_
     e[i] = __fsub_rn(e[i], __fmul_rn(a, ad[i]));
 }
 
-// The same update over the (view, channel-block) tiles a binned forward
-// marked as reached (grid: blocks x views).  A tile is CB consecutive
-// channels of one view, i.e. one contiguous run of CB * R cells.
+// One tile (channel block b, view v) of the touched-tile sinogram update.
 template <typename T>
-__global__ void __launch_bounds__(256)
-vcd_sino_update_tiles_kernel(int C, int R, int CB, const unsigned char *__restrict__ touched,
-                             const float *__restrict__ alpha, T *__restrict__ e,
-                             const T *__restrict__ ad) {
-  const int b = blockIdx.x, v = blockIdx.y;
-  if (!touched[(size_t)v * gridDim.x + b]) return;
+__device__ __forceinline__ void sino_tile_cta(int C, int R, int CB,
+                                              const unsigned char *__restrict__ touched,
+                                              const float *__restrict__ alpha, T *__restrict__ e,
+                                              const T *__restrict__ ad, int b, int v, int nblk) {
+  if (!touched[(size_t)v * nblk + b]) return;
   const float a = alpha[0];
   const int c0 = b * CB;
   const int n = min(CB, C - c0) * R;
@@ -560,6 +575,62 @@ vcd_sino_update_tiles_kernel(int C, int R, int CB, const unsigned char *__restri
       if (i < n) et[i] = from_f32<T>(__fsub_rn(ev[u], __fmul_rn(a, dv[u])));
     }
   }
+}
+
+// The same update over the (view, channel-block) tiles a binned forward
+// marked as reached (grid: blocks x views).  A tile is CB consecutive
+// channels of one view, i.e. one contiguous run of CB * R cells.
+template <typename T>
+__global__ void __launch_bounds__(256)
+vcd_sino_update_tiles_kernel(int C, int R, int CB, const unsigned char *__restrict__ touched,
+                             const float *__restrict__ alpha, T *__restrict__ e,
+                             const T *__restrict__ ad) {
+  sino_tile_cta(C, R, CB, touched, alpha, e, ad, blockIdx.x, blockIdx.y, gridDim.x);
+}
+
+// The bins of the next subset of a partition pass (cone_bin_kernel's
+// arguments for view chunk 0).
+struct TailBins {
+  Geo g;
+  const float *vp;
+  const int64_t *pix;
+  int P;
+  ConeFwdRec *recs;
+  int *list, *offs;
+};
+
+// The work of a binned subset step after alpha, in one launch: CTAs
+// [0, nbin) bin the next subset of a partition pass (cone_bin_view, one
+// view each; nbin = 0 when there is none), the next ux * uy CTAs update the
+// recon (pixel_update_cta) and the rest update the sinogram's touched tiles
+// (sino_tile_cta, nblk x V).  The three roles share no buffer, so the
+// latency-bound binning and recon update run under the HBM-bound tile
+// update.  Dynamic shared memory: the binning's key counters.  Six CTAs
+// per SM (at most 40 registers) keep enough of the tile update's loads in
+// flight to hold the copy bandwidth.
+template <typename T>
+__global__ void __launch_bounds__(256, 6)
+vcd_tail_kernel(int nbin, TailBins tb, int P, int S, int pchunk, const int64_t *__restrict__ pix,
+                const float *__restrict__ delta, const float *__restrict__ alpha,
+                float *__restrict__ flat, double *__restrict__ sq_part,
+                double *__restrict__ l1_part, unsigned int *__restrict__ counter,
+                double *__restrict__ accum, int ux, int uy, int C, int R, int CB,
+                const unsigned char *__restrict__ touched, T *__restrict__ e,
+                const T *__restrict__ ad, int nblk) {
+  extern __shared__ int tail_sm[];
+  int b = blockIdx.x;
+  if (b < nbin) {
+    cone_bin_view(tb.g, tb.vp, 0, b, tb.pix, tb.P, 0, tb.recs, tb.list, tb.offs, tail_sm);
+    return;
+  }
+  b -= nbin;
+  if (b < ux * uy) {
+    pixel_update_cta(P, S, pchunk, pix, delta, alpha, flat, sq_part, l1_part, counter, accum,
+                     b % ux, b / ux, ux, uy);
+    return;
+  }
+  b -= ux * uy;
+  sino_tile_cta<T>(C, R, CB, touched, alpha, e, ad, b % nblk, b / nblk, nblk);
 }
 
 // ── QGGMRF denoiser (identity forward model; denoising.py:35-83) ──────────
