@@ -73,6 +73,39 @@ int fail(int code, const char *fmt, ...) {
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Programmatic dependent launch inside a VCD step or denoise pass: while a
+// PdlScope is open on this thread, launch() lets each kernel begin as the
+// stream's previous kernel winds down (the kernels open with
+// MBIR_PDL_ENTRY, which waits for that kernel's writes).  Per-launch timing
+// keeps ordinary launches so that each event pair brackets one kernel.
+thread_local bool t_pdl = false;
+struct PdlScope {
+  bool prev;
+  PdlScope() : prev(t_pdl) { t_pdl = true; }
+  ~PdlScope() { t_pdl = prev; }
+};
+
+// Launch errors surface through cudaGetLastError (MBIR_CHECK_LAUNCH).
+template <typename... KArgs, typename... Args>
+void launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+            Args... args) {
+  if (!t_pdl || g_timing.load(std::memory_order_relaxed)) {
+    k<<<grid, block, smem, st>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  (void)cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+
 inline int next_pow2(int x) {
   int p = 1;
   while (p < x) p <<= 1;
@@ -179,12 +212,12 @@ int launch_back_t(const Geo &geo, const mbir_geometry *g, const float *vp, int v
     auto k = back_cone_kernel<CP, SPL, NT, RD>;
     if (s.smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     tpre(st);
-    k<<<grid, kThreads, s.smem, st>>>(geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P,
-                                      slice_start, band, s.slice_chunks, dst, recs);
+    launch(k, grid, kThreads, s.smem, st, geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P,
+           slice_start, band, s.slice_chunks, dst, recs);
   } else {
     tpre(st);
-    back_parallel_kernel<CP, SPL, NT, RD><<<grid, kThreads, 0, st>>>(
-        geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P, band, s.T, s.slice_chunks, dst);
+    launch(back_parallel_kernel<CP, SPL, NT, RD>, grid, kThreads, 0, st, geo, vp, v_start,
+           v_count, s.vpc, rd, pix, (int)P, band, s.T, s.slice_chunks, dst);
   }
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
@@ -238,7 +271,7 @@ int run_back(const mbir_geometry *g, const float *vp, int v_start, int v_count, 
     const size_t n = (size_t)P * band;
     const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
     tpre(st);
-    reduce_chunks_kernel<<<blocks, 256, 0, st>>>(partials, s.nchunks, n, out);
+    launch(reduce_chunks_kernel, blocks, 256, 0, st, (const float *)partials, s.nchunks, n, out);
     MBIR_CHECK_LAUNCH("chunk reduction");
   }
   return MBIR_OK;
@@ -274,8 +307,8 @@ int launch_forward(const mbir_geometry *g, const float *vp, int v_start, int v_c
   }
   dim3 grid((g->num_det_channels + fs.CB - 1) / fs.CB, v_count);
   tpre(st);
-  k<<<grid, kThreads, smem, st>>>(geo, vp, v_start, values, (int)P, band, slice_start, pix, fs,
-                                  by_pixel, epi);
+  launch(k, grid, kThreads, smem, st, geo, vp, v_start, values, (int)P, band, slice_start, pix, fs,
+         by_pixel, epi);
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
 }
@@ -311,8 +344,8 @@ int launch_cone_rt(const mbir_geometry *g, const float *vp, int v_start, int v_c
   }
   dim3 grid((g->num_det_channels + kFwdCB - 1) / kFwdCB, v_count);
   tpre(st);
-  k<<<grid, cone_rt_threads(g), smem, st>>>(geo, vp, v_start, values, (int)P, band, slice_start,
-                                             pix, by_pixel, epi);
+  launch(k, grid, cone_rt_threads(g), smem, st, geo, vp, v_start, values, (int)P, band,
+         slice_start, pix, by_pixel, epi);
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
 }
@@ -359,8 +392,8 @@ int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count
                   smem, cudaGetErrorString(e));
   }
   tpre(st);
-  cone_bin_kernel<<<v_count, kThreads, smem, st>>>(geo, vp, v_start, pix, (int)P, 0, b.recs,
-                                                   b.list, b.offs);
+  launch(cone_bin_kernel, v_count, kThreads, smem, st, geo, vp, v_start, pix, (int)P, 0, b.recs,
+         b.list, b.offs);
   MBIR_CHECK_LAUNCH("vcd forward binning");
   return MBIR_OK;
 }
@@ -380,8 +413,8 @@ int launch_binned(const mbir_geometry *g, int v_start, int v_count, const float 
   }
   dim3 grid(fwd_nblk(g), v_count);
   tpre(st);
-  k<<<grid, cone_rt_threads(g), smem, st>>>(geo, v_start, values, (int)P, band, 0, b.recs,
-                                             b.list, b.offs, b.touched, epi);
+  launch(k, grid, cone_rt_threads(g), smem, st, geo, v_start, values, (int)P, band, 0,
+         (const ConeFwdRec *)b.recs, (const int *)b.list, (const int *)b.offs, b.touched, epi);
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
 }
@@ -524,27 +557,25 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   const int nb = w.prior_blocks;
   if (!DCon) {
     tpre(st);
-    vcd_direction_kernel<false><<<nb, kThreads, 0, st>>>(
-        (int)Ps, S, pix, g->num_recon_rows, g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H,
-        sc, w.delta, nullptr, nullptr, nullptr, nullptr, w.prior_part);
+    launch(vcd_direction_kernel<false>, nb, kThreads, 0, st, (int)Ps, S, pix, g->num_recon_rows,
+           g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H, sc, w.delta, nullptr, nullptr,
+           nullptr, nullptr, w.prior_part);
     MBIR_CHECK_LAUNCH("vcd direction");
   } else {
     tpre(st);
-    vcd_direction_kernel<true><<<nb, kThreads, 0, st>>>(
-        (int)Ps, S, pix, g->num_recon_rows, g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H,
-        sc, nullptr, w.gbuf, w.hinv, w.gpbuf, w.hpbuf, nullptr);
+    launch(vcd_direction_kernel<true>, nb, kThreads, 0, st, (int)Ps, S, pix, g->num_recon_rows,
+           g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H, sc, nullptr, w.gbuf, w.hinv,
+           w.gpbuf, w.hpbuf, nullptr);
     MBIR_CHECK_LAUNCH("vcd direction (damped)");
     dim3 gs((S + 127) / 128, w.dc_chunks);
     tpre(st);
-    vcd_dc_sums_kernel<<<gs, 128, 0, st>>>((int)Ps, S, kDcChunk, w.gbuf, w.hinv, w.dc_sums);
+    launch(vcd_dc_sums_kernel, gs, 128, 0, st, (int)Ps, S, kDcChunk, w.gbuf, w.hinv, w.dc_sums);
     MBIR_CHECK_LAUNCH("vcd DC sums");
     tpre(st);
-    vcd_dc_direction_kernel<<<nb, kThreads, 0, st>>>((int)Ps, S, w.dc_chunks, w.dc_sums, dc,
-                                                     w.gbuf, w.hinv, w.gpbuf, w.hpbuf, w.delta,
-                                                     w.prior_part);
+    launch(vcd_dc_direction_kernel, nb, kThreads, 0, st, (int)Ps, S, w.dc_chunks, w.dc_sums, dc,
+           w.gbuf, w.hinv, w.gpbuf, w.hpbuf, w.delta, w.prior_part);
     MBIR_CHECK_LAUNCH("vcd DC direction");
   }
-  // 3. forward A delta + line-search partials
   // 3. forward A delta + line-search partials
   LineSearchEpi<T> epi{err, es, wts, wsc, static_cast<T *>(w.ad), C, R, w.fwd_part, 1, 0.0, 0.0};
   if (w.binned)
@@ -555,13 +586,13 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   if (rc) return rc;
   // 4. alpha
   tpre(st);
-  vcd_alpha_kernel<<<1, kAlphaThreads, 0, st>>>(w.prior_part, nb, w.fwd_part, w.fwd_blocks, sc.fmc,
-                                           sc.max_alpha, w.alpha, alpha_user);
+  launch(vcd_alpha_kernel, 1, kAlphaThreads, 0, st, w.prior_part, nb, w.fwd_part, w.fwd_blocks,
+         sc.fmc, sc.max_alpha, w.alpha, alpha_user);
   MBIR_CHECK_LAUNCH("vcd alpha");
   if (prm->positivity) {
     tpre(st);
-    vcd_positivity_kernel<<<(unsigned)((PS + 255) / 256), 256, 0, st>>>((int)Ps, S, pix, flat,
-                                                                        w.alpha, w.delta);
+    launch(vcd_positivity_kernel, (unsigned)((PS + 255) / 256), 256, 0, st, (int)Ps, S, pix,
+           flat, w.alpha, w.delta);
     MBIR_CHECK_LAUNCH("vcd positivity");
     LineSearchEpi<T> epi2{err, es, wts, wsc, static_cast<T *>(w.ad), C, R, nullptr, 0, 0.0, 0.0};
     if (w.binned)
@@ -592,25 +623,23 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
     const long long ctas = (long long)nbin + (long long)w.upd_chunks * w.upd_yblocks +
                            (long long)nblk * V;
     tpre(st);
-    k<<<(unsigned)ctas, 256, smem, st>>>(nbin, tb, (int)Ps, S, kUpdChunk, pix, w.delta, w.alpha,
-                                          flat, w.sq_part, w.l1_part, w.counters + 1, accum,
-                                          w.upd_chunks, w.upd_yblocks, C, R, kFwdCB,
-                                          w.bins.touched, err, static_cast<const T *>(w.ad),
-                                          nblk);
+    launch(k, (unsigned)ctas, 256, smem, st, nbin, tb, (int)Ps, S, kUpdChunk, pix, w.delta,
+           w.alpha, flat, w.sq_part, w.l1_part, w.counters + 1, accum, w.upd_chunks,
+           w.upd_yblocks, C, R, kFwdCB, w.bins.touched, err, static_cast<const T *>(w.ad), nblk);
     MBIR_CHECK_LAUNCH("vcd pixel + sinogram update");
     if (binned_next) *binned_next = nbin > 0;
     return MBIR_OK;
   }
   dim3 gu(w.upd_chunks, w.upd_yblocks);
   tpre(st);
-  vcd_pixel_update_kernel<<<gu, kThreads, 0, st>>>((int)Ps, S, kUpdChunk, pix, w.delta, w.alpha,
-                                                   flat, w.sq_part, w.l1_part, w.counters + 1,
-                                                   accum);
+  launch(vcd_pixel_update_kernel, gu, kThreads, 0, st, (int)Ps, S, kUpdChunk, pix, w.delta,
+         w.alpha, flat, w.sq_part, w.l1_part, w.counters + 1, accum);
   MBIR_CHECK_LAUNCH("vcd pixel update");
   const size_t n = (size_t)V * C * R;
   const int blocks = (int)std::min<size_t>((n / 4 + 255) / 256 + 1, 148 * 32);
   tpre(st);
-  vcd_sino_update_kernel<T><<<blocks, 256, 0, st>>>(n, w.alpha, err, static_cast<const T *>(w.ad));
+  launch(vcd_sino_update_kernel<T>, blocks, 256, 0, st, n, w.alpha, err,
+         static_cast<const T *>(w.ad));
   MBIR_CHECK_LAUNCH("vcd sinogram update");
   return MBIR_OK;
 }
@@ -951,6 +980,7 @@ int32_t subset_update(const mbir_geometry *geom, const float *view_params,
     return fail(MBIR_ERR_WORKSPACE, "VCD workspace of %zu bytes < %zu needed", workspace_bytes,
                 w.bytes);
   cudaStream_t st = as_stream(stream);
+  const PdlScope pdl;
   if (fresh) {
     const cudaError_t e = cudaMemsetAsync(w.counters, 0, 2 * sizeof(unsigned int), st);
     if (e != cudaSuccess)
@@ -1067,6 +1097,7 @@ int32_t mbir_denoise_pass(int32_t num_rows, int32_t num_cols, int32_t num_slices
     return fail(MBIR_ERR_WORKSPACE, "denoiser workspace of %zu bytes < %zu needed",
                 workspace_bytes, w.bytes);
   cudaStream_t st = as_stream(stream);
+  const PdlScope pdl;
   cudaError_t e = cudaMemsetAsync(w.counter, 0, sizeof(unsigned int), st);
   if (e != cudaSuccess)
     return fail(MBIR_ERR_CUDA, "denoiser counter reset failed: %s", cudaGetErrorString(e));
@@ -1074,18 +1105,16 @@ int32_t mbir_denoise_pass(int32_t num_rows, int32_t num_cols, int32_t num_slices
   for (int k = 0; k < num_subsets; ++k) {
     const int64_t *pix = partition + (size_t)k * subset_pixels;
     tpre(st);
-    denoise_direction_kernel<<<w.blocks, kThreads, 0, st>>>(
-        (int)subset_pixels, num_slices, pix, num_rows, num_cols, flat_image, flat_error, sc,
-        w.delta, w.prior, w.fwd);
+    launch(denoise_direction_kernel, w.blocks, kThreads, 0, st, (int)subset_pixels, num_slices,
+           pix, num_rows, num_cols, flat_image, flat_error, sc, w.delta, w.prior, w.fwd);
     MBIR_CHECK_LAUNCH("denoise direction");
     tpre(st);
-    vcd_alpha_kernel<<<1, kAlphaThreads, 0, st>>>(w.prior, w.blocks, w.fwd, w.blocks, sc.fmc,
-                                                 sc.max_alpha, w.alpha, nullptr);
+    launch(vcd_alpha_kernel, 1, kAlphaThreads, 0, st, w.prior, w.blocks, w.fwd, w.blocks, sc.fmc,
+           sc.max_alpha, w.alpha, nullptr);
     MBIR_CHECK_LAUNCH("denoise alpha");
     tpre(st);
-    denoise_update_kernel<<<w.blocks, kThreads, 0, st>>>((int)subset_pixels, num_slices, pix,
-                                                         w.delta, w.alpha, flat_image,
-                                                         flat_error, w.l1, w.counter, accum);
+    launch(denoise_update_kernel, w.blocks, kThreads, 0, st, (int)subset_pixels, num_slices, pix,
+           w.delta, w.alpha, flat_image, flat_error, w.l1, w.counter, accum);
     MBIR_CHECK_LAUNCH("denoise update");
   }
   return MBIR_OK;

@@ -198,6 +198,23 @@ __device__ __forceinline__ void cone_tcoef(const Geo &g, float mag, float z_off,
   a0 = __fmul_rn(__fmul_rn(mag, __fsub_rn(z_off, __fmul_rn(g.dvs, g.slice_c))), g.inv_sdd);
 }
 
+// Programmatic dependent launch (sm_90 and later).  A kernel launched with
+// programmatic stream serialization may begin while the kernel before it
+// in the stream is still running: pdl_wait() returns once that grid has
+// completed and its writes are visible (at once for a kernel launched the
+// ordinary way), and pdl_release() lets the stream's next kernel begin its
+// launch.  MBIR_PDL_ENTRY() opens every kernel that the library may launch
+// that way, before the kernel touches global memory.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+#define MBIR_PDL_ENTRY() \
+  do {                   \
+    pdl_wait();          \
+    pdl_release();       \
+  } while (0)
+
 // sqrt(1 + t^2) from the fast reciprocal square root (q * rsqrt(q)).
 __device__ __forceinline__ float inv_cos_from_t(float t) {
   const float q = fmaf(t, t, 1.f);

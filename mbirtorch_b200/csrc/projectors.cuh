@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(kThreads)
 back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
                      RD rd, const int64_t *__restrict__ pix, int P, int band, int T,
                      int slice_chunks, float *__restrict__ out) {
+  MBIR_PDL_ENTRY();
   __shared__ ParRec tab[kThreads];
   constexpr int MT = MBIR_TAPS(NT);
   const int RT = NT ? (NT - 1) / 2 : g.psf, nt = 2 * RT + 1;
@@ -238,6 +239,7 @@ back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, 
                  const int64_t *__restrict__ pix, int P, int slice_start, int band,
                  int slice_chunks, float *__restrict__ out,
                  const ConeFwdRec *__restrict__ recs) {
+  MBIR_PDL_ENTRY();
   extern __shared__ float smem[];
   constexpr int MT = MBIR_TAPS(NT);
   const int RT = NT ? (NT - 1) / 2 : g.psf, nt = 2 * RT + 1;
@@ -371,6 +373,7 @@ back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, 
 // out[i] = sum over chunks of part[chunk * n + i], in chunk order.
 __global__ void reduce_chunks_kernel(const float *__restrict__ part, int chunks, size_t n,
                                      float *__restrict__ out) {
+  MBIR_PDL_ENTRY();
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     float s = 0.f;
@@ -422,6 +425,7 @@ __global__ void __launch_bounds__(kThreads)
 forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__restrict__ values,
                int P, int band, int slice_start, const int64_t *__restrict__ pix, FwdShape fs,
                int by_pixel, EPI epi) {
+  MBIR_PDL_ENTRY();
   extern __shared__ float sm[];
   constexpr int MT = MBIR_TAPS(NT);
   const int RT = NT ? (NT - 1) / 2 : g.psf, nt = 2 * RT + 1;
@@ -779,6 +783,7 @@ __global__ void __launch_bounds__(1024)
 forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
                        const float *__restrict__ values, int P, int band, int slice_start,
                        const int64_t *__restrict__ pix, int by_pixel, EPI epi) {
+  MBIR_PDL_ENTRY();
   extern __shared__ float4 sm4[];
   const int nthr = blockDim.x;
   const int cap = fwd_cap(nthr);
@@ -983,6 +988,7 @@ __global__ void __launch_bounds__(256)
 cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
                 const int64_t *__restrict__ pix, int P, int by_pixel,
                 ConeFwdRec *__restrict__ recs, int *__restrict__ list, int *__restrict__ offs) {
+  MBIR_PDL_ENTRY();
   extern __shared__ int bsm[];
   cone_bin_view(g, vp, v_start, blockIdx.x, pix, P, by_pixel, recs, list, offs, bsm);
 }
@@ -997,6 +1003,7 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
                            int slice_start, const ConeFwdRec *__restrict__ recs,
                            const int *__restrict__ list, const int *__restrict__ offs,
                            unsigned char *__restrict__ touched, EPI epi) {
+  MBIR_PDL_ENTRY();
   extern __shared__ float4 sm4[];
   const int nthr = blockDim.x, tid = threadIdx.x;
   const int cap = fwd_cap(nthr);

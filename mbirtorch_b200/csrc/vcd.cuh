@@ -138,6 +138,7 @@ vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int 
                      VcdScalars sc, float *__restrict__ delta, float *__restrict__ gbuf,
                      float *__restrict__ hinv, float *__restrict__ gpbuf,
                      float *__restrict__ hpbuf, double *__restrict__ partials) {
+  MBIR_PDL_ENTRY();
   const size_t n = (size_t)P * S;
   const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
   double pl = 0.0, pq = 0.0;
@@ -185,6 +186,7 @@ vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int 
 // Per-slice sums over pixel chunks: part[chunk][l] = (sum h^-1 g, sum h^-1).
 __global__ void vcd_dc_sums_kernel(int P, int S, int pchunk, const float *__restrict__ gbuf,
                                    const float *__restrict__ hinv, double *__restrict__ part) {
+  MBIR_PDL_ENTRY();
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   const int chunk = blockIdx.y;
   if (l >= S) return;
@@ -208,6 +210,7 @@ vcd_dc_direction_kernel(int P, int S, int nchunks, const double *__restrict__ su
                         const float *__restrict__ hinv, const float *__restrict__ gpbuf,
                         const float *__restrict__ hpbuf, float *__restrict__ delta,
                         double *__restrict__ partials) {
+  MBIR_PDL_ENTRY();
   const size_t n = (size_t)P * S;
   const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
   double pl = 0.0, pq = 0.0;
@@ -387,6 +390,7 @@ __global__ void __launch_bounds__(kAlphaThreads)
 vcd_alpha_kernel(const double *__restrict__ prior, int np, const double *__restrict__ fwd, int nf,
                  float fmc, float max_alpha, float *__restrict__ alpha_out,
                  float *__restrict__ alpha_user) {
+  MBIR_PDL_ENTRY();
   double pl = 0.0, pq = 0.0, fl = 0.0, fq = 0.0;
   const double2 *pr2 = reinterpret_cast<const double2 *>(prior);
   const double2 *fw2 = reinterpret_cast<const double2 *>(fwd);
@@ -419,6 +423,7 @@ vcd_alpha_kernel(const double *__restrict__ prior, int np, const double *__restr
 __global__ void vcd_positivity_kernel(int P, int S, const int64_t *__restrict__ pix,
                                       const float *__restrict__ flat,
                                       const float *__restrict__ alpha, float *__restrict__ delta) {
+  MBIR_PDL_ENTRY();
   const size_t n = (size_t)P * S;
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -506,6 +511,7 @@ vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pi
                         float *__restrict__ flat, double *__restrict__ sq_part,
                         double *__restrict__ l1_part, unsigned int *__restrict__ counter,
                         double *__restrict__ accum) {
+  MBIR_PDL_ENTRY();
   pixel_update_cta(P, S, pchunk, pix, delta, alpha, flat, sq_part, l1_part, counter, accum,
                    blockIdx.x, blockIdx.y, gridDim.x, gridDim.y);
 }
@@ -515,6 +521,7 @@ vcd_pixel_update_kernel(int P, int S, int pchunk, const int64_t *__restrict__ pi
 template <typename T>
 __global__ void vcd_sino_update_kernel(size_t n, const float *__restrict__ alpha,
                                        T *__restrict__ e, const T *__restrict__ ad) {
+  MBIR_PDL_ENTRY();
   const float a = alpha[0];
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -528,6 +535,7 @@ template <>
 __global__ void vcd_sino_update_kernel<float>(size_t n, const float *__restrict__ alpha,
                                               float *__restrict__ e,
                                               const float *__restrict__ ad) {
+  MBIR_PDL_ENTRY();
   const float a = alpha[0];
   const size_t n4 = n / 4;
   float4 *e4 = reinterpret_cast<float4 *>(e);
@@ -617,6 +625,7 @@ vcd_tail_kernel(int nbin, TailBins tb, int P, int S, int pchunk, const int64_t *
                 double *__restrict__ accum, int ux, int uy, int C, int R, int CB,
                 const unsigned char *__restrict__ touched, T *__restrict__ e,
                 const T *__restrict__ ad, int nblk) {
+  MBIR_PDL_ENTRY();
   extern __shared__ int tail_sm[];
   int b = blockIdx.x;
   if (b < nbin) {
@@ -642,6 +651,7 @@ denoise_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, 
                          const float *__restrict__ flat, const float *__restrict__ err,
                          VcdScalars sc, float *__restrict__ delta, double *__restrict__ prior,
                          double *__restrict__ fwd) {
+  MBIR_PDL_ENTRY();
   const size_t n = (size_t)P * S;
   const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
   double pl = 0.0, pq = 0.0, fl = 0.0, fq = 0.0;
@@ -677,6 +687,7 @@ denoise_update_kernel(int P, int S, const int64_t *__restrict__ pix,
                       float *__restrict__ flat, float *__restrict__ err,
                       double *__restrict__ l1_part, unsigned int *__restrict__ counter,
                       double *__restrict__ accum) {
+  MBIR_PDL_ENTRY();
   const size_t n = (size_t)P * S;
   const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
   const float a = alpha[0];
