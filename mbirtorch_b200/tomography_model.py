@@ -482,26 +482,40 @@ class TomographyModel(ParameterHandler):
         seq = vcd_utils.gen_partition_sequence(self.get_params('partition_sequence'),
                                                max_iterations=max_iterations)
         seq = seq[first_iteration:]
+        on_device = self.torch_device.type == 'cuda'
+        if not torch.is_tensor(sinogram):
+            s_np = np.asarray(sinogram)
+            if np.iscomplexobj(s_np):
+                raise TypeError("sinogram must be real-valued; got complex dtype.")
+            if on_device:
+                # The host array goes to the device once; the checks and the
+                # recon then read the device copy.
+                sinogram = self._sino_device(s_np)
+            elif not np.isfinite(s_np).all():
+                raise ValueError("sinogram contains NaN and/or Inf values.")
         if torch.is_tensor(sinogram):
             if sinogram.is_complex():
                 raise TypeError("sinogram must be real-valued; got complex dtype.")
             if not bool(torch.isfinite(sinogram).all()):
                 raise ValueError("sinogram contains NaN and/or Inf values.")
-        else:
-            s_np = np.asarray(sinogram)
-            if np.iscomplexobj(s_np):
-                raise TypeError("sinogram must be real-valued; got complex dtype.")
-            if not np.isfinite(s_np).all():
-                raise ValueError("sinogram contains NaN and/or Inf values.")
         if weights is not None:
-            w_np = weights.detach().cpu().numpy() if torch.is_tensor(weights) \
-                else np.asarray(weights)
-            if not np.isfinite(w_np).all():
-                raise ValueError("weights contains NaN and/or Inf values.")
-            if (w_np < 0).any():
-                raise ValueError("weights contain negative values.")
-            if (w_np == 0).all():
-                raise ValueError("all weights are zero.")
+            if not torch.is_tensor(weights) and on_device and np.ndim(weights) > 0:
+                weights = self._sino_device(np.asarray(weights))
+            if torch.is_tensor(weights):
+                if not bool(torch.isfinite(weights).all()):
+                    raise ValueError("weights contains NaN and/or Inf values.")
+                if bool((weights < 0).any()):
+                    raise ValueError("weights contain negative values.")
+                if bool((weights == 0).all()):
+                    raise ValueError("all weights are zero.")
+            else:
+                w_np = np.asarray(weights)
+                if not np.isfinite(w_np).all():
+                    raise ValueError("weights contains NaN and/or Inf values.")
+                if (w_np < 0).any():
+                    raise ValueError("weights contain negative values.")
+                if (w_np == 0).all():
+                    raise ValueError("all weights are zero.")
         reg = self.auto_set_regularization_params(sinogram, weights=weights)
         return sinogram, weights, init_recon, partitions, seq, granularity, reg
 
