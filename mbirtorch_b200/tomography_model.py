@@ -190,7 +190,17 @@ class TomographyModel(ParameterHandler):
 
     @staticmethod
     def _out(t, output_sharded):
-        return t if output_sharded else t.detach().cpu().numpy()
+        if output_sharded:
+            return t
+        t = t.detach()
+        if not t.is_cuda:
+            return t.numpy()
+        # Through a pinned staging buffer (reused by torch's host caching
+        # allocator): one DMA at link speed and one host copy, where a
+        # pageable copy stages through the driver at a fraction of the rate.
+        host = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        host.copy_(t)
+        return host.numpy().copy()
 
     # ── projections ─────────────────────────────────────────────────────────
     def sparse_forward_project(self, voxel_values, pixel_indices):
