@@ -46,6 +46,32 @@ def _default_device():
     return torch.device('cpu')
 
 
+class _DeferredPartitions:
+    """The pixel partitions of a recon, one per granularity, drawn from
+    numpy's global generator (gen_pixel_partition, in granularity order) at
+    the first access rather than at construction."""
+
+    def __init__(self, recon_shape, granularity, use_ror_mask):
+        self._args = (tuple(recon_shape), list(granularity), use_ror_mask)
+        self._parts = None
+
+    def _get(self):
+        if self._parts is None:
+            shape, gran, ror = self._args
+            self._parts = [vcd_utils.gen_pixel_partition(shape, n, use_ror_mask=ror)
+                           for n in gran]
+        return self._parts
+
+    def __len__(self):
+        return len(self._args[1])
+
+    def __getitem__(self, k):
+        return self._get()[k]
+
+    def __iter__(self):
+        return iter(self._get())
+
+
 class TomographyModel(ParameterHandler):
     """Base class of the geometry models (see ParallelBeamModel,
     ConeBeamModel)."""
@@ -478,17 +504,26 @@ class TomographyModel(ParameterHandler):
     # ── reconstruction ──────────────────────────────────────────────────────
     def initialize_recon(self, sinogram, weights=None, init_recon=None, max_iterations=15,
                          first_iteration=0, logfile_path='~/.mbirtorch/logs/recon.log',
-                         print_logs=True):
+                         print_logs=True, _defer_partitions=False):
         """Partitions (np.random, reference order), partition sequence, input
-        checks and auto-regularization (tomography_model.py:3015-3095)."""
+        checks and auto-regularization (tomography_model.py:3015-3095).
+        ``_defer_partitions`` (internal): return the partitions as a
+        _DeferredPartitions list, drawn from the global generator at first
+        use; recon() uses it so that the host draws them while the device
+        runs the initial reconstruction and the Hessian.  Nothing between
+        the two points draws random numbers, so the partitions are the
+        same."""
         if first_iteration == 0 or self.log_buffer is None:
             self.setup_logger(logfile_path=logfile_path, print_logs=print_logs)
         from . import __version__
         self.logger.info(f'MBIRTorch-B200 Version = {__version__}')
         recon_shape, granularity, use_ror_mask = self.get_params(
             ['recon_shape', 'granularity', 'use_ror_mask'])
-        partitions = [vcd_utils.gen_pixel_partition(recon_shape, n, use_ror_mask=use_ror_mask)
-                      for n in granularity]
+        if _defer_partitions:
+            partitions = _DeferredPartitions(recon_shape, granularity, use_ror_mask)
+        else:
+            partitions = [vcd_utils.gen_pixel_partition(recon_shape, n, use_ror_mask=use_ror_mask)
+                          for n in granularity]
         seq = vcd_utils.gen_partition_sequence(self.get_params('partition_sequence'),
                                                max_iterations=max_iterations)
         seq = seq[first_iteration:]
@@ -538,7 +573,7 @@ class TomographyModel(ParameterHandler):
         (sinogram, weights, init_recon, partitions, seq, granularity,
          reg) = self.initialize_recon(sinogram, weights, init_recon, max_iterations,
                                       first_iteration, logfile_path=logfile_path,
-                                      print_logs=print_logs)
+                                      print_logs=print_logs, _defer_partitions=True)
         with torch.no_grad():
             recon, losses = self._vcd_recon(sinogram, partitions, seq, stop_threshold_change_pct,
                                             weights=weights, init_recon=init_recon,
