@@ -383,14 +383,22 @@ def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd):
     bytes_per_launch = {
         "vcd gradient (back projection)": frac * sino * b_e,
         "vcd forward + line search": 2 * frac * sino * b_e,
-        "vcd sinogram update": 3 * sino * b_e,
+        # the tail's tile role: read e and A delta, write e, over the reached tiles
+        "vcd pixel + sinogram update": 3 * frac * sino * b_e,
     }
+    # DRAM bytes of one forward + line-search launch at this workload (FP32
+    # storage), measured by ncu on one launch of the 399-pixel subset step:
+    # 103.9 MB read + 58.3 MB written.
+    traffic = {("vcd forward + line search", "float32"): (103.9e6 + 58.3e6)}
     tms, tcnt = kt[top]
     alg = bytes_per_launch.get(top)
     if alg is not None:
         ach = alg / (tms / tcnt / 1e3) / 1e9
         res["roofline"] = {"kernel": top, "bound": "hbm", "achieved": ach, "peak": hbm,
-                           "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                           "unit": "GB/s", "frac": ach / hbm,
+                           "traffic": traffic.get((top, args.storage)),
+                           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                             "one launch of the subset-step capture",
                            "algorithmic_bytes_per_launch": alg,
                            "avg_launch_ms": tms / tcnt, "launches": tcnt,
                            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}

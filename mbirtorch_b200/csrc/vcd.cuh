@@ -555,7 +555,10 @@ __global__ void vcd_sino_update_kernel<float>(size_t n, const float *__restrict_
     e[i] = __fsub_rn(e[i], __fmul_rn(a, ad[i]));
 }
 
-// One tile (channel block b, view v) of the touched-tile sinogram update.
+// One tile (channel block b, view v) of the touched-tile sinogram update:
+// e -= alpha * Ad over CB consecutive channels of one view (one contiguous
+// run of CB * R cells), skipped when the binned forward marked the tile as
+// not reached.
 template <typename T>
 __device__ __forceinline__ void sino_tile_cta(int C, int R, int CB,
                                               const unsigned char *__restrict__ touched,
@@ -583,17 +586,6 @@ __device__ __forceinline__ void sino_tile_cta(int C, int R, int CB,
       if (i < n) et[i] = from_f32<T>(__fsub_rn(ev[u], __fmul_rn(a, dv[u])));
     }
   }
-}
-
-// The same update over the (view, channel-block) tiles a binned forward
-// marked as reached (grid: blocks x views).  A tile is CB consecutive
-// channels of one view, i.e. one contiguous run of CB * R cells.
-template <typename T>
-__global__ void __launch_bounds__(256)
-vcd_sino_update_tiles_kernel(int C, int R, int CB, const unsigned char *__restrict__ touched,
-                             const float *__restrict__ alpha, T *__restrict__ e,
-                             const T *__restrict__ ad) {
-  sino_tile_cta(C, R, CB, touched, alpha, e, ad, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 // The bins of the next subset of a partition pass (cone_bin_kernel's
