@@ -221,6 +221,17 @@ __device__ __forceinline__ float inv_cos_from_t(float t) {
   return q * rsqrtf(q);
 }
 
+// The same value through the flush-to-zero form of the hardware reciprocal
+// square root: q >= 1 is never subnormal, so the result equals
+// inv_cos_from_t without rsqrtf's subnormal-input handling.  Used where it
+// measured faster (the forward's cylinder staging).
+__device__ __forceinline__ float inv_cos_from_t_ftz(float t) {
+  const float q = fmaf(t, t, 1.f);
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(q));
+  return q * r;
+}
+
 // 1 / cos(phi) for the voxel at global slice k of a cone (view, pixel):
 // sqrt(1 + (v / SDD)^2) with v = mag * z_k, the same quantity as the
 // reference's 1 / cos(atan2(v, SDD)) (exactly 1 at SDD = inf).

@@ -747,7 +747,7 @@ __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec,
         for (int e = 0; e < kFwdEB; ++e) {
           if (e >= nb) break;
           const float4 c = rec[b0 + e].c;
-          sk[e * SP] = val[e] * inv_cos_from_t(fmaf(c.y, kf, c.x));
+          sk[e * SP] = val[e] * inv_cos_from_t_ftz(fmaf(c.y, kf, c.x));
         }
       }
     } else {
@@ -756,7 +756,7 @@ __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec,
         const float4 c = rec[b0 + e].c;
         stage[e * SP + kFwdVPad + k] =
             __ldg(values + (size_t)__float_as_int(c.w) * band + k) *
-            inv_cos_from_t(fmaf(c.y, (float)(slice_start + k), c.x));
+            inv_cos_from_t_ftz(fmaf(c.y, (float)(slice_start + k), c.x));
       }
     }
     __syncthreads();
