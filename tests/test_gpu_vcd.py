@@ -289,3 +289,87 @@ def test_prox_map_matches_reference_and_oracle(name):
     with pytest.raises(ValueError, match='prox_input'):
         m.prox_map(d['prox_input'][:, :, :2], d['sino'], max_iterations=1, logfile_path=None,
                    print_logs=False)
+
+
+def test_cone_partition_pass_truncated_detector_ragged_channels():
+    """A partition pass (each step bins the next subset in its tail) on a
+    cone geometry whose detector (37 channels: a ragged last channel block)
+    sees only the middle of the object: pixels centred off the detector,
+    and on its edge channels -1 and C, against the FP64 oracle applying the
+    same subsets in the same order."""
+    from oracle import vcd as ovcd
+    from mbirtorch_b200.vcd_engine import ResidentSinogram
+    from mbirtorch_b200 import _lib
+    V, R, C = 24, 8, 37
+    m = mb.ConeBeamModel((V, R, C), np.linspace(0, 2 * np.pi, V, endpoint=False), 512.0, 256.0)
+    m.set_params(no_warning=True, verbose=0, delta_det_channel=2.0, delta_det_row=2.0)
+    m.auto_set_recon_geometry(no_warning=True)
+    m.set_params(no_warning=True, recon_shape=(48, 48, 4))
+    rs = m.get_params('recon_shape')
+    rng = np.random.default_rng(17)
+    x_true = rng.random(rs).astype(np.float32)
+    sino = m.forward_project(x_true)
+    m.auto_set_regularization_params(sino)
+    x0 = (0.05 * rng.standard_normal(rs)).astype(np.float32)
+    e0 = sino - m.forward_project(x0)
+    H = m.compute_hessian_diagonal()
+    upd = m.create_vcd_subset_updater(H, weights=1)
+    np.random.seed(4)
+    part = mb.gen_pixel_partition(rs, 8)
+    order = np.random.permutation(8).astype(np.int32)
+    flat = torch.as_tensor(x0.reshape(-1, rs[2]), device='cuda').clone()
+    err = ResidentSinogram.from_vrc(torch.as_tensor(e0, device='cuda'), _lib.MBIR_F32)
+    acc = torch.zeros(2 + rs[2], dtype=torch.float64, device='cuda')
+    upd.engine.partition_pass(flat, err, torch.as_tensor(part, device='cuda'), order, acc)
+    prob = _oracle_problem(m)
+    sy, sx = m.get_params(['sigma_y', 'sigma_x'])
+    ou = ovcd.SubsetUpdater(prob, H.reshape(-1, rs[2]), None, sy, sx,
+                            dc_profile=ovcd.dc_damping_profile(prob))
+    oflat = x0.reshape(-1, rs[2]).astype(np.float64)
+    oerr = e0.astype(np.float64)
+    alpha_sum = 0.0
+    for k in order:
+        _, oalpha, _ = ou(oflat, oerr, part[k].astype(np.int64))
+        alpha_sum += oalpha
+    assert abs(float(acc[1]) - alpha_sum) / alpha_sum <= 1e-4
+    assert rel_l2(flat.cpu().numpy(), oflat) <= 2e-5
+    assert rel_l2(err.to_vrc().cpu().numpy(), oerr) <= 2e-5
+
+
+def test_cone_subset_step_wide_detector_scanning_forward():
+    """6000 channels: too many centre-channel keys for the binning's shared
+    memory, so the subset step takes the scanning forward and the separate
+    update kernels.  One step against the FP64 oracle.  Channel coordinates
+    near 3000 resolve to 2.4e-4 of a channel in FP32, so the tap weights
+    carry ~1e-4 relative error at this width (the same object on a
+    384-channel detector agrees to 1.5e-6 / 4.9e-6); the bounds follow that
+    resolution."""
+    from oracle import vcd as ovcd
+    V, R, C = 4, 4, 6000
+    m = mb.ConeBeamModel((V, R, C), np.linspace(0, np.pi, V, endpoint=False), 2048.0, 1024.0)
+    m.set_params(no_warning=True, verbose=0, delta_det_channel=0.02, delta_det_row=0.02)
+    m.auto_set_recon_geometry(no_warning=True)
+    m.set_params(no_warning=True, recon_shape=(32, 32, 2))
+    rs = m.get_params('recon_shape')
+    rng = np.random.default_rng(23)
+    x_true = rng.random(rs).astype(np.float32)
+    sino = m.forward_project(x_true)
+    m.auto_set_regularization_params(sino)
+    x0 = (0.05 * rng.standard_normal(rs)).astype(np.float32)
+    e0 = sino - m.forward_project(x0)
+    H = m.compute_hessian_diagonal()
+    upd = m.create_vcd_subset_updater(H, weights=1)
+    idx = np.sort(rng.choice(mb.gen_full_indices(rs), size=100, replace=False)).astype(np.int64)
+    flat = torch.as_tensor(x0.reshape(-1, rs[2]), device='cuda').clone()
+    err = torch.as_tensor(e0, device='cuda').clone()
+    flat, err, ell1, alpha, sumsq = upd(flat, err, torch.as_tensor(idx, device='cuda'))
+    prob = _oracle_problem(m)
+    sy, sx = m.get_params(['sigma_y', 'sigma_x'])
+    ou = ovcd.SubsetUpdater(prob, H.reshape(-1, rs[2]), None, sy, sx,
+                            dc_profile=ovcd.dc_damping_profile(prob))
+    oflat = x0.reshape(-1, rs[2]).astype(np.float64)
+    oerr = e0.astype(np.float64)
+    _, oalpha, _ = ou(oflat, oerr, idx)
+    assert abs(float(alpha) - oalpha) / oalpha <= 1e-4
+    assert rel_l2(flat.cpu().numpy(), oflat) <= 1e-4
+    assert rel_l2(err.cpu().numpy(), oerr) <= 2e-4
