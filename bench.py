@@ -538,7 +538,8 @@ def serving_mix_extra(mb, torch, n_jobs=16):
     form (each job alone, FP32, one after another through model.recon) vs
     the served form (all jobs submitted at once to a ReconServer with
     float16 storage: resident, admitted against the memory ledger, advancing
-    concurrently).  Both with 10 VCD iterations and the same per-job seeds,
+    concurrently, recurring partition passes replayed as CUDA graphs; the
+    served form with direct launches is timed beside it).  Both with 10 VCD iterations and the same per-job seeds,
     so each served result is compared with its own plain result."""
     from mbirtorch_b200.serving import ReconServer
     jobs = mix_jobs(mb, torch, n_jobs)
@@ -555,8 +556,8 @@ def serving_mix_extra(mb, torch, n_jobs=16):
             out.append(r)
         return out, time.perf_counter() - t0
 
-    def served():
-        srv = ReconServer(storage_dtype="float16", max_active=8)
+    def served(graphs=True):
+        srv = ReconServer(storage_dtype="float16", max_active=8, cuda_graphs=graphs)
         t0 = time.perf_counter()
         reqs = [srv.submit(make(), sino, max_iterations=iters, seed=seed, arrival=t0)
                 for make, sino, seed in jobs]
@@ -566,7 +567,9 @@ def serving_mix_extra(mb, torch, n_jobs=16):
     plain()        # warm-up (library load, allocator)
     served()
     ref, t_plain = plain()
+    reqs_ng, t_srv_ng, _ = served(graphs=False)
     reqs, t_srv, st = served()
+    same = all(np.array_equal(a.recon, b.recon) for a, b in zip(reqs, reqs_ng))
     rel = [float(np.linalg.norm(r.recon.astype(np.float64) - p) / np.linalg.norm(p))
            for r, p in zip(reqs, ref)]
     kinds = {}
@@ -577,6 +580,9 @@ def serving_mix_extra(mb, torch, n_jobs=16):
             "plain_f32_recons_per_s": n_jobs / t_plain,
             "served_f16_recons_per_s": n_jobs / t_srv,
             "served_over_plain": t_plain / t_srv,
+            "served_f16_direct_launch_recons_per_s": n_jobs / t_srv_ng,
+            "graph_replays": int(sum(r.graph_replays for r in reqs)),
+            "graphs_bitwise_equal_direct": bool(same),
             "served_p50_latency_s": st["p50_latency_s"],
             "served_p99_latency_s": st["p99_latency_s"],
             "max_concurrent": st["max_concurrent"], "failed": st["failed"],

@@ -158,8 +158,19 @@ def launch_count():
     return int(load().mbir_launch_count())
 
 
+_timing_on = False
+
+
 def timing_enable(on=True):
-    return bool(load().mbir_timing_enable(int(bool(on))))
+    """Turn the library's per-launch CUDA-event timing on or off; returns
+    the previous setting."""
+    global _timing_on
+    _timing_on = bool(on)
+    return bool(load().mbir_timing_enable(int(_timing_on)))
+
+
+def timing_enabled():
+    return _timing_on
 
 
 def timing_collect(max_entries=64):

@@ -92,6 +92,7 @@ class Request:
         self._out_event = None
         self._state = None       # a preempted run's state, to resume from
         self.preempted = False   # taken off the device by ReconServer.preempt
+        self.graph_replays = 0   # partition passes replayed from a captured graph
 
     def done(self):
         return self.finished is not None
@@ -115,10 +116,14 @@ class ReconServer:
         max_active: most jobs resident at once.
         storage_dtype: resident precision of the error sinogram, weights and
             delta sinogram ('float16' by default; see TomographyModel).
+        cuda_graphs: replay each job's recurring partition passes as captured
+            CUDA graphs (default True; see :class:`VcdRun`).  Results are
+            bitwise the same either way; the graphs take the per-kernel
+            launch work off the scheduler thread.
     """
 
     def __init__(self, device=None, memory_budget_bytes=None, max_active=8,
-                 storage_dtype='float16'):
+                 storage_dtype='float16', cuda_graphs=True):
         self.device = torch.device('cuda', torch.cuda.current_device()) if device is None \
             else torch.device(device)
         if memory_budget_bytes is None:
@@ -127,6 +132,7 @@ class ReconServer:
         self.ledger = MemoryLedger(memory_budget_bytes)
         self.max_active = int(max_active)
         self.storage_dtype = storage_dtype
+        self.cuda_graphs = bool(cuda_graphs)
         storage_code(storage_dtype)
         self.waiting = []
         self.active = []
@@ -185,7 +191,8 @@ class ReconServer:
                               f'{self.ledger.budget}')
         r._stream = self._streams.pop() if self._streams else torch.cuda.Stream(self.device)
         with torch.cuda.device(self.device):
-            r._run = VcdRun.from_state(m, state, stream=r._stream)
+            r._run = VcdRun.from_state(m, state, stream=r._stream,
+                                       cuda_graphs=self.cuda_graphs)
         r._state = None
         self.ledger.take(resident)
         r._charge = resident
@@ -218,7 +225,7 @@ class ReconServer:
         m.auto_set_regularization_params(r.sinogram, weights=r.weights)
         r._stream = self._streams.pop() if self._streams else torch.cuda.Stream(self.device)
         r._run = VcdRun(m, r.sinogram, parts, seq, r.stop_pct, weights=r.weights, rng=rng,
-                        stream=r._stream)
+                        stream=r._stream, cuda_graphs=self.cuda_graphs)
         self.ledger.take(peak)
         r._charge = peak
         r.admitted = time.perf_counter()
@@ -232,6 +239,7 @@ class ReconServer:
 
     def _finish(self, r):
         run = r._run
+        r.graph_replays += run.graph_replays
         with torch.cuda.stream(r._stream):
             r._out = torch.empty(run.flat.shape, dtype=torch.float32, pin_memory=True)
             r._out.copy_(run.flat, non_blocking=True)

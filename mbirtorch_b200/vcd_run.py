@@ -19,6 +19,18 @@ This is the body of the reference's ``_vcd_recon`` (tomography_model.py:
 
 Every run owns its stream, its RNG and its buffers, and the kernels are
 deterministic, so a run's result does not depend on what else is running.
+
+With ``cuda_graphs=True`` (the server's default) a partition pass whose
+shape -- (subsets, pixels per subset) -- recurs later in the run is
+captured once as a CUDA graph and replayed.  The graph walks the subsets of
+a run-owned "ordered partition" buffer in row order; before each replay one
+small gather writes the iteration's subsets into that buffer in the drawn
+order (``ordered[k] = partition[order[k]]``).  The graph therefore depends
+only on the shape, not on the partition or the order, and the kernels see
+exactly the pixel lists the direct launch path gives them: the results are
+bitwise the same.  A 128-subset pass is ~640 kernel launches; replaying it
+costs the host one graph launch, which is what lets many small jobs keep
+the device busy from one scheduler thread.
 """
 
 import math
@@ -36,7 +48,7 @@ class VcdRun:
     def __init__(self, model, sinogram, partitions, partition_sequence,
                  stop_threshold_change_pct, weights=None, init_recon=None,
                  init_error_sinogram=None, fm_hessian=None, rng=None, first_iteration=0,
-                 stream=None, prox_input=None):
+                 stream=None, prox_input=None, cuda_graphs=False):
         model.verify_valid_params()
         model._require_cuda()
         self.model = model
@@ -72,6 +84,10 @@ class VcdRun:
         self.finished = n == 0
         self._event = None
         self._pending = None
+        self.cuda_graphs = bool(cuda_graphs)
+        self._graphs = {}
+        self._graph_shapes = set()
+        self.graph_replays = 0
 
     # ── device preparation ───────────────────────────────────────────────
     def prepare(self):
@@ -144,7 +160,64 @@ class VcdRun:
                                      prox_flat=self.prox_flat)
         self.host = torch.empty(2 + self.recon_shape[2] + 4, dtype=torch.float64,
                                 pin_memory=True)
+        self._graph_setup()
         log.info('Starting VCD iterations')
+
+    def _graph_setup(self):
+        """Pick the pass shapes worth a graph -- those used at least twice
+        in the iterations still to run -- and allocate the buffers their
+        replays gather into.  Graphs need a stream of the run's own: the
+        legacy default stream cannot be captured."""
+        self._graph_shapes = set()
+        if not self.cuda_graphs or self.stream == torch.cuda.default_stream(
+                self.model.torch_device):
+            return
+        uses = {}
+        for i in self.seq[self.done:]:
+            shape = tuple(self.parts_dev[int(i)].shape)
+            uses[shape] = uses.get(shape, 0) + 1
+        self._graph_shapes = {s for s, u in uses.items() if u >= 2}
+        if not self._graph_shapes:
+            return
+        dev = self.model.torch_device
+        k_max = max(s[0] for s in self._graph_shapes)
+        self._ordered = torch.empty(max(s[0] * s[1] for s in self._graph_shapes),
+                                    dtype=torch.int64, device=dev)
+        self._order_dev = torch.empty(k_max, dtype=torch.int64, device=dev)
+        self._order_host = torch.empty(k_max, dtype=torch.int64, pin_memory=True)
+
+    def _graph_pass(self, part, order):
+        """One partition pass by graph replay (captured on first use of its
+        shape).  Called on the run's stream."""
+        K, n = part.shape
+        oh = self._order_host[:K]
+        oh.numpy()[:] = order   # the previous copy from it ended before collect()
+        od = self._order_dev[:K]
+        od.copy_(oh, non_blocking=True)
+        ordered = self._ordered[:K * n].view(K, n)
+        torch.index_select(part, 0, od, out=ordered)
+        g = self._graphs.get((K, n))
+        if g is None:
+            self.engine.reserve(n)
+            g = torch.cuda.CUDAGraph()
+            g.capture_begin(capture_error_mode='thread_local')
+            try:
+                self.engine.partition_pass(self.flat, self.err, ordered,
+                                           np.arange(K, dtype=np.int32))
+            except BaseException:
+                try:
+                    g.capture_end()
+                except Exception:
+                    pass
+                raise
+            g.capture_end()
+            self._graphs[(K, n)] = g
+        g.replay()
+        self.graph_replays += 1
+
+    def release_graphs(self):
+        """Drop the captured graphs (their device resources go with them)."""
+        self._graphs.clear()
 
     # ── iterations ───────────────────────────────────────────────────────
     def enqueue_iteration(self):
@@ -156,7 +229,10 @@ class VcdRun:
             part = self.parts_dev[int(self.seq[i])]
             order = order_array(part.shape[0], self.rng)
             self.engine.accum.zero_()
-            self.engine.partition_pass(self.flat, self.err, part, order)
+            if tuple(part.shape) in self._graph_shapes and not _lib.timing_enabled():
+                self._graph_pass(part, order)
+            else:
+                self.engine.partition_pass(self.flat, self.err, part, order)
             if self.y_vcr is not None and (i + 1) % self.refresh == 0:
                 self.engine.refresh_error(self.flat, self.err, self.model.full_indices_device(),
                                           self.y_vcr)
@@ -283,7 +359,7 @@ class VcdRun:
         np.savez(path, **self.state_dict())
 
     @classmethod
-    def from_state(cls, model, state, stream=None):
+    def from_state(cls, model, state, stream=None, cuda_graphs=False):
         """A prepared run that continues from ``state`` (a dict from
         :meth:`state_dict` or the path of a :meth:`save_state` file) on
         ``model`` (the same geometry and regularization)."""
@@ -325,6 +401,9 @@ class VcdRun:
         run.finished = bool(state['finished'])
         run._event = None
         run._pending = None
+        run.cuda_graphs = bool(cuda_graphs)
+        run._graphs = {}
+        run.graph_replays = 0
         run.refresh = int(state['refresh'])
         run.constant_weights = bool(state['constant_weights'])
         dev = model.torch_device
@@ -355,6 +434,7 @@ class VcdRun:
                                             prox_flat=run.prox_flat)
             run.host = torch.empty(2 + run.recon_shape[2] + 4, dtype=torch.float64,
                                    pin_memory=True)
+            run._graph_setup()
         return run
 
     def device_bytes(self):
@@ -365,4 +445,6 @@ class VcdRun:
             n += self.w_res.nbytes()
         if self.y_vcr is not None:
             n += self.y_vcr.numel() * 4
+        if self._graph_shapes:
+            n += (self._ordered.numel() + self._order_dev.numel()) * 8
         return n

@@ -61,14 +61,15 @@ def _jobs():
     return out
 
 
-def _serve(jobs, idxs, storage, max_active=8, budget=None):
-    srv = ReconServer(storage_dtype=storage, max_active=max_active, memory_budget_bytes=budget)
+def _serve(jobs, idxs, storage, max_active=8, budget=None, iterations=3, cuda_graphs=True):
+    srv = ReconServer(storage_dtype=storage, max_active=max_active, memory_budget_bytes=budget,
+                      cuda_graphs=cuda_graphs)
     reqs = []
     for i in idxs:
         make, sino = jobs[i]
         m = make()
         m.set_params(no_warning=True, verbose=0)
-        reqs.append(srv.submit(m, sino, max_iterations=3, seed=1000 + i))
+        reqs.append(srv.submit(m, sino, max_iterations=iterations, seed=1000 + i))
     srv.run_until_idle(timeout_s=300)
     return srv, reqs
 
@@ -82,6 +83,23 @@ def test_results_same_alone_and_in_mix(storage):
         assert alone[0].error is None and mix[i].error is None
         assert np.array_equal(alone[0].recon, mix[i].recon), i
         assert alone[0].recon_params['fm_rmse'] == mix[i].recon_params['fm_rmse']
+
+
+@pytest.mark.parametrize("storage", ["float32", "float16"])
+def test_graph_replay_equals_direct_launch(storage):
+    """Seven iterations use the 128-subset partitions four times: the server
+    captures that pass shape once per job and replays it.  Every served
+    result equals the one served with direct launches, bit for bit."""
+    jobs = _jobs()
+    _, direct = _serve(jobs, range(len(jobs)), storage, max_active=5, iterations=7,
+                       cuda_graphs=False)
+    _, graphed = _serve(jobs, range(len(jobs)), storage, max_active=5, iterations=7)
+    for d, g in zip(direct, graphed):
+        assert d.error is None and g.error is None
+        assert d.graph_replays == 0 and g.graph_replays == 4
+        assert np.array_equal(d.recon, g.recon)
+        assert d.recon_params['fm_rmse'] == g.recon_params['fm_rmse']
+        assert d.recon_params['alpha_values'] == g.recon_params['alpha_values']
 
 
 def test_server_equals_model_recon_with_same_seed():
