@@ -380,6 +380,15 @@ bool use_cone_binned(const mbir_geometry *g) {
   return use_cone_rt(g) && bin_smem(g) <= (size_t)200 * 1024;
 }
 
+// Parallel beam at psf radius 1 with up to 1024 detector rows (one thread
+// per row) projects a VCD subset through the same bins.
+bool use_par_binned(const mbir_geometry *g) {
+  return g->geometry != MBIR_CONE && g->psf_radius == 1 && g->num_det_rows <= 1024 &&
+         bin_smem(g) <= (size_t)200 * 1024;
+}
+
+bool use_binned(const mbir_geometry *g) { return use_cone_binned(g) || use_par_binned(g); }
+
 int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count,
                const int64_t *pix, long long P, const FwdBins &b, cudaStream_t st) {
   const Geo geo = make_geo(*g);
@@ -419,6 +428,31 @@ int launch_binned(const mbir_geometry *g, int v_start, int v_count, const float 
   return MBIR_OK;
 }
 
+template <typename EPI>
+int launch_par_binned(const mbir_geometry *g, int v_start, int v_count, const float *values,
+                      long long P, int band, const FwdBins &b, const EPI &epi, cudaStream_t st,
+                      const char *what) {
+  if (band != g->num_det_rows)
+    return fail(MBIR_ERR_INVALID, "%s: the binned parallel forward projects whole cylinders "
+                "(band %d, detector rows %d)", what, band, g->num_det_rows);
+  const Geo geo = make_geo(*g);
+  const int nthr = cone_rt_threads(g);
+  const size_t smem = par_binned_smem(nthr);
+  auto k = forward_parallel_binned_kernel<EPI>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+      return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s", smem,
+                  cudaGetErrorString(e));
+  }
+  dim3 grid(fwd_nblk(g), v_count);
+  tpre(st);
+  launch(k, grid, nthr, smem, st, geo, v_start, values, (int)P, band, (const ConeFwdRec *)b.recs,
+         (const int *)b.list, (const int *)b.offs, b.touched, epi);
+  MBIR_CHECK_LAUNCH(what);
+  return MBIR_OK;
+}
+
 // Forward of a (P, band) subset array over all views through the bins: per
 // view chunk, bin (when `bin`) and project.  With a single chunk the bins
 // outlive the call, so a later projection of the same subset passes
@@ -435,7 +469,8 @@ int run_forward_binned(const mbir_geometry *g, const float *vp, const float *val
       rc = launch_bin(g, vp, v0, nv, pix, P, b, st);
       if (rc) return rc;
     }
-    rc = launch_binned(g, v0, nv, values, P, band, b, epi, st, what);
+    rc = g->geometry == MBIR_CONE ? launch_binned(g, v0, nv, values, P, band, b, epi, st, what)
+                                  : launch_par_binned(g, v0, nv, values, P, band, b, epi, st, what);
     if (rc) return rc;
   }
   return MBIR_OK;
@@ -459,7 +494,8 @@ int run_forward(const mbir_geometry *g, const float *vp, int v_start, int v_coun
 }
 
 int fwd_blocks(const mbir_geometry *g, int band, int v_count) {
-  if (use_cone_rt(g)) return ((g->num_det_channels + kFwdCB - 1) / kFwdCB) * v_count;
+  if (use_cone_rt(g) || use_par_binned(g))
+    return ((g->num_det_channels + kFwdCB - 1) / kFwdCB) * v_count;
   const FwdShape fs = fwd_shape(g, band);
   return ((g->num_det_channels + fs.CB - 1) / fs.CB) * v_count;
 }
@@ -507,7 +543,7 @@ VcdWs vcd_layout(const mbir_geometry *g, long long Ps, const mbir_vcd_params *pr
   w.alpha = c.take<float>(4);
   w.counters = c.take<unsigned int>(2);
   w.ad = c.take<char>((size_t)V * g->num_det_channels * g->num_det_rows * storage_size(prm->storage));
-  w.binned = use_cone_binned(g);
+  w.binned = use_binned(g);
   w.bins = FwdBins{nullptr, nullptr, nullptr, nullptr, 0};
   if (w.binned) {
     const int vc = bin_views(g, Ps);
@@ -541,7 +577,8 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
     rc = launch_bin(g, vp, 0, V, pix, Ps, w.bins, st);
     if (rc) return rc;
   }
-  const ConeFwdRec *recs = shared_bins ? w.bins.recs : nullptr;
+  // (the cone gradient reads them; the parallel one forms its taps itself)
+  const ConeFwdRec *recs = shared_bins && g->geometry == MBIR_CONE ? w.bins.recs : nullptr;
   // 1. gradient partials of A^T (w e), one slab per view chunk
   if (wts) {
     ReadWeighted<T> rd{err, es, wts, wsc, C, R};

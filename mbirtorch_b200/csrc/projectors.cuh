@@ -920,8 +920,24 @@ __device__ __forceinline__ int block_exclusive_scan(int *a, int n, int *warp_tot
   return total;
 }
 
+// The parallel-beam record of a (view, pixel): the three channel taps of
+// centre ctr (parallel_beam.py:22-53, horizontal_fan.py:51-71) in b.y .. b.w,
+// ctr in c.z and the cylinder's row in c.w, the fields the cone record
+// keeps in the same places; the vertical-fan fields are unused.
+__device__ __forceinline__ ConeFwdRec par_fwd_record(const Geo &g, const ParView &pv, float n_p,
+                                                     int ctr, int row) {
+  ConeFwdRec r;
+  r.a = make_float4(0.f, 0.f, 0.f, 0.f);
+  r.b = make_float4(0.f, tap_weight(n_p, ctr - 1, pv.half_w1, pv.lmax, pv.ws, g.C),
+                    tap_weight(n_p, ctr, pv.half_w1, pv.lmax, pv.ws, g.C),
+                    tap_weight(n_p, ctr + 1, pv.half_w1, pv.lmax, pv.ws, g.C));
+  r.c = make_float4(0.f, 0.f, __int_as_float(ctr), __int_as_float(row));
+  return r;
+}
+
 // One CTA's work of cone_bin_kernel: view vl of the chunk, with bsm the
-// (1 + warps) x (C + 2) ints of dynamic shared memory.
+// (1 + warps) x (C + 2) ints of dynamic shared memory.  Parallel-beam
+// geometries (g.cone = 0) are binned the same way, with par_fwd_record.
 __device__ __forceinline__ void cone_bin_view(const Geo &g, const float *__restrict__ vp,
                                               int v_start, int vl,
                                               const int64_t *__restrict__ pix, int P,
@@ -938,6 +954,8 @@ __device__ __forceinline__ void cone_bin_view(const Geo &g, const float *__restr
   const float ang = vp[2 * v];
   const float cs = cosf(ang), sn = sinf(ang);
   const float z_off = __fsub_rn(g.rso, vp[2 * v + 1]);
+  ParView pv;
+  if (!g.cone) pv = parallel_view(g, ang);
   ConeFwdRec *vrec = recs + (size_t)vl * P;
   int *vlist = list + (size_t)vl * P;
   int *voffs = offs + (size_t)vl * (nkeys + 1);
@@ -949,9 +967,18 @@ __device__ __forceinline__ void cone_bin_view(const Geo &g, const float *__restr
   for (int p = tid; p < P; p += nthr) {
     float xt, yt;
     pixel_xy(g, (int)pix[p], xt, yt);
-    const ConeCenter cc = cone_center(g, cs, sn, xt, yt);
-    vrec[p] = cone_fwd_record(g, ang, z_off, cc, by_pixel ? (int)pix[p] : p);
-    const int key = fwd_key(cc.ctr, g.C);
+    const int row = by_pixel ? (int)pix[p] : p;
+    int ctr;
+    if (g.cone) {
+      const ConeCenter cc = cone_center(g, cs, sn, xt, yt);
+      vrec[p] = cone_fwd_record(g, ang, z_off, cc, row);
+      ctr = cc.ctr;
+    } else {
+      const float n_p = parallel_np(g, pv, xt, yt);
+      ctr = (int)fminf(fmaxf(rintf(n_p), -1.0e6f), 1.0e6f);
+      vrec[p] = par_fwd_record(g, pv, n_p, ctr, row);
+    }
+    const int key = fwd_key(ctr, g.C);
     if (key >= 0) atomicAdd(&cursor[key], 1);
   }
   __syncthreads();
@@ -1064,6 +1091,122 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
   for (int j = 0; j < kFwdCB; ++j) acc[j] = acc_s[(j + 2) * nthr + tid];
   epi.begin(v);
   if (tid < g.R) epi.cells(v, c0, ncb, tid, acc);
+  epi.end(v * nblk + blk);
+}
+
+// ── forward projection, parallel, binned ───────────────────────────────────
+// The parallel-beam counterpart of forward_cone_binned_kernel for a VCD
+// subset: one CTA per (channel block of kFwdCB, view), thread m owns
+// detector row m (row m of a parallel view is slice m of the band, so its
+// value for a pixel is the pixel's cylinder entry m, with no vertical fan).
+// The CTA walks its run of the channel-sorted list (keys c0 .. c0 + 17):
+// records are staged in shared memory a round at a time, and each thread
+// loads the row's values of kParEB pixels at once (coalesced over the rows)
+// before accumulating them.  With the pixels in channel order, the three
+// channel sums a pixel adds to stay in registers (q0..q2 for accumulator
+// rows cj .. cj + 2) and a row that leaves is added into the thread's
+// private shared-memory column once.  No atomics: each cell is a fixed
+// sequence of FMAs in list order.
+constexpr int kParEB = 8;  // pixel values in flight per thread
+
+__host__ __device__ inline size_t par_binned_smem(int nthr) {
+  return (size_t)fwd_cap(nthr) * (sizeof(float4) + sizeof(int)) +
+         (size_t)(kFwdCB + 4) * nthr * sizeof(float);
+}
+
+template <typename EPI>
+__global__ void __launch_bounds__(1024)
+forward_parallel_binned_kernel(Geo g, int v_start, const float *__restrict__ values, int P,
+                               int band, const ConeFwdRec *__restrict__ recs,
+                               const int *__restrict__ list, const int *__restrict__ offs,
+                               unsigned char *__restrict__ touched, EPI epi) {
+  MBIR_PDL_ENTRY();
+  extern __shared__ float4 sm4[];
+  const int nthr = blockDim.x, tid = threadIdx.x;
+  const int cap = fwd_cap(nthr);
+  float4 *wq = sm4;                                   // cap x (w0, w1, w2, ctr)
+  int *rows = reinterpret_cast<int *>(wq + cap);      // cap cylinder rows
+  float *acc_s = reinterpret_cast<float *>(rows + cap);  // (kFwdCB + 4) x nthr
+  const int nblk = gridDim.x, blk = blockIdx.x, vl = blockIdx.y;
+  const int c0 = blk * kFwdCB;
+  const int ncb = min(kFwdCB, g.C - c0);
+  const ConeFwdRec *vrec = recs + (size_t)vl * P;
+  const int *vlist = list + (size_t)vl * P;
+  const int *voffs = offs + (size_t)vl * (fwd_nkeys(g.C) + 1);
+  const int start = voffs[c0];
+  const int end = voffs[min(c0 + kFwdCB + 2, fwd_nkeys(g.C))];
+  const int v = v_start + vl;
+  if (tid == 0) touched[(size_t)v * nblk + blk] = end > start;
+  if (end == start) {
+    epi.begin(v);
+    epi.end(v * nblk + blk);
+    return;
+  }
+#pragma unroll
+  for (int r = 0; r < kFwdCB + 4; ++r) acc_s[r * nthr + tid] = 0.f;
+  epi.prefetch(v, c0, ncb);
+  const bool mine = tid < band;
+  int cj = -1;
+  float q0 = 0.f, q1 = 0.f, q2 = 0.f;
+  for (int base = start; base < end; base += cap) {
+    const int n = min(cap, end - base);
+    __syncthreads();
+    for (int i = tid; i < n; i += nthr) {
+      const ConeFwdRec &r = vrec[vlist[base + i]];
+      const float4 b = r.b, c = r.c;
+      wq[i] = make_float4(b.y, b.z, b.w, c.z);
+      rows[i] = __float_as_int(c.w);
+    }
+    __syncthreads();
+    if (!mine) continue;
+    if (cj < 0) cj = __float_as_int(wq[0].w) - c0 + 1;
+    for (int e0 = 0; e0 < n; e0 += kParEB) {
+      const int nb = min(kParEB, n - e0);
+      float val[kParEB];
+#pragma unroll
+      for (int u = 0; u < kParEB; ++u)
+        val[u] = u < nb ? __ldg(values + (size_t)rows[e0 + u] * band + tid) : 0.f;
+#pragma unroll
+      for (int u = 0; u < kParEB; ++u) {
+        if (u >= nb) break;
+        const float4 w = wq[e0 + u];
+        const int j = __float_as_int(w.w) - c0 + 1;  // in [0, kFwdCB + 1], nondecreasing
+        if (j != cj) {
+          float *a = acc_s + cj * nthr + tid;
+          a[0] += q0;
+          if (j == cj + 1) {
+            q0 = q1;
+            q1 = q2;
+          } else {
+            a[nthr] += q1;
+            if (j == cj + 2) {
+              q0 = q2;
+            } else {
+              a[2 * nthr] += q2;
+              q0 = 0.f;
+            }
+            q1 = 0.f;
+          }
+          q2 = 0.f;
+          cj = j;
+        }
+        q0 = fmaf(w.x, val[u], q0);
+        q1 = fmaf(w.y, val[u], q1);
+        q2 = fmaf(w.z, val[u], q2);
+      }
+    }
+  }
+  if (mine) {
+    float *a = acc_s + cj * nthr + tid;
+    a[0] += q0;
+    a[nthr] += q1;
+    a[2 * nthr] += q2;
+  }
+  float acc[kFwdCB];
+#pragma unroll
+  for (int j = 0; j < kFwdCB; ++j) acc[j] = acc_s[(j + 2) * nthr + tid];
+  epi.begin(v);
+  if (mine) epi.cells(v, c0, ncb, tid, acc);
   epi.end(v * nblk + blk);
 }
 
