@@ -657,12 +657,15 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
         return fail(MBIR_ERR_CUDA, "VCD update: shared memory request of %zu bytes refused: %s",
                     smem, cudaGetErrorString(e));
     }
+    // tiles per tile-role CTA: about 4096 cells each
+    const int tpc = std::max(1, std::min(nblk, 4096 / (kFwdCB * R)));
     const long long ctas = (long long)nbin + (long long)w.upd_chunks * w.upd_yblocks +
-                           (long long)nblk * V;
+                           (long long)((nblk + tpc - 1) / tpc) * V;
     tpre(st);
     launch(k, (unsigned)ctas, 256, smem, st, nbin, tb, (int)Ps, S, kUpdChunk, pix, w.delta,
            w.alpha, flat, w.sq_part, w.l1_part, w.counters + 1, accum, w.upd_chunks,
-           w.upd_yblocks, C, R, kFwdCB, w.bins.touched, err, static_cast<const T *>(w.ad), nblk);
+           w.upd_yblocks, C, R, kFwdCB, w.bins.touched, err, static_cast<const T *>(w.ad), nblk,
+           tpc);
     MBIR_CHECK_LAUNCH("vcd pixel + sinogram update");
     if (binned_next) *binned_next = nbin > 0;
     return MBIR_OK;

@@ -555,35 +555,40 @@ __global__ void vcd_sino_update_kernel<float>(size_t n, const float *__restrict_
     e[i] = __fsub_rn(e[i], __fmul_rn(a, ad[i]));
 }
 
-// One tile (channel block b, view v) of the touched-tile sinogram update:
-// e -= alpha * Ad over CB consecutive channels of one view (one contiguous
-// run of CB * R cells), skipped when the binned forward marked the tile as
-// not reached.
+// Tiles [bg * tpc, bg * tpc + tpc) of view v (channel blocks of CB channels)
+// of the touched-tile sinogram update: e -= alpha * Ad over each tile's CB
+// consecutive channels (one contiguous run of CB * R cells), skipping the
+// tiles the binned forward marked as not reached.  Short detectors give a
+// CTA several tiles (tpc > 1) so that it still moves a few thousand cells.
 template <typename T>
 __device__ __forceinline__ void sino_tile_cta(int C, int R, int CB,
                                               const unsigned char *__restrict__ touched,
                                               const float *__restrict__ alpha, T *__restrict__ e,
-                                              const T *__restrict__ ad, int b, int v, int nblk) {
-  if (!touched[(size_t)v * nblk + b]) return;
+                                              const T *__restrict__ ad, int bg, int v, int nblk,
+                                              int tpc) {
   const float a = alpha[0];
-  const int c0 = b * CB;
-  const int n = min(CB, C - c0) * R;
-  const size_t base = ((size_t)v * C + c0) * R;
-  T *et = e + base;
-  const T *dt = ad + base;
-  constexpr int U = 4;
-  for (int i0 = threadIdx.x; i0 < n; i0 += 256 * U) {
-    float ev[U], dv[U];
+  const int b_end = min(nblk, (bg + 1) * tpc);
+  for (int b = bg * tpc; b < b_end; ++b) {
+    if (!touched[(size_t)v * nblk + b]) continue;
+    const int c0 = b * CB;
+    const int n = min(CB, C - c0) * R;
+    const size_t base = ((size_t)v * C + c0) * R;
+    T *et = e + base;
+    const T *dt = ad + base;
+    constexpr int U = 4;
+    for (int i0 = threadIdx.x; i0 < n; i0 += 256 * U) {
+      float ev[U], dv[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int i = i0 + 256 * u;
-      ev[u] = i < n ? to_f32(et[i]) : 0.f;
-      dv[u] = i < n ? to_f32(dt[i]) : 0.f;
-    }
+      for (int u = 0; u < U; ++u) {
+        const int i = i0 + 256 * u;
+        ev[u] = i < n ? to_f32(et[i]) : 0.f;
+        dv[u] = i < n ? to_f32(dt[i]) : 0.f;
+      }
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int i = i0 + 256 * u;
-      if (i < n) et[i] = from_f32<T>(__fsub_rn(ev[u], __fmul_rn(a, dv[u])));
+      for (int u = 0; u < U; ++u) {
+        const int i = i0 + 256 * u;
+        if (i < n) et[i] = from_f32<T>(__fsub_rn(ev[u], __fmul_rn(a, dv[u])));
+      }
     }
   }
 }
@@ -603,7 +608,7 @@ struct TailBins {
 // [0, nbin) bin the next subset of a partition pass (cone_bin_view, one
 // view each; nbin = 0 when there is none), the next ux * uy CTAs update the
 // recon (pixel_update_cta) and the rest update the sinogram's touched tiles
-// (sino_tile_cta, nblk x V).  The three roles share no buffer, so the
+// (sino_tile_cta, ceil(nblk / tpc) x V).  The three roles share no buffer, so the
 // latency-bound binning and recon update run under the HBM-bound tile
 // update.  Dynamic shared memory: the binning's key counters.  Six CTAs
 // per SM (at most 40 registers) keep enough of the tile update's loads in
@@ -616,7 +621,7 @@ vcd_tail_kernel(int nbin, TailBins tb, int P, int S, int pchunk, const int64_t *
                 double *__restrict__ l1_part, unsigned int *__restrict__ counter,
                 double *__restrict__ accum, int ux, int uy, int C, int R, int CB,
                 const unsigned char *__restrict__ touched, T *__restrict__ e,
-                const T *__restrict__ ad, int nblk) {
+                const T *__restrict__ ad, int nblk, int tpc) {
   MBIR_PDL_ENTRY();
   extern __shared__ int tail_sm[];
   int b = blockIdx.x;
@@ -631,7 +636,8 @@ vcd_tail_kernel(int nbin, TailBins tb, int P, int S, int pchunk, const int64_t *
     return;
   }
   b -= ux * uy;
-  sino_tile_cta<T>(C, R, CB, touched, alpha, e, ad, b % nblk, b / nblk, nblk);
+  const int ngrp = (nblk + tpc - 1) / tpc;
+  sino_tile_cta<T>(C, R, CB, touched, alpha, e, ad, b % ngrp, b / ngrp, nblk, tpc);
 }
 
 // ── QGGMRF denoiser (identity forward model; denoising.py:35-83) ──────────
