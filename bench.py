@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--storage", default="float32")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the projector, mixed-precision and CPU-baseline extras")
-    ap.add_argument("--profile-case", choices=["recon", "subset", "projectors"], default=None,
+    ap.add_argument("--profile-case", choices=["recon", "subset", "projectors",
+                                               "subset-parallel"], default=None,
                     help="run one untimed pass of the workload for an external profiler "
                          "and exit (no JSON line)")
     return ap.parse_args()
@@ -64,7 +65,8 @@ def profile_case(case, m, mb, torch, y):
     """One pass for a profiler: 'recon' is one whole reconstruction;
     'subset' is three VCD subset steps of a 128-subset partition (the subset
     size of 17 of the 20 iterations) from a zero volume; 'projectors' is one
-    full-volume forward and one back projection."""
+    full-volume forward and one back projection.  ('subset-parallel', one
+    partition pass of the parallel workload, is dispatched in main.)"""
     if case == "recon":
         np.random.seed(0)
         m.recon(y, max_iterations=ITERS, stop_threshold_change_pct=0, logfile_path=None,
@@ -227,6 +229,85 @@ def cpu_baseline(m, y_host, reg, mb):
             "seconds_per_recon_extrapolated": per_recon}
 
 
+# The HBM-bound VCD case: a parallel-beam subset step touches most of the
+# sinogram for few voxel-views (survey example: 512^2 x 256 volume, 720 views).
+PAR_V, PAR_R, PAR_C, PAR_N = 720, 256, 768, 512
+
+
+def make_parallel_model(mb):
+    m = mb.ParallelBeamModel((PAR_V, PAR_R, PAR_C),
+                             np.linspace(0, np.pi, PAR_V, endpoint=False))
+    m.set_params(no_warning=True, verbose=0, recon_shape=(PAR_N, PAR_N, PAR_R))
+    return m
+
+
+def parallel_pass_setup(mb, torch):
+    """A parallel 512^2 x 256 model, 720 views, 256 x 768 detector, its VCD
+    engine (FP32 storage, unweighted) on a seeded stand-in error sinogram
+    (566 MB, above L2; a step's cost does not depend on the values), and one
+    128-subset partition with its order."""
+    from mbirtorch_b200 import _lib
+    from mbirtorch_b200.vcd_engine import ResidentSinogram
+    m = make_parallel_model(mb)
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device=dev).manual_seed(3)
+    y = torch.rand((PAR_V, PAR_R, PAR_C), generator=gen, device=dev)
+    m.auto_set_regularization_params(y)
+    H = m.compute_hessian_diagonal(output_sharded=True)
+    upd = m.create_vcd_subset_updater(H, weights=1)
+    rs = m.get_params("recon_shape")
+    flat = torch.zeros(rs[0] * rs[1], rs[2], device=dev)
+    err = ResidentSinogram.from_vrc(y, _lib.MBIR_F32)
+    del y
+    rng = np.random.RandomState(0)
+    part = torch.as_tensor(mb.gen_pixel_partition(rs, 128, rng=rng), device=dev)
+    order = rng.permutation(part.shape[0]).astype(np.int32)
+    acc = torch.zeros(2 + rs[2], dtype=torch.float64, device=dev)
+    return m, upd, flat, err, part, order, acc
+
+
+def parallel_subset_extra(mb, torch, hbm):
+    """One 128-subset partition pass of the parallel workload above: the
+    pass's CUDA-event time (kernels chained as in a recon), then each
+    kernel's CUDA-event average from a second, per-launch timed pass, and
+    the binned forward + line search and the tail against the measured HBM
+    bandwidth (algorithmic bytes: e read and A delta written, resp. e and
+    A delta read and e written, over the reached part of the sinogram)."""
+    from mbirtorch_b200 import _lib
+    m, upd, flat, err, part, order, acc = parallel_pass_setup(mb, torch)
+    upd.engine.partition_pass(flat, err, part, order, acc)  # warm-up
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    upd.engine.partition_pass(flat, err, part, order, acc)
+    ev[1].record()
+    torch.cuda.synchronize()
+    pass_ms = ev[0].elapsed_time(ev[1])
+    _lib.timing_collect()
+    _lib.timing_enable(True)
+    upd.engine.partition_pass(flat, err, part, order, acc)
+    torch.cuda.synchronize()
+    _lib.timing_enable(False)
+    kt = _lib.timing_collect()
+    frac = shadow_fraction(m, mb)
+    sino = PAR_V * PAR_R * PAR_C
+    out = {"workload": f"parallel {PAR_N}^2 x {PAR_R} volume, {PAR_V} views, {PAR_R} x {PAR_C} "
+                       f"detector, FP32 storage, one 128-subset pass "
+                       f"({int(part.shape[1])} pixels per subset)",
+           "subset_step_us": 1e3 * pass_ms / part.shape[0], "shadow_fraction": frac,
+           "kernels_us": {k: 1e3 * v[0] / v[1] for k, v in kt.items()}}
+    for name, nbytes in (("vcd forward + line search", 2 * 4 * frac * sino),
+                         ("vcd pixel + sinogram update", 3 * 4 * frac * sino)):
+        if name in kt:
+            t = kt[name][0] / kt[name][1] / 1e3
+            out[name] = {"algorithmic_bytes": nbytes, "achieved_gbs": nbytes / t / 1e9,
+                         "frac_of_measured_hbm": nbytes / t / 1e9 / hbm}
+    vv = int(part.shape[1]) * PAR_R * PAR_V
+    t_f = kt["vcd forward + line search"][0] / kt["vcd forward + line search"][1] / 1e3
+    out["forward_gvox_views_per_s"] = vv / t_f / 1e9
+    return out
+
+
 def shadow_fraction(m, mb):
     """Fraction of (view, channel) columns that the ROR pixels' channel taps
     reach (the part of the sinogram a subset step must touch)."""
@@ -234,20 +315,25 @@ def shadow_fraction(m, mb):
     rs = m.get_params('recon_shape')
     idx = mb.gen_full_indices(rs).astype(np.int64)
     g = m._geometry()
+    Cm = g.num_det_channels
     row, col = idx // rs[1], idx % rs[1]
     yt = g.delta_voxel_row * (row - (rs[0] - 1) / 2.0)
     xt = g.delta_voxel * (col - (rs[1] - 1) / 2.0)
     tot = 0
-    for a in m._view_params_array()[:, 0][::12]:
+    vp = m._view_params_array()
+    angles = vp[:, 0] if vp.ndim == 2 else vp
+    for a in angles[::12]:
         x = np.cos(a) * xt - np.sin(a) * yt
         y = np.sin(a) * xt + np.cos(a) * yt
-        mag = 1.0 / (1.0 / g.magnification - y / g.source_detector_dist)
-        n = np.rint(mag * x / g.delta_det_channel + (C - 1) / 2.0).astype(int)
-        hit = np.zeros(C + 8, bool)
+        mag = 1.0 / (1.0 / g.magnification - y / g.source_detector_dist) \
+            if g.geometry == 1 else 1.0
+        n = np.rint((mag * x + g.det_channel_offset) / g.delta_det_channel
+                    + (Cm - 1) / 2.0).astype(int)
+        hit = np.zeros(Cm + 8, bool)
         for t in range(-g.psf_radius, g.psf_radius + 1):
-            hit[np.clip(n + t, 0, C - 1)] = True
-        tot += hit[:C].mean()
-    return tot / len(m._view_params_array()[::12])
+            hit[np.clip(n + t, 0, Cm - 1)] = True
+        tot += hit[:Cm].mean()
+    return tot / len(angles[::12])
 
 
 def main():
@@ -277,6 +363,12 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    if args.profile_case == "subset-parallel":
+        # one 128-subset partition pass of the parallel 512^2 x 256 workload
+        _, upd, flat, err, part, order, acc = parallel_pass_setup(mb, torch)
+        upd.engine.partition_pass(flat, err, part, order, acc)
+        torch.cuda.synchronize()
+        return
     m = make_model(mb)
     m.set_storage_precision(args.storage)
     vol, y = make_data(mb, m, torch, dev)
@@ -447,6 +539,7 @@ def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd):
     res["mixed_precision"] = mp
     res["serving"] = serving_extra(mb, torch, y_host, rec_ref)
     res["serving_mix"] = serving_mix_extra(mb, torch)
+    res["parallel_subset"] = parallel_subset_extra(mb, torch, hbm)
     res["fm_rmse_final"] = rd["recon_params"]["fm_rmse"][-1]
     # ── CPU baseline ──
     try:

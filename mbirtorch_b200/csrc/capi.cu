@@ -161,8 +161,14 @@ struct BackShape {
   size_t smem;
 };
 
+// l2_views: also split the views so that one chunk's FP32 sinogram slab
+// stays within about 32 MB of L2.  CTAs are dispatched chunk by chunk, so
+// the warps in flight then share a window of views, and the cells that
+// several subset pixels read come from L2 instead of being re-read from
+// HBM (a VCD subset reads each reached cell once per pixel whose taps
+// reach it).
 BackShape back_shape(const mbir_geometry *g, int view_count, long long P, int band,
-                     size_t partial_budget_bytes) {
+                     size_t partial_budget_bytes, bool l2_views = false) {
   BackShape s;
   if (g->geometry == MBIR_CONE) {
     s.T = 32;
@@ -186,6 +192,11 @@ BackShape back_shape(const mbir_geometry *g, int view_count, long long P, int ba
   const long long target = 148LL * 64;
   long long nch = warps >= target ? 1 : (target + warps - 1) / warps;
   nch = std::min<long long>(nch, std::max(1, view_count / 4));
+  if (l2_views) {
+    const size_t slab = (size_t)g->num_det_rows * g->num_det_channels * sizeof(float);
+    const long long vpc_l2 = std::max<long long>(4, (long long)(((size_t)32 << 20) / slab));
+    nch = std::max<long long>(nch, (view_count + vpc_l2 - 1) / vpc_l2);
+  }
   nch = std::min<long long>(nch, 64);
   const size_t per_chunk = (size_t)P * band * sizeof(float);
   if (nch > 1 && per_chunk > 0) {
@@ -436,6 +447,25 @@ int launch_par_binned(const mbir_geometry *g, int v_start, int v_count, const fl
     return fail(MBIR_ERR_INVALID, "%s: the binned parallel forward projects whole cylinders "
                 "(band %d, detector rows %d)", what, band, g->num_det_rows);
   const Geo geo = make_geo(*g);
+  if (band % 4 == 0 && band >= 128) {
+    // four rows per thread
+    const int nthr4 = (band / 4 + 31) / 32 * 32;
+    const size_t smem4 = par_binned4_smem(nthr4);
+    auto k4 = forward_parallel_binned4_kernel<EPI>;
+    if (smem4 > 48 * 1024) {
+      cudaError_t e =
+          cudaFuncSetAttribute(k4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem4);
+      if (e != cudaSuccess)
+        return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s",
+                    smem4, cudaGetErrorString(e));
+    }
+    dim3 grid(fwd_nblk(g), v_count);
+    tpre(st);
+    launch(k4, grid, nthr4, smem4, st, geo, v_start, values, (int)P, band,
+           (const ConeFwdRec *)b.recs, (const int *)b.list, (const int *)b.offs, b.touched, epi);
+    MBIR_CHECK_LAUNCH(what);
+    return MBIR_OK;
+  }
   const int nthr = cone_rt_threads(g);
   const size_t smem = par_binned_smem(nthr);
   auto k = forward_parallel_binned_kernel<EPI>;
@@ -522,7 +552,7 @@ VcdWs vcd_layout(const mbir_geometry *g, long long Ps, const mbir_vcd_params *pr
   VcdWs w;
   const int S = g->num_slices, V = g->num_views;
   const size_t PS = (size_t)Ps * S;
-  w.bs = back_shape(g, V, Ps, S, (size_t)64 * PS * sizeof(float));
+  w.bs = back_shape(g, V, Ps, S, (size_t)64 * PS * sizeof(float), true);
   Carver c(base);
   w.grad_part = c.take<float>((size_t)std::max(1, w.bs.nchunks) * PS);
   w.delta = c.take<float>(PS);

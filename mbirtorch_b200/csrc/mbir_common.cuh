@@ -89,6 +89,37 @@ template <> __device__ __forceinline__ __half from_f32<__half>(float v) {
   return __float2half_rn(v);
 }
 
+// Four consecutive stored values at p (16-byte aligned for FP32, 8-byte for
+// 16-bit types) as one vector access.
+template <typename T>
+__device__ __forceinline__ void load4(const T *p, float (&o)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+  } else {
+    const uint2 v = *reinterpret_cast<const uint2 *>(p);
+    const T *t = reinterpret_cast<const T *>(&v);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = to_f32(t[k]);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void store4(T *p, const T (&s)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4(s[0], s[1], s[2], s[3]);
+  } else {
+    uint2 v;
+    T *t = reinterpret_cast<T *>(&v);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) t[k] = s[k];
+    *reinterpret_cast<uint2 *>(p) = v;
+  }
+}
+
 // ── geometry chains ────────────────────────────────────────────────────────
 // Un-rotated pixel centre (x, y) relative to iso (note the (i, j) -> (y, x)
 // order of the reference).

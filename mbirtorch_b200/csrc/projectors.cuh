@@ -1109,6 +1109,20 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
 // sequence of FMAs in list order.
 constexpr int kParEB = 8;  // pixel values in flight per thread
 
+__device__ __forceinline__ float4 f4_add(float4 a, float4 b) {
+  return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z),
+                     __fadd_rn(a.w, b.w));
+}
+
+__device__ __forceinline__ float4 f4_fma(float w, float4 x, float4 q) {
+  return make_float4(fmaf(w, x.x, q.x), fmaf(w, x.y, q.y), fmaf(w, x.z, q.z), fmaf(w, x.w, q.w));
+}
+
+__host__ __device__ inline size_t par_binned4_smem(int nthr) {
+  return (size_t)fwd_cap(nthr) * (sizeof(float4) + sizeof(int)) +
+         (size_t)(kFwdCB + 4) * nthr * sizeof(float4);
+}
+
 __host__ __device__ inline size_t par_binned_smem(int nthr) {
   return (size_t)fwd_cap(nthr) * (sizeof(float4) + sizeof(int)) +
          (size_t)(kFwdCB + 4) * nthr * sizeof(float);
@@ -1207,6 +1221,118 @@ forward_parallel_binned_kernel(Geo g, int v_start, const float *__restrict__ val
   for (int j = 0; j < kFwdCB; ++j) acc[j] = acc_s[(j + 2) * nthr + tid];
   epi.begin(v);
   if (mine) epi.cells(v, c0, ncb, tid, acc);
+  epi.end(v * nblk + blk);
+}
+
+// Four rows per thread (band a multiple of 4, at least 128 rows): thread t
+// owns detector rows 4t .. 4t + 3, loads their four values of a pixel as one
+// 16-byte access and keeps four sets of the three channel sums, so that the
+// per-record work (record loads, key test, loop) is shared by four cells.
+// Each cell's sum is the same sequence of FMAs as in
+// forward_parallel_binned_kernel.
+template <typename EPI>
+__global__ void __launch_bounds__(256)
+forward_parallel_binned4_kernel(Geo g, int v_start, const float *__restrict__ values, int P,
+                                int band, const ConeFwdRec *__restrict__ recs,
+                                const int *__restrict__ list, const int *__restrict__ offs,
+                                unsigned char *__restrict__ touched, EPI epi) {
+  MBIR_PDL_ENTRY();
+  extern __shared__ float4 sm4[];
+  const int nthr = blockDim.x, tid = threadIdx.x;
+  const int cap = fwd_cap(nthr);
+  float4 *wq = sm4;                                        // cap x (w0, w1, w2, ctr)
+  int *rows = reinterpret_cast<int *>(wq + cap);           // cap cylinder rows
+  float4 *acc_s = reinterpret_cast<float4 *>(rows + cap);  // (kFwdCB + 4) x nthr
+  const int nblk = gridDim.x, blk = blockIdx.x, vl = blockIdx.y;
+  const int c0 = blk * kFwdCB;
+  const int ncb = min(kFwdCB, g.C - c0);
+  const ConeFwdRec *vrec = recs + (size_t)vl * P;
+  const int *vlist = list + (size_t)vl * P;
+  const int *voffs = offs + (size_t)vl * (fwd_nkeys(g.C) + 1);
+  const int start = voffs[c0];
+  const int end = voffs[min(c0 + kFwdCB + 2, fwd_nkeys(g.C))];
+  const int v = v_start + vl;
+  if (tid == 0) touched[(size_t)v * nblk + blk] = end > start;
+  if (end == start) {
+    epi.begin(v);
+    epi.end(v * nblk + blk);
+    return;
+  }
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int r = 0; r < kFwdCB + 4; ++r) acc_s[r * nthr + tid] = z4;
+  epi.prefetch(v, c0, ncb);
+  const int m0 = 4 * tid;
+  const bool mine = m0 < band;
+  int cj = -1;
+  float4 q0 = z4, q1 = z4, q2 = z4;
+  for (int base = start; base < end; base += cap) {
+    const int n = min(cap, end - base);
+    __syncthreads();
+    for (int i = tid; i < n; i += nthr) {
+      const ConeFwdRec &r = vrec[vlist[base + i]];
+      const float4 b = r.b, c = r.c;
+      wq[i] = make_float4(b.y, b.z, b.w, c.z);
+      rows[i] = __float_as_int(c.w);
+    }
+    __syncthreads();
+    if (!mine) continue;
+    if (cj < 0) cj = __float_as_int(wq[0].w) - c0 + 1;
+    for (int e0 = 0; e0 < n; e0 += kParEB) {
+      const int nb = min(kParEB, n - e0);
+      float4 val[kParEB];
+#pragma unroll
+      for (int u = 0; u < kParEB; ++u)
+        val[u] = u < nb ? __ldg(reinterpret_cast<const float4 *>(
+                              values + (size_t)rows[e0 + u] * band + m0))
+                        : z4;
+#pragma unroll
+      for (int u = 0; u < kParEB; ++u) {
+        if (u >= nb) break;
+        const float4 w = wq[e0 + u];
+        const int j = __float_as_int(w.w) - c0 + 1;  // in [0, kFwdCB + 1], nondecreasing
+        if (j != cj) {
+          float4 *a = acc_s + cj * nthr + tid;
+          a[0] = f4_add(a[0], q0);
+          if (j == cj + 1) {
+            q0 = q1;
+            q1 = q2;
+          } else {
+            a[nthr] = f4_add(a[nthr], q1);
+            if (j == cj + 2) {
+              q0 = q2;
+            } else {
+              a[2 * nthr] = f4_add(a[2 * nthr], q2);
+              q0 = z4;
+            }
+            q1 = z4;
+          }
+          q2 = z4;
+          cj = j;
+        }
+        q0 = f4_fma(w.x, val[u], q0);
+        q1 = f4_fma(w.y, val[u], q1);
+        q2 = f4_fma(w.z, val[u], q2);
+      }
+    }
+  }
+  if (mine) {
+    float4 *a = acc_s + cj * nthr + tid;
+    a[0] = f4_add(a[0], q0);
+    a[nthr] = f4_add(a[nthr], q1);
+    a[2 * nthr] = f4_add(a[2 * nthr], q2);
+  }
+  float acc[kFwdCB][4];
+#pragma unroll
+  for (int j = 0; j < kFwdCB; ++j) {
+    const float4 a = acc_s[(j + 2) * nthr + tid];
+    acc[j][0] = a.x;
+    acc[j][1] = a.y;
+    acc[j][2] = a.z;
+    acc[j][3] = a.w;
+  }
+  epi.begin(v);
+  if (mine) epi.cells4(v, c0, ncb, m0, acc);
   epi.end(v * nblk + blk);
 }
 

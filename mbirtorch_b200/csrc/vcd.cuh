@@ -341,6 +341,52 @@ struct LineSearchEpi {
       }
     }
   }
+  // Four consecutive rows m0 .. m0 + 3 of channels c0 .. c0 + ncb - 1 (R and
+  // m0 multiples of 4, so each channel's four cells are one aligned 16-byte
+  // (FP32) or 8-byte (16-bit) access), eight channels' loads in flight
+  // before their stores.
+  template <int N>
+  __device__ __forceinline__ void cells4(int v, int c0, int ncb, int m0,
+                                         const float (&acc)[N][4]) {
+    const size_t i0 = ((size_t)v * C + c0) * R + m0;
+#pragma unroll
+    for (int g0 = 0; g0 < N; g0 += 8) {
+      float ev[8][4], wv[8][4];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ev[j][k] = wv[j][k] = 0.f;
+        if (with_sums && g0 + j < ncb) {
+          load4(e + i0 + (size_t)(g0 + j) * R, ev[j]);
+          if (w != nullptr) load4(w + i0 + (size_t)(g0 + j) * R, wv[j]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (g0 + j < ncb) {
+          T st[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) st[k] = from_f32<T>(__fmul_rn(acc[g0 + j][k], inv_scale));
+          store4(ad + i0 + (size_t)(g0 + j) * R, st);
+          if (with_sums) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const float adv = __fmul_rn(to_f32(st[k]), scale);
+              const float evs = __fmul_rn(ev[j][k], scale);
+              if (w != nullptr) {
+                const float wvs = __fmul_rn(wv[j][k], wscale);
+                fl += (double)__fmul_rn(__fmul_rn(wvs, evs), adv);
+                fq += (double)__fmul_rn(__fmul_rn(adv, adv), wvs);
+              } else {
+                fl += (double)__fmul_rn(evs, adv);
+                fq += (double)__fmul_rn(adv, adv);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
   __device__ __forceinline__ void end(int slot) {
     if (!with_sums) return;
     block_sum2(fl, fq);

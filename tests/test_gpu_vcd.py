@@ -418,15 +418,20 @@ def test_parallel_partition_pass_ragged_channels_many_rows():
     assert rel_l2(err.to_vrc().cpu().numpy(), oerr) <= 2e-5
 
 
-def test_parallel_subset_step_binned_view_chunks_positivity():
+@pytest.mark.parametrize("rows", [4, 128])
+def test_parallel_subset_step_binned_view_chunks_positivity(rows):
     """A whole-image parallel subset (65536 pixels x 40 views) splits the
     binned forward into view chunks; weighted, with positivity (the
     re-projection goes through the bins too): one step against the FP64
-    oracle."""
+    oracle.  128 rows take the four-rows-per-thread forward, whose 16-bit
+    epilogue is checked too (float16 storage against the FP32 step)."""
     from oracle import vcd as ovcd
+    from mbirtorch_b200.vcd_engine import ResidentSinogram
+    from mbirtorch_b200 import _lib
     V = 40
-    m = mb.ParallelBeamModel((V, 4, 320), np.linspace(0, np.pi, V, endpoint=False))
-    m.set_params(no_warning=True, verbose=0, recon_shape=(256, 256, 4), positivity_flag=True)
+    m = mb.ParallelBeamModel((V, rows, 320), np.linspace(0, np.pi, V, endpoint=False))
+    m.set_params(no_warning=True, verbose=0, recon_shape=(256, 256, rows),
+                 positivity_flag=True)
     rs = m.get_params('recon_shape')
     rng = np.random.default_rng(13)
     x_true = rng.random(rs).astype(np.float32)
@@ -450,3 +455,21 @@ def test_parallel_subset_step_binned_view_chunks_positivity():
     assert abs(float(alpha) - oalpha) / oalpha <= 1e-4
     assert rel_l2(flat.cpu().numpy(), oflat) <= 1e-5
     assert rel_l2(err.cpu().numpy(), oerr) <= 1e-5
+    if rows == 128:
+        w16 = ResidentSinogram.from_vrc(torch.as_tensor(w, device='cuda'), _lib.MBIR_F16)
+        Hd = torch.as_tensor(np.ascontiguousarray(np.asarray(H).reshape(-1, rs[2])),
+                             device='cuda')
+        eng = m._make_engine(Hd, w16, _lib.MBIR_F16, max_subset_pixels=idx.size)
+        f16 = torch.as_tensor(x0.reshape(-1, rs[2]), device='cuda').clone()
+        e16 = ResidentSinogram.from_vrc(torch.as_tensor(e0, device='cuda'), _lib.MBIR_F16)
+        # storing e in float16 alone (before any step) costs this much
+        q0 = rel_l2(e16.to_vrc().cpu().numpy(), e0)
+        _, a16, _ = eng.subset_update(f16, e16, torch.as_tensor(idx, device='cuda'))
+        assert abs(float(a16) - float(alpha)) / float(alpha) <= 1e-3
+        assert rel_l2(f16.cpu().numpy(), flat.cpu().numpy()) <= 1e-3
+        # the step's error, in units of |e0| (the step shrinks e, so relative
+        # to the new e it reads larger): the rounding of e0, of A delta and
+        # of the new e, each at most the storage rounding q0
+        e_new = err.cpu().numpy().astype(np.float64)
+        gap = np.linalg.norm(e16.to_vrc().cpu().numpy() - e_new) / np.linalg.norm(e0)
+        assert gap <= 3 * q0
