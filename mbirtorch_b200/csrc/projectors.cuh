@@ -152,26 +152,41 @@ back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_cou
     }
     __syncwarp();
     if (!active) continue;
-    for (int i = 0; i < nv; ++i) {
-      const int v = vg + i;
-      const int ctr = mytab[i].ctr;
-      float w[MT];
-      size_t base[MT];
+    // Two views per step: both views' taps are loaded before either is
+    // accumulated (the accumulation order is unchanged: view by view).
+    constexpr int VU = 2;
+    for (int i = 0; i < nv; i += VU) {
+      float w[VU][MT], scl[VU], col[VU][SPL][MT];
 #pragma unroll
-      for (int t = 0; t < MT; ++t) {
-        w[t] = mytab[i].w[t];
-        base[t] = rd.base(v, min(max(ctr + t - RT, 0), g.C - 1));
+      for (int u = 0; u < VU; ++u) {
+        const bool on = i + u < nv;
+        const int v = vg + (on ? i + u : i);
+        const int ctr = mytab[on ? i + u : i].ctr;
+        scl[u] = rd.scale(v);
+#pragma unroll
+        for (int t = 0; t < MT; ++t) {
+          w[u][t] = mytab[on ? i + u : i].w[t];
+          const size_t base = rd.base(v, min(max(ctr + t - RT, 0), g.C - 1));
+#pragma unroll
+          for (int j = 0; j < SPL; ++j) {
+            const int l = l0 + tl + T * j;
+            col[u][j][t] = (on && l < band && MBIR_TAP_ON(NT, t, nt)) ? rd.get(base + l) : 0.f;
+          }
+        }
       }
-      const float scl = rd.scale(v);
 #pragma unroll
-      for (int j = 0; j < SPL; ++j) {
-        const int l = l0 + tl + T * j;
-        if (l < band) {
-          float s = 0.f;
+      for (int u = 0; u < VU; ++u) {
+        if (i + u >= nv) break;
 #pragma unroll
-          for (int t = 0; t < MT; ++t)
-            if (MBIR_TAP_ON(NT, t, nt)) s = fmaf(w[t], rd.get(base[t] + l), s);
-          acc[j] = fmaf(scl, s, acc[j]);
+        for (int j = 0; j < SPL; ++j) {
+          const int l = l0 + tl + T * j;
+          if (l < band) {
+            float s = 0.f;
+#pragma unroll
+            for (int t = 0; t < MT; ++t)
+              if (MBIR_TAP_ON(NT, t, nt)) s = fmaf(w[u][t], col[u][j][t], s);
+            acc[j] = fmaf(scl[u], s, acc[j]);
+          }
         }
       }
     }
@@ -1118,9 +1133,11 @@ __device__ __forceinline__ float4 f4_fma(float w, float4 x, float4 q) {
   return make_float4(fmaf(w, x.x, q.x), fmaf(w, x.y, q.y), fmaf(w, x.z, q.z), fmaf(w, x.w, q.w));
 }
 
+constexpr int kPar4Cap = 128;  // records per round of the four-row forward
+
 __host__ __device__ inline size_t par_binned4_smem(int nthr) {
-  return (size_t)fwd_cap(nthr) * (sizeof(float4) + sizeof(int)) +
-         (size_t)(kFwdCB + 4) * nthr * sizeof(float4);
+  return (size_t)kPar4Cap * (sizeof(float4) + sizeof(int)) +
+         (size_t)kFwdCB * nthr * sizeof(float4);
 }
 
 __host__ __device__ inline size_t par_binned_smem(int nthr) {
@@ -1228,7 +1245,9 @@ forward_parallel_binned_kernel(Geo g, int v_start, const float *__restrict__ val
 // owns detector rows 4t .. 4t + 3, loads their four values of a pixel as one
 // 16-byte access and keeps four sets of the three channel sums, so that the
 // per-record work (record loads, key test, loop) is shared by four cells.
-// Each cell's sum is the same sequence of FMAs as in
+// The accumulator column holds the tile's kFwdCB channels only (a sum that
+// leaves the registers for a channel outside the tile is dropped).  Each
+// cell's sum is the same sequence of FMAs as in
 // forward_parallel_binned_kernel.
 template <typename EPI>
 __global__ void __launch_bounds__(256)
@@ -1239,10 +1258,9 @@ forward_parallel_binned4_kernel(Geo g, int v_start, const float *__restrict__ va
   MBIR_PDL_ENTRY();
   extern __shared__ float4 sm4[];
   const int nthr = blockDim.x, tid = threadIdx.x;
-  const int cap = fwd_cap(nthr);
-  float4 *wq = sm4;                                        // cap x (w0, w1, w2, ctr)
-  int *rows = reinterpret_cast<int *>(wq + cap);           // cap cylinder rows
-  float4 *acc_s = reinterpret_cast<float4 *>(rows + cap);  // (kFwdCB + 4) x nthr
+  float4 *wq = sm4;                                            // kPar4Cap x (w0, w1, w2, ctr)
+  int *rows = reinterpret_cast<int *>(wq + kPar4Cap);          // kPar4Cap cylinder rows
+  float4 *acc_s = reinterpret_cast<float4 *>(rows + kPar4Cap);  // kFwdCB x nthr
   const int nblk = gridDim.x, blk = blockIdx.x, vl = blockIdx.y;
   const int c0 = blk * kFwdCB;
   const int ncb = min(kFwdCB, g.C - c0);
@@ -1260,14 +1278,22 @@ forward_parallel_binned4_kernel(Geo g, int v_start, const float *__restrict__ va
   }
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-  for (int r = 0; r < kFwdCB + 4; ++r) acc_s[r * nthr + tid] = z4;
+  for (int r = 0; r < kFwdCB; ++r) acc_s[r * nthr + tid] = z4;
   epi.prefetch(v, c0, ncb);
   const int m0 = 4 * tid;
   const bool mine = m0 < band;
+  // slot r of the register window is channel c0 + r - 2; channel slot
+  // r - 2 of acc_s when inside the tile
+  auto spill = [&](int r, float4 q) {
+    if ((unsigned)(r - 2) < (unsigned)kFwdCB) {
+      float4 *a = acc_s + (r - 2) * nthr + tid;
+      *a = f4_add(*a, q);
+    }
+  };
   int cj = -1;
   float4 q0 = z4, q1 = z4, q2 = z4;
-  for (int base = start; base < end; base += cap) {
-    const int n = min(cap, end - base);
+  for (int base = start; base < end; base += kPar4Cap) {
+    const int n = min(kPar4Cap, end - base);
     __syncthreads();
     for (int i = tid; i < n; i += nthr) {
       const ConeFwdRec &r = vrec[vlist[base + i]];
@@ -1292,17 +1318,16 @@ forward_parallel_binned4_kernel(Geo g, int v_start, const float *__restrict__ va
         const float4 w = wq[e0 + u];
         const int j = __float_as_int(w.w) - c0 + 1;  // in [0, kFwdCB + 1], nondecreasing
         if (j != cj) {
-          float4 *a = acc_s + cj * nthr + tid;
-          a[0] = f4_add(a[0], q0);
+          spill(cj, q0);
           if (j == cj + 1) {
             q0 = q1;
             q1 = q2;
           } else {
-            a[nthr] = f4_add(a[nthr], q1);
+            spill(cj + 1, q1);
             if (j == cj + 2) {
               q0 = q2;
             } else {
-              a[2 * nthr] = f4_add(a[2 * nthr], q2);
+              spill(cj + 2, q2);
               q0 = z4;
             }
             q1 = z4;
@@ -1317,22 +1342,12 @@ forward_parallel_binned4_kernel(Geo g, int v_start, const float *__restrict__ va
     }
   }
   if (mine) {
-    float4 *a = acc_s + cj * nthr + tid;
-    a[0] = f4_add(a[0], q0);
-    a[nthr] = f4_add(a[nthr], q1);
-    a[2 * nthr] = f4_add(a[2 * nthr], q2);
-  }
-  float acc[kFwdCB][4];
-#pragma unroll
-  for (int j = 0; j < kFwdCB; ++j) {
-    const float4 a = acc_s[(j + 2) * nthr + tid];
-    acc[j][0] = a.x;
-    acc[j][1] = a.y;
-    acc[j][2] = a.z;
-    acc[j][3] = a.w;
+    spill(cj, q0);
+    spill(cj + 1, q1);
+    spill(cj + 2, q2);
   }
   epi.begin(v);
-  if (mine) epi.cells4(v, c0, ncb, m0, acc);
+  if (mine) epi.cells4(v, c0, ncb, m0, acc_s + tid, nthr);
   epi.end(v * nblk + blk);
 }
 

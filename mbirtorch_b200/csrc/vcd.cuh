@@ -343,17 +343,15 @@ struct LineSearchEpi {
   }
   // Four consecutive rows m0 .. m0 + 3 of channels c0 .. c0 + ncb - 1 (R and
   // m0 multiples of 4, so each channel's four cells are one aligned 16-byte
-  // (FP32) or 8-byte (16-bit) access), eight channels' loads in flight
-  // before their stores.
-  template <int N>
+  // (FP32) or 8-byte (16-bit) access).  Channel j's four sums are acc[j *
+  // stride]; four channels' loads go out before their stores.
   __device__ __forceinline__ void cells4(int v, int c0, int ncb, int m0,
-                                         const float (&acc)[N][4]) {
+                                         const float4 *__restrict__ acc, int stride) {
     const size_t i0 = ((size_t)v * C + c0) * R + m0;
+    for (int g0 = 0; g0 < ncb; g0 += 4) {
+      float ev[4][4], wv[4][4];
 #pragma unroll
-    for (int g0 = 0; g0 < N; g0 += 8) {
-      float ev[8][4], wv[8][4];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
+      for (int j = 0; j < 4; ++j) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) ev[j][k] = wv[j][k] = 0.f;
         if (with_sums && g0 + j < ncb) {
@@ -362,11 +360,13 @@ struct LineSearchEpi {
         }
       }
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
+      for (int j = 0; j < 4; ++j) {
         if (g0 + j < ncb) {
+          const float4 a4 = acc[(g0 + j) * stride];
+          const float a[4] = {a4.x, a4.y, a4.z, a4.w};
           T st[4];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) st[k] = from_f32<T>(__fmul_rn(acc[g0 + j][k], inv_scale));
+          for (int k = 0; k < 4; ++k) st[k] = from_f32<T>(__fmul_rn(a[k], inv_scale));
           store4(ad + i0 + (size_t)(g0 + j) * R, st);
           if (with_sums) {
 #pragma unroll
