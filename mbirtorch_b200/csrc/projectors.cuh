@@ -45,12 +45,20 @@ __device__ __forceinline__ void prefetch_l1(const void *p) {
 
 // ── sinogram readers (resident VCR layout) ─────────────────────────────────
 // value(v, c, m) = scale(v) * get(base(v, c) + m)
+// get4(i, o): the four values at i .. i + 3 as one vector access (i a
+// multiple of 4 and aligned16() true); aligned16() is checked on the host.
+__host__ __device__ inline bool is_aligned16(const void *p) {
+  return (reinterpret_cast<uintptr_t>(p) & 15u) == 0;
+}
+
 struct ReadF32 {
   const float *s;
   int C, R;
   __device__ __forceinline__ size_t base(int v, int c) const { return ((size_t)v * C + c) * R; }
   __device__ __forceinline__ float scale(int) const { return 1.f; }
   __device__ __forceinline__ float get(size_t i) const { return __ldg(s + i); }
+  __device__ __forceinline__ void get4(size_t i, float (&o)[4]) const { load4(s + i, o); }
+  __host__ bool aligned16() const { return is_aligned16(s); }
 };
 
 template <typename T>
@@ -61,6 +69,8 @@ struct ReadScaled {
   __device__ __forceinline__ size_t base(int v, int c) const { return ((size_t)v * C + c) * R; }
   __device__ __forceinline__ float scale(int v) const { return __ldg(es + v); }
   __device__ __forceinline__ float get(size_t i) const { return to_f32(e[i]); }
+  __device__ __forceinline__ void get4(size_t i, float (&o)[4]) const { load4(e + i, o); }
+  __host__ bool aligned16() const { return is_aligned16(e); }
 };
 
 // weights * error, the gradient's operand (tomography_model.py:2548-2552).
@@ -78,6 +88,14 @@ struct ReadWeighted {
   __device__ __forceinline__ float get(size_t i) const {
     return __fmul_rn(to_f32(w[i]), to_f32(e[i]));
   }
+  __device__ __forceinline__ void get4(size_t i, float (&o)[4]) const {
+    float ev[4], wv[4];
+    load4(e + i, ev);
+    load4(w + i, wv);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = __fmul_rn(wv[k], ev[k]);
+  }
+  __host__ bool aligned16() const { return is_aligned16(e) && is_aligned16(w); }
 };
 
 // Tap loops: NT is the compile-time tap count (3 for psf radius 1, the
@@ -198,6 +216,87 @@ back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_cou
       const int l = l0 + tl + T * j;
       if (l < band) o[l] = acc[j];
     }
+  }
+}
+
+// The parallel back projector at psf radius 1 with four consecutive slices
+// per lane (a team of 32 lanes covers 128 slices, as T = 32, SPL = 4 does):
+// each tap of a view is one 16-byte load per lane, and two views' taps are
+// in flight before either is accumulated.  Each output is the same sequence
+// of FMAs as in back_parallel_kernel.  Needs band a multiple of 4 and the
+// operands 16-byte aligned (checked on the host).
+template <int CP, typename RD>
+__global__ void __launch_bounds__(kThreads)
+back_parallel4_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
+                      RD rd, const int64_t *__restrict__ pix, int P, int band, int slice_chunks,
+                      float *__restrict__ out) {
+  MBIR_PDL_ENTRY();
+  __shared__ ParRec tab[kThreads];
+  constexpr int T = 32, MT = 3;
+  const int tid = threadIdx.x;
+  const int team = tid / T, tl = tid - team * T;
+  const int teams_per_block = kThreads / T;
+  const long long gteam = (long long)blockIdx.x * teams_per_block + team;
+  const int p = (int)(gteam / slice_chunks);
+  const int sc = (int)(gteam - (long long)p * slice_chunks);
+  const int l = sc * T * 4 + 4 * tl;  // this lane's slices l .. l + 3
+  const bool active = p < P;
+  const bool mine = active && l < band;
+  const int chunk = blockIdx.y;
+  const int vb = chunk * vpc, ve = min(v_count, vb + vpc);
+  ParRec *mytab = tab + team * T;
+  float xt = 0.f, yt = 0.f;
+  if (active) pixel_xy(g, (int)pix[p], xt, yt);
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+
+  for (int vg = vb; vg < ve; vg += T) {
+    const int nv = min(T, ve - vg);
+    __syncwarp();
+    if (active && tl < nv) {
+      const ParView pv = parallel_view(g, vp[2 * (v_start + vg + tl)]);
+      const float n_p = parallel_np(g, pv, xt, yt);
+      ParRec r;
+      r.ctr = (int)fminf(fmaxf(rintf(n_p), -1.0e6f), 1.0e6f);
+#pragma unroll
+      for (int t = 0; t < MT; ++t) {
+        const float a = tap_weight(n_p, r.ctr + t - 1, pv.half_w1, pv.lmax, pv.ws, g.C);
+        r.w[t] = CP == 2 ? __fmul_rn(a, a) : a;
+      }
+      mytab[tl] = r;
+    }
+    __syncwarp();
+    if (!mine) continue;
+    constexpr int VU = 2;
+    for (int i = 0; i < nv; i += VU) {
+      float w[VU][MT], scl[VU], col[VU][MT][4];
+#pragma unroll
+      for (int u = 0; u < VU; ++u) {
+        const int iu = i + u < nv ? i + u : i;
+        const int v = vg + iu;
+        const int ctr = mytab[iu].ctr;
+        scl[u] = rd.scale(v);
+#pragma unroll
+        for (int t = 0; t < MT; ++t) {
+          w[u][t] = mytab[iu].w[t];
+          rd.get4(rd.base(v, min(max(ctr + t - 1, 0), g.C - 1)) + l, col[u][t]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < VU; ++u) {
+        if (i + u >= nv) break;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          float s = 0.f;
+#pragma unroll
+          for (int t = 0; t < MT; ++t) s = fmaf(w[u][t], col[u][t][k], s);
+          acc[k] = fmaf(scl[u], s, acc[k]);
+        }
+      }
+    }
+  }
+  if (mine) {
+    float *o = out + (size_t)chunk * P * band + (size_t)p * band + l;
+    *reinterpret_cast<float4 *>(o) = make_float4(acc[0], acc[1], acc[2], acc[3]);
   }
 }
 
