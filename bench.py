@@ -308,6 +308,140 @@ def parallel_subset_extra(mb, torch, hbm):
     return out
 
 
+def phantom_torch(torch, shape, seed, dev):
+    """The ellipsoid phantom of phantom() built on the device for large
+    grids: 10 seeded ellipsoids on [-1, 1]^3 (centres U[-0.5, 0.5],
+    semi-axes U[0.05, 0.4], in-plane angle U[0, 180) deg, density
+    U[0.1, 1])."""
+    rng = np.random.default_rng(seed)
+    nr, nc, ns = shape
+    g1 = torch.linspace(-1, 1, nr, device=dev)
+    g0 = torch.linspace(-1, 1, nc, device=dev)
+    gz = torch.linspace(-1, 1, ns, device=dev)
+    Y, X = torch.meshgrid(g1, g0, indexing="ij")
+    vol = torch.zeros(shape, device=dev)
+    for _ in range(10):
+        c = rng.uniform(-0.5, 0.5, 3)
+        a = rng.uniform(0.05, 0.4, 3)
+        ang = np.deg2rad(rng.uniform(0, 180))
+        dens = float(rng.uniform(0.1, 1.0))
+        ca, sa = float(np.cos(ang)), float(np.sin(ang))
+        xr = ca * (X - c[0]) + sa * (Y - c[1])
+        yr = -sa * (X - c[0]) + ca * (Y - c[1])
+        xy = (xr / a[0]) ** 2 + (yr / a[1]) ** 2
+        z = ((gz - c[2]) / a[2]) ** 2
+        vol += dens * ((xy[:, :, None] + z[None, None, :]) <= 1).float()
+    return vol
+
+
+def cone_large_extra(mb, torch, iters=ITERS):
+    """The mixed-precision cone configuration: 512 x 512 x 256 ellipsoid
+    phantom, 720 views on [0, 2 pi), curved 320 x 768 detector (pitch 2),
+    SID 1024, SDD 2048, Poisson counts at I0 = 1e4, 20 VCD iterations; one
+    recon each with FP32, float16 and bfloat16 storage, their recons/s and
+    each 16-bit result's relative L2 to the FP32 result.  (The FP64 oracle
+    is out of reach at this size on the host; the tests hold the 16-bit
+    paths to the FP64 oracle at smaller sizes.)"""
+    dev = torch.device("cuda", 0)
+    Vl, Rl, Cl, Nl, Sl = 720, 320, 768, 512, 256
+    m = mb.ConeBeamModel((Vl, Rl, Cl), np.linspace(0, 2 * np.pi, Vl, endpoint=False),
+                         source_detector_dist=SDD, source_iso_dist=SID,
+                         use_curved_detector=True)
+    m.set_params(no_warning=True, verbose=0, delta_det_channel=2.0, delta_det_row=2.0)
+    m.auto_set_recon_geometry(no_warning=True)
+    m.set_params(no_warning=True, recon_shape=(Nl, Nl, Sl))
+    vol = phantom_torch(torch, (Nl, Nl, Sl), 5, dev)
+    clean = m.forward_project(vol, output_sharded=True)
+    del vol
+    mu = 3.0 / float(clean.max())
+    gen = torch.Generator(device=dev).manual_seed(2)
+    counts = torch.poisson(I0 * torch.exp(-mu * clean), generator=gen)
+    del clean
+    y = (-torch.log(torch.clamp(counts, min=1.0) / I0) / mu).to(torch.float32).contiguous()
+    del counts
+    out = {"workload": f"cone curved {Nl}x{Nl}x{Sl} volume, {Vl} views on [0, 2pi), "
+                       f"{Rl}x{Cl} detector (pitch 2), SID 1024, SDD 2048, Poisson I0=1e4, "
+                       f"{iters} VCD iterations",
+           "voxel_views_full_projection": int(m.full_indices_device().shape[0]) * Sl * Vl}
+    ref = None
+    for st in ("float32", "float16", "bfloat16"):
+        m.set_storage_precision(st)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        np.random.seed(0)
+        r, _ = m.recon(y, max_iterations=iters, stop_threshold_change_pct=0,
+                       logfile_path=None, print_logs=False, output_sharded=True)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        entry = {"recons_per_s": 1.0 / dt, "seconds": dt}
+        if ref is None:
+            ref = r.double()
+        else:
+            entry["rel_l2_vs_f32_recon"] = float((r.double() - ref).norm() / ref.norm())
+        out[st] = entry
+        del r
+    return out
+
+
+def autograd_extra(mb, torch, steps=3):
+    """The differentiable-projector configuration: a batch of 4 volumes of
+    128^3 (Gaussian-smoothed N(0, 1) fields, seeded), loss
+    sum w (A x - y)^2 with y from a second seeded volume and random
+    positive weights, forward + backward through weighted_residual_loss
+    (sinogram formed in view chunks of at most 2 GB, A x recomputed in the
+    backward), for parallel beam (256 views, 128 x 192) and cone beam (256
+    views, 128 x 192, magnification 1.5).  Per step: 3 projector calls per
+    volume (A x, A x again in the backward, A^T r)."""
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device=dev).manual_seed(4)
+
+    def field(n):
+        x = torch.randn((n, 1, 128, 128, 128), generator=gen, device=dev)
+        k = torch.exp(-0.5 * (torch.arange(-4, 5, device=dev, dtype=torch.float32) / 2.0) ** 2)
+        k = k / k.sum()
+        for dim in range(3):
+            shape = [1, 1, 1, 1, 1]
+            shape[2 + dim] = 9
+            pad = [0, 0, 0, 0, 0, 0]
+            pad[2 * (2 - dim)] = pad[2 * (2 - dim) + 1] = 4
+            x = torch.nn.functional.conv3d(torch.nn.functional.pad(x, pad, mode="replicate"),
+                                           k.view(shape))
+        return x[:, 0].contiguous()
+
+    out = {}
+    for kind in ("parallel", "cone"):
+        if kind == "parallel":
+            m = mb.ParallelBeamModel((256, 128, 192), np.linspace(0, np.pi, 256, endpoint=False))
+        else:
+            m = mb.ConeBeamModel((256, 128, 192), np.linspace(0, 2 * np.pi, 256, endpoint=False),
+                                 source_detector_dist=1152.0, source_iso_dist=768.0)
+            m.set_params(no_warning=True, delta_det_channel=1.5, delta_det_row=1.5)
+            m.auto_set_recon_geometry(no_warning=True)
+        m.set_params(no_warning=True, verbose=0, recon_shape=(128, 128, 128))
+        x = field(4).requires_grad_(True)
+        with torch.no_grad():
+            y = mb.forward_project_differentiable(m, field(4))
+        w = 0.5 + torch.rand(y.shape, generator=gen, device=dev)
+        for _ in range(2):
+            loss = mb.weighted_residual_loss(m, x, y, w)
+            loss.backward()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        for _ in range(steps):
+            x.grad = None
+            loss = mb.weighted_residual_loss(m, x, y, w)
+            loss.backward()
+        ev[1].record()
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1]) / steps
+        vv = int(m.full_indices_device().shape[0]) * 128 * 256
+        out[kind] = {"ms_per_step": ms, "volumes": 4,
+                     "gvox_views_per_s": 3 * 4 * vv / (ms / 1e3) / 1e9,
+                     "loss": float(loss.detach())}
+    return out
+
+
 def shadow_fraction(m, mb):
     """Fraction of (view, channel) columns that the ROR pixels' channel taps
     reach (the part of the sinogram a subset step must touch)."""
@@ -540,6 +674,8 @@ def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd):
     res["serving"] = serving_extra(mb, torch, y_host, rec_ref)
     res["serving_mix"] = serving_mix_extra(mb, torch)
     res["parallel_subset"] = parallel_subset_extra(mb, torch, hbm)
+    res["cone_large"] = cone_large_extra(mb, torch)
+    res["autograd"] = autograd_extra(mb, torch)
     res["fm_rmse_final"] = rd["recon_params"]["fm_rmse"][-1]
     # ── CPU baseline ──
     try:
