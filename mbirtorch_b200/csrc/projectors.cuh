@@ -722,8 +722,13 @@ constexpr int kFwdEB = 16;   // pixels staged per batch
 constexpr int kFwdVPad = 8;  // zero slices either side of a staged cylinder (>= 2 bp + 1)
 
 // Record capacity of one round (at least one scan chunk); the shared memory
-// also holds the stage and (kFwdCB + 4) accumulator rows per thread.
-__host__ __device__ inline int fwd_cap(int nthr) { return nthr > 256 ? nthr : 256; }
+// also holds the stage and (kFwdCB + 4) accumulator rows per thread.  Short
+// detectors (fewer than 128 threads) take two scan chunks per round: their
+// tiles hold a few tens of records, and a smaller round leaves room for
+// more CTAs per SM.
+__host__ __device__ inline int fwd_cap(int nthr) {
+  return nthr >= 128 ? (nthr > 256 ? nthr : 256) : 2 * nthr;
+}
 
 __device__ __forceinline__ ConeFwdRec cone_fwd_record(const Geo &g, float ang, float z_off,
                                                       const ConeCenter &cc, int row) {
