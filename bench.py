@@ -485,6 +485,7 @@ def main():
     import torch.distributed as dist
     import mbirtorch_b200 as mb
     from mbirtorch_b200 import _lib
+    from mbirtorch_b200.replicas import max_over_ranks, replica_rate
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -530,13 +531,9 @@ def main():
         t1.record()
         barrier()
     launches = _lib.launch_count() - launches0
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(t0.elapsed_time(t1), dev)
     ms_per_step = ms / args.steps
-    value = world * args.steps / (ms / 1e3)
+    value = replica_rate(args.steps, ms / 1e3, world)
     clocks = clk.summary()
     rec_ref = rec.detach().clone()
 
@@ -552,13 +549,9 @@ def main():
                             logfile_path=None, print_logs=False)
     e1.record()
     barrier()
-    ms_e2e = e0.elapsed_time(e1)
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dev)
     wall_e2e = time.perf_counter() - t0e
-    if world > 1:
-        tt = torch.tensor([ms_e2e], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_e2e = float(tt.item())
-    e2e = {"value": world * args.steps / (ms_e2e / 1e3), "unit": "recons/s",
+    e2e = {"value": replica_rate(args.steps, ms_e2e / 1e3, world), "unit": "recons/s",
            "h2d_bytes_per_step": int(y_host.nbytes), "d2h_bytes_per_step": int(rec_np.nbytes),
            "wall_s": wall_e2e}
 
@@ -575,7 +568,9 @@ def main():
            "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks}
 
     if rank == 0 and not args.no_extras:
-        out.update(extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd))
+        # N > 1: the roofline and kernel shares only (the CPU baseline and the
+        # other extras are single-GPU measurements, taken at N = 1)
+        out.update(extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd, full=world == 1))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -583,7 +578,7 @@ def main():
         print(json.dumps(out), flush=True)
 
 
-def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd):
+def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd, full=True):
     from mbirtorch_b200 import _lib
     res = {}
     # ── per-kernel timing over one timed recon -> roofline of the top kernel
@@ -630,6 +625,8 @@ def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd):
                            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
     res["kernel_time_share"] = {k: {"ms": v[0], "launches": v[1], "share": v[0] / total}
                                 for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
+    if not full:
+        return res
     # ── projector throughput (full volume, f32, device-resident) ──
     idx = m.full_indices_device()
     vals = torch.rand(idx.shape[0], NVOX, device=dev)
