@@ -473,3 +473,50 @@ def test_parallel_subset_step_binned_view_chunks_positivity(rows):
         e_new = err.cpu().numpy().astype(np.float64)
         gap = np.linalg.norm(e16.to_vrc().cpu().numpy() - e_new) / np.linalg.norm(e0)
         assert gap <= 3 * q0
+
+
+def test_curved_cone_partition_pass_weighted_positivity():
+    """A curved-detector cone partition pass (the geometry of the large
+    mixed-precision configuration), weighted, with positivity and DC
+    damping, against the FP64 oracle applying the same subsets in the same
+    order."""
+    from oracle import vcd as ovcd
+    from mbirtorch_b200.vcd_engine import ResidentSinogram
+    from mbirtorch_b200 import _lib
+    V, R, C = 30, 12, 40
+    m = mb.ConeBeamModel((V, R, C), np.linspace(0, 2 * np.pi, V, endpoint=False), 256.0, 128.0,
+                         use_curved_detector=True)
+    m.set_params(no_warning=True, verbose=0, delta_det_channel=2.0, delta_det_row=2.0,
+                 positivity_flag=True)
+    m.auto_set_recon_geometry(no_warning=True)
+    rs = m.get_params('recon_shape')
+    rng = np.random.default_rng(29)
+    x_true = rng.random(rs).astype(np.float32)
+    sino = m.forward_project(x_true)
+    w = (0.5 + rng.random(sino.shape)).astype(np.float32)
+    m.auto_set_regularization_params(sino, weights=w)
+    x0 = (0.05 * rng.standard_normal(rs)).astype(np.float32)
+    e0 = sino - m.forward_project(x0)
+    H = m.compute_hessian_diagonal(weights=w)
+    w_res = ResidentSinogram.from_vrc(torch.as_tensor(w, device='cuda'), _lib.MBIR_F32)
+    upd = m.create_vcd_subset_updater(H, weights=w_res)
+    np.random.seed(6)
+    part = mb.gen_pixel_partition(rs, 8)
+    order = np.random.permutation(8).astype(np.int32)
+    flat = torch.as_tensor(x0.reshape(-1, rs[2]), device='cuda').clone()
+    err = ResidentSinogram.from_vrc(torch.as_tensor(e0, device='cuda'), _lib.MBIR_F32)
+    acc = torch.zeros(2 + rs[2], dtype=torch.float64, device='cuda')
+    upd.engine.partition_pass(flat, err, torch.as_tensor(part, device='cuda'), order, acc)
+    prob = _oracle_problem(m)
+    sy, sx = m.get_params(['sigma_y', 'sigma_x'])
+    ou = ovcd.SubsetUpdater(prob, H.reshape(-1, rs[2]), w, sy, sx, positivity=True,
+                            dc_profile=ovcd.dc_damping_profile(prob))
+    oflat = x0.reshape(-1, rs[2]).astype(np.float64)
+    oerr = e0.astype(np.float64)
+    alpha_sum = 0.0
+    for k in order:
+        _, oalpha, _ = ou(oflat, oerr, part[k].astype(np.int64))
+        alpha_sum += oalpha
+    assert abs(float(acc[1]) - alpha_sum) / alpha_sum <= 1e-4
+    assert rel_l2(flat.cpu().numpy(), oflat) <= 2e-5
+    assert rel_l2(err.to_vrc().cpu().numpy(), oerr) <= 2e-5
