@@ -441,8 +441,10 @@ back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, 
       const float hi = fminf(ceilf(fmaxf(ma, mb)) + (float)(RT + 1), (float)(g.R - 1));
       if (lo <= hi) {
         // Column rows in batches of HB per lane, every load of a batch in
-        // flight before the first use.
-        constexpr int HB = NT == 3 ? 8 : 2;
+        // flight before the first use.  A short band (SPL <= 2, at most 64
+        // slices) spans about 64 w_r rows, so its batches are 4 rows deep:
+        // fewer predicated-off loads than 8.
+        constexpr int HB = NT == 3 ? (SPL <= 2 ? 4 : 8) : 2;
         const int m_lo = (int)lo, m_hi = (int)hi;
         for (int mb = m_lo + lane; mb <= m_hi; mb += 32 * HB) {
           float col[HB][MT];
