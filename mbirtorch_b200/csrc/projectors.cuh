@@ -345,6 +345,35 @@ __device__ __forceinline__ void back_cone_slices(float (&acc)[SPL], const float 
   }
 }
 
+// HB rows mb, mb + 32, ... of a view's detector column into h: the MT
+// channel taps weighted and summed, times the view's scale.  Every load of
+// the batch is in flight before the first use.  CHECK: rows past m_hi are
+// skipped (the batch's last rows may not exist).
+template <int HB, int MT, int NT, bool CHECK, typename RD>
+__device__ __forceinline__ void column_batch(const RD &rd, const size_t (&base)[MT],
+                                             const float (&w)[MT], float scl, int mb, int m_hi,
+                                             float *__restrict__ h, int nt) {
+  float col[HB][MT];
+#pragma unroll
+  for (int u = 0; u < HB; ++u) {
+    const int m = mb + 32 * u;
+#pragma unroll
+    for (int t = 0; t < MT; ++t)
+      col[u][t] = (MBIR_TAP_ON(NT, t, nt) && (!CHECK || m <= m_hi)) ? rd.get(base[t] + m) : 0.f;
+  }
+#pragma unroll
+  for (int u = 0; u < HB; ++u) {
+    const int m = mb + 32 * u;
+    if (!CHECK || m <= m_hi) {
+      float s = 0.f;
+#pragma unroll
+      for (int t = 0; t < MT; ++t)
+        if (MBIR_TAP_ON(NT, t, nt)) s = fmaf(w[t], col[u][t], s);
+      h[m] = __fmul_rn(s, scl);
+    }
+  }
+}
+
 // One warp per (pixel, chunk of 32*SPL slices).  Dynamic shared memory:
 // 8 warps x (R + 2 kPad) floats of column buffer, then 8 x 32 ConeRec.
 template <int CP, int SPL, int NT, typename RD>
@@ -446,24 +475,36 @@ back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, 
         // fewer predicated-off loads than 8.
         constexpr int HB = NT == 3 ? (SPL <= 2 ? 4 : 8) : 2;
         const int m_lo = (int)lo, m_hi = (int)hi;
-        for (int mb = m_lo + lane; mb <= m_hi; mb += 32 * HB) {
-          float col[HB][MT];
+        if constexpr (SPL <= 2) {
+          // Short bands: whole batches (every lane's HB rows exist, no row
+          // test), then the remaining rows in batches of 2.  (For longer
+          // bands the split costs registers and occupancy: the plain loop
+          // below is faster there.)
+          int g0 = m_lo;
+          for (; g0 + 32 * HB - 1 <= m_hi; g0 += 32 * HB)
+            column_batch<HB, MT, NT, false>(rd, base, w, scl, g0 + lane, m_hi, h, nt);
+          for (; g0 <= m_hi; g0 += 32 * 2)
+            column_batch<2, MT, NT, true>(rd, base, w, scl, g0 + lane, m_hi, h, nt);
+        } else {
+          for (int mb = m_lo + lane; mb <= m_hi; mb += 32 * HB) {
+            float col[HB][MT];
 #pragma unroll
-          for (int u = 0; u < HB; ++u) {
-            const int m = mb + 32 * u;
-#pragma unroll
-            for (int t = 0; t < MT; ++t)
-              col[u][t] = (MBIR_TAP_ON(NT, t, nt) && m <= m_hi) ? rd.get(base[t] + m) : 0.f;
-          }
-#pragma unroll
-          for (int u = 0; u < HB; ++u) {
-            const int m = mb + 32 * u;
-            if (m <= m_hi) {
-              float s = 0.f;
+            for (int u = 0; u < HB; ++u) {
+              const int m = mb + 32 * u;
 #pragma unroll
               for (int t = 0; t < MT; ++t)
-                if (MBIR_TAP_ON(NT, t, nt)) s = fmaf(w[t], col[u][t], s);
-              h[m] = __fmul_rn(s, scl);
+                col[u][t] = (MBIR_TAP_ON(NT, t, nt) && m <= m_hi) ? rd.get(base[t] + m) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < HB; ++u) {
+              const int m = mb + 32 * u;
+              if (m <= m_hi) {
+                float s = 0.f;
+#pragma unroll
+                for (int t = 0; t < MT; ++t)
+                  if (MBIR_TAP_ON(NT, t, nt)) s = fmaf(w[t], col[u][t], s);
+                h[m] = __fmul_rn(s, scl);
+              }
             }
           }
         }
