@@ -225,12 +225,15 @@ int launch_back_t(const Geo &geo, const mbir_geometry *g, const float *vp, int v
     tpre(st);
     launch(k, grid, kThreads, s.smem, st, geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P,
            slice_start, band, s.slice_chunks, dst, recs);
-  } else if (NT == 3 && SPL == 4 && s.T == 32 && band % 4 == 0 && rd.aligned16() &&
-             is_aligned16(dst)) {
+  } else if (NT == 3 && SPL == 4 && band % 4 == 0 && rd.aligned16() && is_aligned16(dst)) {
     // four consecutive slices per lane: the same teams, one 16-byte load per tap
+    auto k4 = s.T == 32 ? back_parallel4_kernel<CP, 32, RD>
+            : s.T == 16 ? back_parallel4_kernel<CP, 16, RD>
+            : s.T == 8  ? back_parallel4_kernel<CP, 8, RD>
+                        : back_parallel4_kernel<CP, 4, RD>;
     tpre(st);
-    launch(back_parallel4_kernel<CP, RD>, grid, kThreads, 0, st, geo, vp, v_start, v_count,
-           s.vpc, rd, pix, (int)P, band, s.slice_chunks, dst);
+    launch(k4, grid, kThreads, 0, st, geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P, band,
+           s.slice_chunks, dst);
   } else {
     tpre(st);
     launch(back_parallel_kernel<CP, SPL, NT, RD>, grid, kThreads, 0, st, geo, vp, v_start,

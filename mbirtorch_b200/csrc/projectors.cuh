@@ -220,19 +220,19 @@ back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_cou
 }
 
 // The parallel back projector at psf radius 1 with four consecutive slices
-// per lane (a team of 32 lanes covers 128 slices, as T = 32, SPL = 4 does):
+// per lane (a team of T lanes covers 4 T slices, as SPL = 4 does):
 // each tap of a view is one 16-byte load per lane, and two views' taps are
 // in flight before either is accumulated.  Each output is the same sequence
 // of FMAs as in back_parallel_kernel.  Needs band a multiple of 4 and the
 // operands 16-byte aligned (checked on the host).
-template <int CP, typename RD>
+template <int CP, int T, typename RD>
 __global__ void __launch_bounds__(kThreads)
 back_parallel4_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
                       RD rd, const int64_t *__restrict__ pix, int P, int band, int slice_chunks,
                       float *__restrict__ out) {
   MBIR_PDL_ENTRY();
   __shared__ ParRec tab[kThreads];
-  constexpr int T = 32, MT = 3;
+  constexpr int MT = 3;
   const int tid = threadIdx.x;
   const int team = tid / T, tl = tid - team * T;
   const int teams_per_block = kThreads / T;

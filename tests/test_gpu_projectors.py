@@ -162,6 +162,29 @@ def test_medium_parallel_vs_oracle_with_view_tail():
         assert rel_l2(b, oracle.parallel_back(g, vp, y, sub, 2)) <= TOL, n
 
 
+@pytest.mark.parametrize("rows", [16, 32, 64, 128])
+def test_parallel_back_four_slices_per_lane_team_widths(rows):
+    """Rows a multiple of 4 take the back projector with four consecutive
+    slices per lane, in teams of 4, 8, 16 and 32 lanes (16, 32, 64 and 128
+    rows): full and subset back projections, coefficient power 1 and 2,
+    against the FP64 oracle."""
+    import oracle
+    m = mb.ParallelBeamModel((37, rows, 48), np.linspace(0, np.pi, 37, endpoint=False))
+    m.set_params(no_warning=True, verbose=0)
+    rs = m.get_params('recon_shape')
+    rng = np.random.default_rng(rows)
+    idx = mb.gen_full_indices(rs).astype(np.int64)
+    y = rng.standard_normal(m.get_params('sinogram_shape')).astype(np.float32)
+    g = _oracle_geom(m)
+    vp = m._view_params_array().astype(np.float64)
+    for cp in (1, 2):
+        b = m.sparse_back_project(_t(y), _t(idx, torch.int64), coeff_power=cp).cpu().numpy()
+        assert rel_l2(b, oracle.parallel_back(g, vp, y, idx, cp)) <= TOL, cp
+    sub = np.sort(rng.choice(idx, size=33, replace=False))
+    b = m.sparse_back_project(_t(y), _t(sub, torch.int64)).cpu().numpy()
+    assert rel_l2(b, oracle.parallel_back(g, vp, y, sub, 1)) <= TOL
+
+
 def test_cone_slice_band_and_layouts():
     """Banded cone calls sum to the unbanded projection; VCR == VRC^T."""
     m = _cone_model(views=30, rows=24, chans=32)
