@@ -32,6 +32,17 @@ from .vcd_engine import make_vcd_params, storage_code
 from .vcd_run import VcdRun
 
 
+_STREAMS = {}
+
+
+def _free_streams(device):
+    """The process-wide free list of server streams on ``device``."""
+    key = torch.device(device).index
+    if key is None:
+        key = torch.cuda.current_device()
+    return _STREAMS.setdefault(key, [])
+
+
 class MemoryLedger:
     """Admission by device bytes: ``fits`` / ``take`` / ``release``."""
 
@@ -140,10 +151,12 @@ class ReconServer:
         self._next_id = 0
         self.max_concurrent = 0
         self.deferred = 0   # admissions put off because the ledger was full
-        # Streams are reused from job to job: the caching allocator keeps its
-        # freed blocks per stream, so a fresh stream per job would grow the
-        # pool (synchronizing cudaMalloc calls) instead of reusing it.
-        self._streams = []
+        # Streams are reused from job to job, and from server to server in
+        # one process: the caching allocator keeps its freed blocks per
+        # stream, so fresh streams would grow the pool (cudaMalloc calls)
+        # instead of reusing it.  A stream is out of the shared free list
+        # while a job holds it.
+        self._streams = _free_streams(self.device)
         self.t0 = None
 
     # ── requests ───────────────────────────────────────────────────────────
