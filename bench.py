@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the projector, mixed-precision and CPU-baseline extras")
     ap.add_argument("--profile-case", choices=["recon", "subset", "projectors",
-                                               "subset-parallel"], default=None,
+                                               "subset-parallel", "subset-cone64"], default=None,
                     help="run one untimed pass of the workload for an external profiler "
                          "and exit (no JSON line)")
     return ap.parse_args()
@@ -264,6 +264,44 @@ def parallel_pass_setup(mb, torch):
     order = rng.permutation(part.shape[0]).astype(np.int32)
     acc = torch.zeros(2 + rs[2], dtype=torch.float64, device=dev)
     return m, upd, flat, err, part, order, acc
+
+
+def cone64_pass(mb, torch):
+    """One 128-subset partition pass of the serving mix's largest cone jobs
+    (256^2 x 64 volume, 360 views, 64 x 384 flat detector of pitch 2, SID
+    512, SDD 1024; FP32 storage on a seeded stand-in error sinogram), then
+    a second pass with per-launch CUDA events, whose per-kernel averages
+    are printed (one line each)."""
+    from mbirtorch_b200 import _lib
+    from mbirtorch_b200.vcd_engine import ResidentSinogram
+    dev = torch.device("cuda", 0)
+    Vc, Sc, Cc, Nc = 360, 64, 384, 256
+    m = mb.ConeBeamModel((Vc, Sc, Cc), np.linspace(0, 2 * np.pi, Vc, endpoint=False),
+                         source_detector_dist=4.0 * Nc, source_iso_dist=2.0 * Nc)
+    m.set_params(no_warning=True, delta_det_channel=2.0, delta_det_row=2.0)
+    m.auto_set_recon_geometry(no_warning=True)
+    m.set_params(no_warning=True, verbose=0, recon_shape=(Nc, Nc, Sc))
+    y = torch.rand((Vc, Sc, Cc), generator=torch.Generator(device=dev).manual_seed(1),
+                   device=dev)
+    m.auto_set_regularization_params(y)
+    H = m.compute_hessian_diagonal(output_sharded=True)
+    upd = m.create_vcd_subset_updater(H, weights=1)
+    rs = m.get_params("recon_shape")
+    flat = torch.zeros(rs[0] * rs[1], rs[2], device=dev)
+    err = ResidentSinogram.from_vrc(y, _lib.MBIR_F32)
+    rng = np.random.RandomState(0)
+    part = torch.as_tensor(mb.gen_pixel_partition(rs, 128, rng=rng), device=dev)
+    order = rng.permutation(part.shape[0]).astype(np.int32)
+    acc = torch.zeros(2 + rs[2], dtype=torch.float64, device=dev)
+    upd.engine.partition_pass(flat, err, part, order, acc)
+    torch.cuda.synchronize()
+    _lib.timing_collect()
+    _lib.timing_enable(True)
+    upd.engine.partition_pass(flat, err, part, order, acc)
+    torch.cuda.synchronize()
+    _lib.timing_enable(False)
+    for k, v in sorted(_lib.timing_collect().items(), key=lambda kv: -kv[1][0]):
+        print(f"{k}: {1e3 * v[0] / v[1]:.1f} us x {v[1]}")
 
 
 def parallel_subset_extra(mb, torch, hbm):
@@ -498,6 +536,9 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    if args.profile_case == "subset-cone64":
+        cone64_pass(mb, torch)
+        return
     if args.profile_case == "subset-parallel":
         # one 128-subset partition pass of the parallel 512^2 x 256 workload
         _, upd, flat, err, part, order, acc = parallel_pass_setup(mb, torch)
