@@ -643,9 +643,9 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
            g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H, sc, nullptr, w.gbuf, w.hinv,
            w.gpbuf, w.hpbuf, nullptr);
     MBIR_CHECK_LAUNCH("vcd direction (damped)");
-    dim3 gs((S + 127) / 128, w.dc_chunks);
+    dim3 gs((S + 31) / 32, w.dc_chunks);
     tpre(st);
-    launch(vcd_dc_sums_kernel, gs, 128, 0, st, (int)Ps, S, kDcChunk, w.gbuf, w.hinv, w.dc_sums);
+    launch(vcd_dc_sums_kernel, gs, dim3(32, kDcGroups), 0, st, (int)Ps, S, kDcChunk, w.gbuf, w.hinv, w.dc_sums);
     MBIR_CHECK_LAUNCH("vcd DC sums");
     tpre(st);
     launch(vcd_dc_direction_kernel, nb, kThreads, 0, st, (int)Ps, S, w.dc_chunks, w.dc_sums, dc,

@@ -184,23 +184,52 @@ vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int 
 
 // ── 2'. DC damping ───────────────────────────────────────────────────────
 // Per-slice sums over pixel chunks: part[chunk][l] = (sum h^-1 g, sum h^-1).
-__global__ void vcd_dc_sums_kernel(int P, int S, int pchunk, const float *__restrict__ gbuf,
-                                   const float *__restrict__ hinv, double *__restrict__ part) {
+// A CTA of (32 slices, 8 groups) covers one chunk of pchunk <= 32 pixels:
+// group y sums the pixels y, y + 8, ... of the chunk with all its loads in
+// flight, then the 8 group sums fold in a fixed order.
+constexpr int kDcGroups = 8;
+
+__global__ void __launch_bounds__(32 * kDcGroups)
+vcd_dc_sums_kernel(int P, int S, int pchunk, const float *__restrict__ gbuf,
+                   const float *__restrict__ hinv, double *__restrict__ part) {
   MBIR_PDL_ENTRY();
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ double s_num[kDcGroups][32], s_den[kDcGroups][32];
+  constexpr int U = 32 / kDcGroups;  // pixels per group (pchunk <= 32)
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int l = blockIdx.x * 32 + tx;
   const int chunk = blockIdx.y;
-  if (l >= S) return;
   const int p0 = chunk * pchunk, p1 = min(P, p0 + pchunk);
   double num = 0.0, den = 0.0;
-#pragma unroll 8
-  for (int p = p0; p < p1; ++p) {
-    const size_t i = (size_t)p * S + l;
-    const float hi = hinv[i];
-    num += (double)__fmul_rn(hi, gbuf[i]);
-    den += (double)hi;
+  if (l < S) {
+    float hv[U], gv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int p = p0 + ty + kDcGroups * u;
+      const size_t i = (size_t)p * S + l;
+      hv[u] = p < p1 ? hinv[i] : 0.f;
+      gv[u] = p < p1 ? gbuf[i] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (p0 + ty + kDcGroups * u < p1) {
+        num += (double)__fmul_rn(hv[u], gv[u]);
+        den += (double)hv[u];
+      }
+    }
   }
-  part[((size_t)chunk * S + l) * 2] = num;
-  part[((size_t)chunk * S + l) * 2 + 1] = den;
+  s_num[ty][tx] = num;
+  s_den[ty][tx] = den;
+  __syncthreads();
+  if (ty == 0 && l < S) {
+    double a = 0.0, b = 0.0;
+#pragma unroll
+    for (int k = 0; k < kDcGroups; ++k) {
+      a += s_num[k][tx];
+      b += s_den[k][tx];
+    }
+    part[((size_t)chunk * S + l) * 2] = a;
+    part[((size_t)chunk * S + l) * 2 + 1] = b;
+  }
 }
 
 // delta = -(g - (1 - s_l) * gbar_l) * h^-1, plus the prior line-term partials.
