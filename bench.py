@@ -1,29 +1,36 @@
-"""Benchmark: plain cone-beam MBIR on B200 (one JSON line on stdout).
+"""Benchmark: cone-beam MBIR on B200 (one JSON line on stdout).
 
-Workload (the reference's cone-beam configuration): a 256 x 256 x 256 volume
-of 10 seeded ellipsoids, 360 views on [0, 2 pi), a flat 256 x 384 detector
-with 2-unit pixels, source-to-iso 1024, source-to-detector 2048
+Headline workload, the largest single-GPU configuration: a 512 x 512 x 256
+volume of 10 seeded ellipsoids, 720 views on [0, 2 pi), a curved 320 x 768
+detector with 2-unit pixels, source-to-iso 1024, source-to-detector 2048
 (magnification 2), Poisson counts at I0 = 1e4 converted back to line
-integrals, qGGMRF prior (p = 2, q = 1.2), 20 VCD iterations.  One STEP is
-one complete reconstruction (direct-recon init, Hessian, 20 iterations).
+integrals, qGGMRF prior (p = 2, q = 1.2), 20 VCD iterations, FP32 storage.
+One STEP is one complete reconstruction (direct-recon init, Hessian, 20
+iterations).
 
   value      recons/s with the sinogram resident in HBM before the timed
              region (model.recon on a CUDA tensor)
-  e2e        recons/s through the public API with host numpy in and out
-             (sinogram host->device and recon device->host inside)
-  roofline   the dominant kernel's algorithmic bytes / CUDA-event duration
-             against the measured HBM copy bandwidth
-  cpu_baseline  the FP64 C oracle (all host threads) on a bounded sample:
-             one 128-subset VCD step, extrapolated to a whole recon
+  e2e        recons/s through the public API from a pinned host sinogram to a
+             host volume (copies inside the timed region)
+  roofline   the dominant kernel's algorithmic bytes (one read of each error-
+             sinogram cell its subset reaches, counted on the device) over its
+             CUDA-event duration, against the measured HBM copy bandwidth
+  cpu_baseline  the FP64 C oracle (the reference's algorithm restated, all
+             host threads) on one 128-subset VCD step of this workload,
+             extrapolated to a whole recon, with the GPU step's parity
+             against it; the reference's own eager CPU code (mbirtorch 0.0.2,
+             installed under baseline/_ref) timed whole on its small CPU
+             configuration beside it
 
---impl reference times that CPU implementation alone (the reference's
-algorithm restated; the reference itself is Python and is not shipped).
+--impl reference times the reference's own CPU code on this workload (rank 0;
+other ranks exit): each step one warm 128-subset step over 90 of the 720
+views, scaled to the whole scan by a measured full-scan step and to a whole
+recon.
 Multi-GPU: independent replicas, one per rank (no data exchange).
 """
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -34,106 +41,115 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
 
-V, R, C = 360, 256, 384
-NVOX = 256
 SDD, SID = 2048.0, 1024.0
 ITERS = 20
 I0 = 1e4
-METRIC = "recons/s (cone-beam MBIR 256^3, 360 views, 20 VCD iterations)"
-WORKLOAD = ("cone flat 256x256x256 volume, 360 views on [0, 2pi), 256x384 detector "
-            "(pitch 2), SID 1024, SDD 2048, Poisson I0=1e4, qGGMRF p=2 q=1.2, 20 VCD iterations")
+# name: (views, detector rows, channels, in-plane N, slices, curved)
+CONFIGS = {
+    "cone512_curved": (720, 320, 768, 512, 256, True),
+    "cone256_flat": (360, 256, 384, 256, 256, False),
+}
+HEAD = "cone512_curved"
+METRIC = "recons/s (cone-beam MBIR 512^2 x 256, 720 views, curved 320 x 768, 20 VCD iterations)"
+
+
+def workload(name, iters=ITERS, storage="float32"):
+    V, R, C, N, S, curved = CONFIGS[name]
+    return (f"cone {'curved' if curved else 'flat'} {N}x{N}x{S} volume, {V} views on "
+            f"[0, 2pi), {R}x{C} detector (pitch 2), SID 1024, SDD 2048, Poisson I0=1e4, "
+            f"qGGMRF p=2 q=1.2, {iters} VCD iterations, {storage} storage")
+
+
+def config_block(storage="float32", world=1):
+    V, R, C, N, S, curved = CONFIGS[HEAD]
+    sino_mb = V * R * C * 4 / 1e6
+    return {"workload": workload(HEAD, storage=storage), "volume": [N, N, S], "views": V,
+            "detector_rows_channels": [R, C], "curved_detector": curved,
+            "iterations": ITERS, "storage": storage, "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2 ({sino_mb:.0f} MB f32 sinogram vs 126 MB L2)"}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mbir", choices=["mbir", "reference"])
     ap.add_argument("--storage", default="float32")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the projector, mixed-precision and CPU-baseline extras")
+                    help="skip every extra measurement (headline value and e2e only)")
+    ap.add_argument("--only-extra", default=None,
+                    help="run one extra by name after the headline (e.g. triton_reference)")
     ap.add_argument("--profile-case", choices=["recon", "subset", "projectors",
-                                               "subset-parallel", "subset-cone64"], default=None,
+                                               "subset-parallel", "subset-cone64",
+                                               "subset-small"], default=None,
                     help="run one untimed pass of the workload for an external profiler "
                          "and exit (no JSON line)")
     return ap.parse_args()
 
 
-def profile_case(case, m, mb, torch, y):
-    """One pass for a profiler: 'recon' is one whole reconstruction;
-    'subset' is three VCD subset steps of a 128-subset partition (the subset
-    size of 17 of the 20 iterations) from a zero volume; 'projectors' is one
-    full-volume forward and one back projection.  ('subset-parallel', one
-    partition pass of the parallel workload, is dispatched in main.)"""
-    if case == "recon":
-        np.random.seed(0)
-        m.recon(y, max_iterations=ITERS, stop_threshold_change_pct=0, logfile_path=None,
-                print_logs=False, output_sharded=True)
-    elif case == "subset":
-        from mbirtorch_b200.vcd_engine import ResidentSinogram, storage_code
-        m.auto_set_regularization_params(y)
-        H = m.compute_hessian_diagonal(output_sharded=True)
-        upd = m.create_vcd_subset_updater(H, weights=1)
-        rs = m.get_params('recon_shape')
-        flat = torch.zeros(rs[0] * rs[1], rs[2], device=y.device)
-        err = ResidentSinogram.from_vrc(y, storage_code(m.storage_dtype))
-        np.random.seed(0)
-        parts = torch.as_tensor(mb.gen_pixel_partition(rs, 128), device=y.device)
-        for i in range(3):
-            upd.engine.subset_update(flat, err, parts[i])
-    else:
-        idx = m.full_indices_device()
-        vals = torch.rand(idx.shape[0], NVOX, device=y.device)
-        s = m.projector.forward(vals, idx)
-        m.projector.back(s, idx)
-    torch.cuda.synchronize()
-
-
 # ── synthetic data ──────────────────────────────────────────────────────────
-def phantom(seed=0):
-    """10 seeded ellipsoids on [-1, 1]^3 grids (centres U[-0.5, 0.5],
-    semi-axes U[0.05, 0.4], in-plane angle U[0, 180) deg, density U[0.1, 1])."""
+def phantom_torch(torch, shape, seed, dev):
+    """10 seeded ellipsoids on [-1, 1]^3 grids, built on the device: centres
+    U[-0.5, 0.5], semi-axes U[0.05, 0.4], in-plane angle U[0, 180) deg,
+    density U[0.1, 1]."""
     rng = np.random.default_rng(seed)
-    g = np.linspace(-1, 1, NVOX, dtype=np.float32)
-    X, Y = np.meshgrid(g, g)
-    vol = np.zeros((NVOX, NVOX, NVOX), np.float32)
+    nr, nc, ns = shape
+    g1 = torch.linspace(-1, 1, nr, device=dev)
+    g0 = torch.linspace(-1, 1, nc, device=dev)
+    gz = torch.linspace(-1, 1, ns, device=dev)
+    Y, X = torch.meshgrid(g1, g0, indexing="ij")
+    vol = torch.zeros(shape, device=dev)
     for _ in range(10):
         c = rng.uniform(-0.5, 0.5, 3)
         a = rng.uniform(0.05, 0.4, 3)
         ang = np.deg2rad(rng.uniform(0, 180))
-        dens = np.float32(rng.uniform(0.1, 1.0))
-        ca, sa = np.cos(ang), np.sin(ang)
+        dens = float(rng.uniform(0.1, 1.0))
+        ca, sa = float(np.cos(ang)), float(np.sin(ang))
         xr = ca * (X - c[0]) + sa * (Y - c[1])
         yr = -sa * (X - c[0]) + ca * (Y - c[1])
         xy = (xr / a[0]) ** 2 + (yr / a[1]) ** 2
-        z = ((g - c[2]) / a[2]) ** 2
-        inside = (xy[:, :, None] + z[None, None, :]) <= 1
-        vol += dens * inside.astype(np.float32)
+        z = ((gz - c[2]) / a[2]) ** 2
+        vol += dens * ((xy[:, :, None] + z[None, None, :]) <= 1).float()
     return vol
 
 
-def make_model(mb):
+def cone_model(pkg, name, views=None, **ctor):
+    """The configuration's ConeBeamModel in package ``pkg`` (this one or the
+    reference); ``views`` keeps every k-th view of the scan."""
+    V, R, C, N, S, curved = CONFIGS[name]
     ang = np.linspace(0, 2 * np.pi, V, endpoint=False)
-    m = mb.ConeBeamModel((V, R, C), ang, source_detector_dist=SDD, source_iso_dist=SID)
+    if views is not None:
+        ang = ang[views]
+    m = pkg.ConeBeamModel((len(ang), R, C), ang, source_detector_dist=SDD, source_iso_dist=SID,
+                          use_curved_detector=curved, **ctor)
     m.set_params(no_warning=True, verbose=0, delta_det_channel=2.0, delta_det_row=2.0)
     m.auto_set_recon_geometry(no_warning=True)
-    m.set_params(no_warning=True, recon_shape=(NVOX, NVOX, NVOX))
+    m.set_params(no_warning=True, recon_shape=(N, N, S))
     return m
 
 
-def make_data(mb, m, torch, dev):
-    """Noisy line integrals: the phantom is scaled so that the largest line
-    integral is 3 (transmission >= 5%), counts ~ Poisson(I0 exp(-Ax)),
-    y = -log(max(counts, 1) / I0), returned in phantom units."""
-    vol = phantom()
+def make_data(m, torch, dev, seed):
+    """Noisy line integrals on the device: the phantom is scaled so that the
+    largest line integral is 3 (transmission >= 5%), counts ~ Poisson(I0
+    exp(-Ax)), y = -log(max(counts, 1) / I0), returned in phantom units."""
+    vol = phantom_torch(torch, tuple(m.get_params('recon_shape')), seed, dev)
     clean = m.forward_project(vol, output_sharded=True)
+    del vol
     mu = 3.0 / float(clean.max())
-    gen = torch.Generator(device=dev).manual_seed(1)
+    gen = torch.Generator(device=dev).manual_seed(seed)
     counts = torch.poisson(I0 * torch.exp(-mu * clean), generator=gen)
-    y = (-torch.log(torch.clamp(counts, min=1.0) / I0) / mu).to(torch.float32)
-    return vol, y.contiguous()
+    del clean
+    y = (-torch.log(torch.clamp(counts, min=1.0) / I0) / mu).to(torch.float32).contiguous()
+    return y
+
+
+def recon(m, sino, iters=ITERS, seed=0, **kw):
+    np.random.seed(seed)
+    return m.recon(sino, max_iterations=iters, stop_threshold_change_pct=0, logfile_path=None,
+                   print_logs=False, **kw)
 
 
 # ── clocks ──────────────────────────────────────────────────────────────────
@@ -189,56 +205,380 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-# ── CPU baseline: the FP64 C oracle on one 128-subset VCD step ─────────────
-def cpu_baseline(m, y_host, reg, mb):
-    import oracle
-    from oracle import OracleGeometry
-    from oracle import vcd as ovcd
-    g = m._geometry()
-    og = OracleGeometry(num_det_rows=R, num_det_channels=C, num_recon_rows=NVOX,
-                        num_recon_cols=NVOX, num_slices=NVOX, delta_det_channel=2.0,
-                        delta_det_row=2.0, delta_voxel=1.0, delta_voxel_row=1.0,
-                        delta_voxel_slice=1.0, magnification=g.magnification,
-                        source_detector_dist=SDD, psf_radius=g.psf_radius,
-                        bp_psf_radius=g.bp_psf_radius)
-    oracle.build()
-    prob = ovcd.Problem('cone', og, m._view_params_array(), (NVOX, NVOX, NVOX),
-                        source_iso_dist=SID)
-    rs = (NVOX, NVOX, NVOX)
-    rng = np.random.default_rng(0)
-    part = mb.gen_pixel_partition(rs, 128)
-    idx = part[0].astype(np.int64)
-    x0 = np.zeros((NVOX * NVOX, NVOX))
-    H = np.ones_like(x0)   # the Hessian scale does not change the step's cost
-    upd = ovcd.SubsetUpdater(prob, H, None, reg['sigma_y'], reg['sigma_x'],
-                             dc_profile=ovcd.dc_damping_profile(prob))
-    err = np.asarray(y_host, np.float64).copy()
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ── the reference's own CPU code (baseline/_ref) ───────────────────────────
+def import_reference():
+    """mbirtorch 0.0.2 from its install under baseline/_ref (None if absent)."""
+    if not os.path.isdir(os.path.join(REF_DIR, "mbirtorch")):
+        return None
+    if REF_DIR not in sys.path:
+        sys.path.insert(0, REF_DIR)
+    import mbirtorch
+    return mbirtorch
+
+
+# A 20-iteration recon in subset steps: 4 + 16 + 64 + 17 x 128 steps, plus
+# the direct recon, the initial error and the Hessian (about three full
+# projections = 1.5 x 128 subset steps' projector work).  The larger subsets
+# of the first three iterations are counted at the cost of a 128-subset step,
+# which under-counts their projector work (in the reference's favour).
+SUBSET_STEPS_PER_RECON = 4 + 16 + 64 + 17 * 128 + 1.5 * 128
+
+
+class ReferenceStep:
+    """One 128-subset VCD step of the reference's own eager CPU updater
+    (create_vcd_subset_updater, tomography_model.py:2434-2660) on a
+    configuration restricted to every ``view_stride``-th view, from a zero
+    volume and a seeded stand-in error sinogram (a step's cost does not
+    depend on the values; the state is updated in place call after call)."""
+
+    def __init__(self, ref, torch, name, view_stride, seed=0):
+        m = cone_model(ref, name, views=slice(None, None, view_stride), compile_mode='off')
+        m.configure_devices(devices=['cpu'])
+        m.set_params(no_warning=True, sigma_y=1.0, sigma_x=0.1)
+        rs = m.get_params('recon_shape')
+        self.views = int(m.get_params('sinogram_shape')[0])
+        V, R, C = m.get_params('sinogram_shape')
+        rng = np.random.default_rng(seed)
+        self.err = m._as_shards(torch.as_tensor(rng.random((V, R, C), dtype=np.float32)),
+                                m.sino_placement)
+        self.flat = m._as_shards(torch.zeros(rs[0] * rs[1], rs[2]), m.recon_placement)
+        H = m._as_shards(torch.ones(rs[0] * rs[1], rs[2]), m.recon_placement)
+        self.upd = m.create_vcd_subset_updater(H, weights=1)
+        np.random.seed(seed)
+        self.idx = torch.as_tensor(ref.gen_pixel_partition(rs, 128)[0], dtype=torch.int64)
+        self.pixels = int(self.idx.shape[0])
+
+    def seconds(self):
+        t = time.perf_counter()
+        self.upd(self.flat, self.err, self.idx)
+        return time.perf_counter() - t
+
+
+class ReferenceCpu:
+    """The reference's own CPU recon rate on the headline workload, from a
+    bounded sample.  Each sample times one warm 128-subset step over 90 of
+    the 720 views.  The ratio of a warm 720-view step to a warm 90-view step,
+    measured once at the first sample (the reference's cost is not linear in
+    the view count: its driver projects in view batches), scales a sample to
+    the whole scan, and SUBSET_STEPS_PER_RECON to a whole recon."""
+
+    def __init__(self, torch):
+        self.torch = torch
+        self.ref = import_reference()
+        torch.set_num_threads(os.cpu_count())
+        self.V = CONFIGS[HEAD][0]
+        self.s90 = None
+        self.t_full_cal = self.t90_cal = None
+
+    def available(self):
+        return self.ref is not None
+
+    def sample(self):
+        if self.s90 is None:
+            full = ReferenceStep(self.ref, self.torch, HEAD, 1)
+            full.seconds()                 # first call: allocator and thread-pool warm-up
+            self.t_full_cal = full.seconds()
+            del full
+            self.s90 = ReferenceStep(self.ref, self.torch, HEAD, 8)
+            self.s90.seconds()
+            self.t90_cal = self.s90.seconds()
+        t90 = self.s90.seconds()
+        ratio = self.t_full_cal / self.t90_cal
+        t_full = t90 * ratio
+        per_recon = t_full * SUBSET_STEPS_PER_RECON
+        return {"value": 1.0 / per_recon, "unit": "recons/s", "cores": os.cpu_count(),
+                "cpu_model": cpu_model(), "kind": "reference",
+                "sample": (f"mbirtorch 0.0.2's own eager CPU subset updater (torch "
+                           f"{self.torch.__version__}, {self.torch.get_num_threads()} threads) "
+                           f"on one warm 128-subset step of the headline workload "
+                           f"({self.s90.pixels} pixels x 256 slices) over {self.s90.views} "
+                           f"views ({t90:.2f} s), scaled by the measured ratio of a warm "
+                           f"{self.V}-view step ({self.t_full_cal:.1f} s) to a warm "
+                           f"{self.s90.views}-view step ({self.t90_cal:.2f} s) and multiplied by "
+                           f"{SUBSET_STEPS_PER_RECON:.0f} subset-step equivalents per recon"),
+                "seconds_per_recon_extrapolated": per_recon,
+                "subset_step_seconds": t_full,
+                "subset_step_seconds_full_scan_measured": self.t_full_cal}
+
+
+def reference_cpu_recon_cfg1(torch):
+    """The reference's own recon_simple_parallel on its CPU configuration
+    (128 x 128 x 16 phantom, 180 views, 16 x 192 detector, 10 iterations),
+    timed whole: no extrapolation."""
+    ref = import_reference()
+    if ref is None:
+        return {"value": None, "error": "reference not installed under baseline/_ref"}
+    torch.set_num_threads(os.cpu_count())
+    shape = (180, 16, 192)
+    ang = np.linspace(0, np.pi, shape[0], endpoint=False)
+    mp = ref.ParallelBeamModel(shape, ang, compile_mode='off')
+    mp.set_params(no_warning=True, verbose=0, recon_shape=(128, 128, 16))
+    mp.configure_devices(devices=['cpu'])
+    vol = phantom_torch(torch, (128, 128, 16), 61, torch.device('cpu')).numpy()
+    clean = mp.forward_project(vol)
+    rng = np.random.default_rng(62)
+    sino = (clean + rng.normal(0, 0.01 * clean.max(), clean.shape)).astype(np.float32)
+    m = ref.ParallelBeamModel(shape, ang, compile_mode='off')
+    m.configure_devices(devices=['cpu'])
+    m.set_params(no_warning=True, verbose=0)
+    np.random.seed(63)
     t = time.perf_counter()
-    upd(x0, err, idx)
+    m.recon(sino, max_iterations=10, stop_threshold_change_pct=0, logfile_path=None,
+            print_logs=False)
     dt = time.perf_counter() - t
-    # a whole recon: 4 + 16 + 64 + 17 * 128 subset steps of the same total
-    # pixel work, plus direct recon, initial error and Hessian (about three
-    # full projections, i.e. 3 x 128 subset-sized projector passes / 2)
-    n_sub_equiv = 3 * 128 + 17 * 128 + 3 * 128 / 2
-    per_recon = dt * n_sub_equiv
-    _ = rng
-    return {"value": 1.0 / per_recon, "unit": "recons/s", "cores": os.cpu_count(),
-            "kind": "port", "sample": f"one 128-subset VCD step ({idx.size} pixels x 256 slices "
-            f"x 360 views, {dt:.2f} s, FP64 C oracle with OpenMP) extrapolated to a full "
-            f"20-iteration recon ({n_sub_equiv:.0f} subset-step equivalents)",
+    return {"value": 1.0 / dt, "unit": "recons/s", "seconds": dt, "cores": os.cpu_count(),
+            "threads": torch.get_num_threads(), "cpu_model": cpu_model(), "kind": "reference",
+            "workload": "recon of a 128x128x16 ellipsoid phantom's parallel sinogram (180 "
+                        "views, 16 x 192, 1% Gaussian noise) at the default 192x192x16 grid, "
+                        "10 VCD iterations, eager torch on the CPU, timed whole",
+            "sino": sino}
+
+
+# ── the CPU-baseline leg: reference timing, FP64 oracle parity ─────────────
+def oracle_problem(m):
+    from oracle import OracleGeometry, vcd
+    g = m._geometry()
+    og = OracleGeometry(
+        num_det_rows=g.num_det_rows, num_det_channels=g.num_det_channels,
+        num_recon_rows=g.num_recon_rows, num_recon_cols=g.num_recon_cols,
+        num_slices=g.num_slices, delta_det_channel=g.delta_det_channel,
+        delta_det_row=g.delta_det_row, det_channel_offset=g.det_channel_offset,
+        det_row_offset=g.det_row_offset, delta_voxel=g.delta_voxel,
+        delta_voxel_row=g.delta_voxel_row, delta_voxel_slice=g.delta_voxel_slice,
+        recon_slice_offset=g.recon_slice_offset, magnification=g.magnification,
+        source_detector_dist=g.source_detector_dist,
+        use_curved_detector=bool(g.use_curved_detector), psf_radius=g.psf_radius,
+        bp_psf_radius=g.bp_psf_radius)
+    kind = 'cone' if g.geometry == 1 else 'parallel'
+    return vcd.Problem(kind, og, m._view_params_array(), m.get_params('recon_shape'),
+                       source_iso_dist=m.get_params('source_iso_dist') if kind == 'cone'
+                       else None)
+
+
+def subset_parity(m, mb, torch, y, x, seed=1):
+    """One GPU subset step from the state (x, e = y - A x) against the FP64
+    oracle's step from the same state (one subset of the 128-subset
+    partition).  Returns the relative errors and the oracle step's seconds.
+    The caller passes a state some way from convergence, so that the update
+    itself is large against the FP32 rounding of the volume."""
+    import oracle
+    from oracle import vcd as ovcd
+    oracle.build()
+    rs = m.get_params('recon_shape')
+    dev = y.device
+    e0 = (y - m.forward_project(x, output_sharded=True)).contiguous()
+    H = m.compute_hessian_diagonal(output_sharded=True)
+    upd = m.create_vcd_subset_updater(H, weights=1)
+    rng = np.random.RandomState(seed)
+    idx = mb.gen_pixel_partition(rs, 128, rng=rng)[rng.randint(128)].astype(np.int64)
+    flat = x.reshape(-1, rs[2]).clone()
+    err = e0.clone()
+    flat, err, ell1, alpha, _ = upd(flat, err, torch.as_tensor(idx, device=dev))
+    prob = oracle_problem(m)
+    sy, sx = m.get_params(['sigma_y', 'sigma_x'])
+    ou = ovcd.SubsetUpdater(prob, H.reshape(-1, rs[2]).cpu().numpy(), None, sy, sx,
+                            dc_profile=ovcd.dc_damping_profile(prob))
+    oflat = x.reshape(-1, rs[2]).cpu().numpy().astype(np.float64)
+    oerr = e0.cpu().numpy().astype(np.float64)
+    x_sub = oflat[idx].copy()
+    t = time.perf_counter()
+    _, oalpha, _ = ou(oflat, oerr, idx)
+    dt = time.perf_counter() - t
+    got = flat.cpu().numpy().astype(np.float64)
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    return {"state": "0.9 x the timed recon", "pixels": int(idx.size),
+            "alpha": float(alpha), "alpha_oracle": float(oalpha),
+            "alpha_rel": abs(float(alpha) - oalpha) / abs(oalpha),
+            "update_rel_l2": rel(got[idx] - x_sub, oflat[idx] - x_sub),
+            "recon_rel_l2": rel(got, oflat),
+            "error_sinogram_rel_l2": rel(err.cpu().numpy().astype(np.float64), oerr),
+            "oracle_step_s": dt, "oracle_threads": os.cpu_count()}
+
+
+def cpu_baseline_leg(m, mb, torch, y, rec):
+    """The CPU-baseline leg of the headline line: the FP64 oracle (the
+    reference's algorithm restated in C with OpenMP, all host threads) on one
+    128-subset step of the headline workload from the state the timed recon
+    ended in, extrapolated to a whole recon; the GPU step's parity against
+    that oracle step; and the reference's own eager CPU code timed whole on
+    its small CPU configuration.  (`bench.py --impl reference` times the
+    reference's own code on the headline workload.)"""
+    out = {}
+    try:
+        # 0.9 x the timed recon: a state with a sizeable update
+        par = subset_parity(m, mb, torch, y, 0.9 * rec)
+        per_recon = par["oracle_step_s"] * SUBSET_STEPS_PER_RECON
+        out["cpu_baseline"] = {
+            "value": 1.0 / per_recon, "unit": "recons/s", "cores": os.cpu_count(),
+            "cpu_model": cpu_model(), "kind": "port",
+            "sample": (f"one 128-subset VCD step of the headline workload ({par['pixels']} "
+                       f"pixels x 256 slices x 720 views, {par['oracle_step_s']:.2f} s) by the "
+                       f"FP64 C oracle with OpenMP, multiplied by {SUBSET_STEPS_PER_RECON:.0f} "
+                       f"subset-step equivalents per recon"),
             "seconds_per_recon_extrapolated": per_recon}
+        out["parity_vs_fp64_oracle"] = par
+    except Exception as exc:
+        out["cpu_baseline"] = {"value": None, "error": repr(exc)[:300]}
+    r1 = reference_cpu_recon_cfg1(torch)
+    r1.pop("sino", None)
+    out["reference_cpu_recon_small"] = r1
+    return out
+
+
+# ── measured extras ─────────────────────────────────────────────────────────
+def subset_touch(m, torch, y, n_subsets=128, samples=4):
+    """Mean count of error-sinogram cells a subset step must read (N_touch):
+    the cells where A has a nonzero entry for some pixel of the subset,
+    counted on the device by forward-projecting ones over whole cylinders
+    of `samples` subsets of the `n_subsets`-subset partition."""
+    import mbirtorch_b200 as mb
+    rs = m.get_params('recon_shape')
+    rng = np.random.RandomState(11)
+    part = mb.gen_pixel_partition(rs, n_subsets, rng=rng)
+    counts = []
+    for k in range(samples):
+        idx = torch.as_tensor(part[k].astype(np.int64), device=y.device)
+        ones = torch.ones(idx.shape[0], rs[2], device=y.device)
+        s = m.projector.forward(ones, idx)
+        counts.append(int((s != 0).sum()))
+    return float(np.mean(counts)), int(part.shape[1])
+
+
+def kernel_timing(m, torch, y, storage):
+    """One recon with the library's per-launch CUDA events: {name: (ms, n)}.
+    Timing mode launches each kernel the ordinary way (no programmatic
+    dependent launch) so that an event pair brackets one kernel."""
+    from mbirtorch_b200 import _lib
+    m.set_storage_precision(storage)
+    _lib.timing_collect()
+    _lib.timing_enable(True)
+    recon(m, y, output_sharded=True)
+    torch.cuda.synchronize()
+    _lib.timing_enable(False)
+    return _lib.timing_collect()
+
+
+def roofline_block(m, torch, y, kt, storage, hbm):
+    """The dominant kernel against HBM with the survey's algorithmic bytes:
+    b_e per reached error-sinogram cell for the gradient and for the forward
+    with line search (one read of e; its A delta store is the design's, and
+    counts only in `traffic`), 2 b_e for the tail (read and write e)."""
+    b_e = 4 if storage == "float32" else 2
+    n_touch, ps = subset_touch(m, torch, y)
+    per = {"vcd gradient (back projection)": 1.0, "vcd forward + line search": 1.0,
+           "vcd pixel + sinogram update": 2.0}
+    total = sum(v[0] for v in kt.values())
+    top = max((k for k in kt if k in per), key=lambda k: kt[k][0])
+    tms, tcnt = kt[top]
+    alg = per[top] * b_e * n_touch
+    ach = alg / (tms / tcnt / 1e3) / 1e9
+    V, R, C = m.get_params('sinogram_shape')
+    # DRAM bytes per launch of the dominant kernel (ncu, dram__bytes_read.sum +
+    # dram__bytes_write.sum) on this workload's 128-subset step, FP32 storage.
+    traffic = {("vcd forward + line search", "float32"): TRAFFIC_FWD_LS_FP32}
+    return {"kernel": top, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+            "frac": ach / hbm, "traffic": traffic.get((top, storage)),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                              "(profiles/), 128-subset step of this workload",
+            "algorithmic_bytes_per_launch": alg,
+            "algorithmic_bytes_rule": f"{per[top]:g} x {b_e} B x N_touch",
+            "n_touch_cells": n_touch, "subset_pixels": ps,
+            "n_touch_fraction_of_sinogram": n_touch / (V * R * C),
+            "avg_launch_ms": tms / tcnt, "launches": tcnt,
+            "share_of_kernel_time": tms / total,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+
+
+# DRAM traffic of one forward + line-search launch of the headline workload's
+# 128-subset step (ncu; see profiles/); None until captured.
+TRAFFIC_FWD_LS_FP32 = None
+
+
+def projector_block(m, torch, dev):
+    """Full-volume forward and back projection of the model's ROR pixels."""
+    S = m.get_params('recon_shape')[2]
+    V = m.get_params('sinogram_shape')[0]
+    idx = m.full_indices_device()
+    vals = torch.rand(idx.shape[0], S, device=dev)
+    for _ in range(2):
+        s = m.projector.forward(vals, idx)
+        m.projector.back(s, idx)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record()
+    for _ in range(3):
+        s = m.projector.forward(vals, idx)
+    ev[1].record()
+    for _ in range(3):
+        m.projector.back(s, idx)
+    ev[2].record()
+    torch.cuda.synchronize()
+    tf = ev[0].elapsed_time(ev[1]) / 3 / 1e3
+    tb = ev[1].elapsed_time(ev[2]) / 3 / 1e3
+    vv = idx.shape[0] * S * V
+    return {"voxel_views": int(vv), "forward_gvox_views_per_s": vv / tf / 1e9,
+            "back_gvox_views_per_s": vv / tb / 1e9, "forward_ms": tf * 1e3,
+            "back_ms": tb * 1e3, "pixels_ror": int(idx.shape[0])}
+
+
+def precision_block(m, torch, y, ref_rec, parity_f32=None):
+    """bfloat16 / float16 storage recons of the same data: recons/s (one
+    untimed warm-up recon each, then one timed) and relative L2 to the FP32
+    recon.  The FP32 path's own distance to the FP64 oracle is bounded per
+    step by `parity_vs_fp64_oracle`; the 16-bit paths are held to the FP64
+    oracle directly at smaller sizes by the tests."""
+    out = {}
+    ref = ref_rec.double()
+    for st in ("bfloat16", "float16"):
+        m.set_storage_precision(st)
+        recon(m, y, output_sharded=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r2, _ = recon(m, y, output_sharded=True)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[st] = {"recons_per_s": 1.0 / dt, "seconds": dt,
+                   "rel_l2_vs_f32_recon": float((r2.double() - ref).norm() / ref.norm())}
+        del r2
+    m.set_storage_precision("float32")
+    return out
+
+
+def cone256_extra(mb, torch, dev):
+    """The 256^3 flat-cone configuration (360 views, 256 x 384): recons/s at
+    FP32 (three timed recons after a warm-up) and the 16-bit storages."""
+    m = cone_model(mb, "cone256_flat")
+    y = make_data(m, torch, dev, 0)
+    recon(m, y, output_sharded=True)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for _ in range(3):
+        r, rd = recon(m, y, output_sharded=True)
+    ev[1].record()
+    torch.cuda.synchronize()
+    s = ev[0].elapsed_time(ev[1]) / 3 / 1e3
+    out = {"workload": workload("cone256_flat"), "recons_per_s": 1.0 / s, "seconds": s,
+           "fm_rmse_final": rd["recon_params"]["fm_rmse"][-1]}
+    out["mixed_precision"] = precision_block(m, torch, y, r)
+    return out
 
 
 # The HBM-bound VCD case: a parallel-beam subset step touches most of the
-# sinogram for few voxel-views (survey example: 512^2 x 256 volume, 720 views).
+# sinogram for few voxel-views (512^2 x 256 volume, 720 views).
 PAR_V, PAR_R, PAR_C, PAR_N = 720, 256, 768, 512
-
-
-def make_parallel_model(mb):
-    m = mb.ParallelBeamModel((PAR_V, PAR_R, PAR_C),
-                             np.linspace(0, np.pi, PAR_V, endpoint=False))
-    m.set_params(no_warning=True, verbose=0, recon_shape=(PAR_N, PAR_N, PAR_R))
-    return m
 
 
 def parallel_pass_setup(mb, torch):
@@ -248,7 +588,8 @@ def parallel_pass_setup(mb, torch):
     128-subset partition with its order."""
     from mbirtorch_b200 import _lib
     from mbirtorch_b200.vcd_engine import ResidentSinogram
-    m = make_parallel_model(mb)
+    m = mb.ParallelBeamModel((PAR_V, PAR_R, PAR_C), np.linspace(0, np.pi, PAR_V, endpoint=False))
+    m.set_params(no_warning=True, verbose=0, recon_shape=(PAR_N, PAR_N, PAR_R))
     dev = torch.device("cuda", 0)
     gen = torch.Generator(device=dev).manual_seed(3)
     y = torch.rand((PAR_V, PAR_R, PAR_C), generator=gen, device=dev)
@@ -258,61 +599,22 @@ def parallel_pass_setup(mb, torch):
     rs = m.get_params("recon_shape")
     flat = torch.zeros(rs[0] * rs[1], rs[2], device=dev)
     err = ResidentSinogram.from_vrc(y, _lib.MBIR_F32)
-    del y
     rng = np.random.RandomState(0)
     part = torch.as_tensor(mb.gen_pixel_partition(rs, 128, rng=rng), device=dev)
     order = rng.permutation(part.shape[0]).astype(np.int32)
     acc = torch.zeros(2 + rs[2], dtype=torch.float64, device=dev)
-    return m, upd, flat, err, part, order, acc
-
-
-def cone64_pass(mb, torch):
-    """One 128-subset partition pass of the serving mix's largest cone jobs
-    (256^2 x 64 volume, 360 views, 64 x 384 flat detector of pitch 2, SID
-    512, SDD 1024; FP32 storage on a seeded stand-in error sinogram), then
-    a second pass with per-launch CUDA events, whose per-kernel averages
-    are printed (one line each)."""
-    from mbirtorch_b200 import _lib
-    from mbirtorch_b200.vcd_engine import ResidentSinogram
-    dev = torch.device("cuda", 0)
-    Vc, Sc, Cc, Nc = 360, 64, 384, 256
-    m = mb.ConeBeamModel((Vc, Sc, Cc), np.linspace(0, 2 * np.pi, Vc, endpoint=False),
-                         source_detector_dist=4.0 * Nc, source_iso_dist=2.0 * Nc)
-    m.set_params(no_warning=True, delta_det_channel=2.0, delta_det_row=2.0)
-    m.auto_set_recon_geometry(no_warning=True)
-    m.set_params(no_warning=True, verbose=0, recon_shape=(Nc, Nc, Sc))
-    y = torch.rand((Vc, Sc, Cc), generator=torch.Generator(device=dev).manual_seed(1),
-                   device=dev)
-    m.auto_set_regularization_params(y)
-    H = m.compute_hessian_diagonal(output_sharded=True)
-    upd = m.create_vcd_subset_updater(H, weights=1)
-    rs = m.get_params("recon_shape")
-    flat = torch.zeros(rs[0] * rs[1], rs[2], device=dev)
-    err = ResidentSinogram.from_vrc(y, _lib.MBIR_F32)
-    rng = np.random.RandomState(0)
-    part = torch.as_tensor(mb.gen_pixel_partition(rs, 128, rng=rng), device=dev)
-    order = rng.permutation(part.shape[0]).astype(np.int32)
-    acc = torch.zeros(2 + rs[2], dtype=torch.float64, device=dev)
-    upd.engine.partition_pass(flat, err, part, order, acc)
-    torch.cuda.synchronize()
-    _lib.timing_collect()
-    _lib.timing_enable(True)
-    upd.engine.partition_pass(flat, err, part, order, acc)
-    torch.cuda.synchronize()
-    _lib.timing_enable(False)
-    for k, v in sorted(_lib.timing_collect().items(), key=lambda kv: -kv[1][0]):
-        print(f"{k}: {1e3 * v[0] / v[1]:.1f} us x {v[1]}")
+    return m, upd, flat, err, part, order, acc, y
 
 
 def parallel_subset_extra(mb, torch, hbm):
     """One 128-subset partition pass of the parallel workload above: the
     pass's CUDA-event time (kernels chained as in a recon), then each
     kernel's CUDA-event average from a second, per-launch timed pass, and
-    the binned forward + line search and the tail against the measured HBM
-    bandwidth (algorithmic bytes: e read and A delta written, resp. e and
-    A delta read and e written, over the reached part of the sinogram)."""
+    the forward + line search and the tail against the measured HBM
+    bandwidth (algorithmic bytes: one e read over the reached cells, resp.
+    an e read and write)."""
     from mbirtorch_b200 import _lib
-    m, upd, flat, err, part, order, acc = parallel_pass_setup(mb, torch)
+    m, upd, flat, err, part, order, acc, y = parallel_pass_setup(mb, torch)
     upd.engine.partition_pass(flat, err, part, order, acc)  # warm-up
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     torch.cuda.synchronize()
@@ -327,97 +629,22 @@ def parallel_subset_extra(mb, torch, hbm):
     torch.cuda.synchronize()
     _lib.timing_enable(False)
     kt = _lib.timing_collect()
-    frac = shadow_fraction(m, mb)
-    sino = PAR_V * PAR_R * PAR_C
+    n_touch, ps = subset_touch(m, torch, y)
     out = {"workload": f"parallel {PAR_N}^2 x {PAR_R} volume, {PAR_V} views, {PAR_R} x {PAR_C} "
-                       f"detector, FP32 storage, one 128-subset pass "
-                       f"({int(part.shape[1])} pixels per subset)",
-           "subset_step_us": 1e3 * pass_ms / part.shape[0], "shadow_fraction": frac,
+                       f"detector, FP32 storage, one 128-subset pass ({ps} pixels per subset)",
+           "subset_step_us": 1e3 * pass_ms / part.shape[0], "n_touch_cells": n_touch,
+           "n_touch_fraction_of_sinogram": n_touch / (PAR_V * PAR_R * PAR_C),
            "kernels_us": {k: 1e3 * v[0] / v[1] for k, v in kt.items()}}
-    for name, nbytes in (("vcd forward + line search", 2 * 4 * frac * sino),
-                         ("vcd pixel + sinogram update", 3 * 4 * frac * sino)):
+    for name, nbytes in (("vcd forward + line search", 4 * n_touch),
+                         ("vcd gradient (back projection)", 4 * n_touch),
+                         ("vcd pixel + sinogram update", 2 * 4 * n_touch)):
         if name in kt:
             t = kt[name][0] / kt[name][1] / 1e3
             out[name] = {"algorithmic_bytes": nbytes, "achieved_gbs": nbytes / t / 1e9,
                          "frac_of_measured_hbm": nbytes / t / 1e9 / hbm}
-    vv = int(part.shape[1]) * PAR_R * PAR_V
+    vv = ps * PAR_R * PAR_V
     t_f = kt["vcd forward + line search"][0] / kt["vcd forward + line search"][1] / 1e3
     out["forward_gvox_views_per_s"] = vv / t_f / 1e9
-    return out
-
-
-def phantom_torch(torch, shape, seed, dev):
-    """The ellipsoid phantom of phantom() built on the device for large
-    grids: 10 seeded ellipsoids on [-1, 1]^3 (centres U[-0.5, 0.5],
-    semi-axes U[0.05, 0.4], in-plane angle U[0, 180) deg, density
-    U[0.1, 1])."""
-    rng = np.random.default_rng(seed)
-    nr, nc, ns = shape
-    g1 = torch.linspace(-1, 1, nr, device=dev)
-    g0 = torch.linspace(-1, 1, nc, device=dev)
-    gz = torch.linspace(-1, 1, ns, device=dev)
-    Y, X = torch.meshgrid(g1, g0, indexing="ij")
-    vol = torch.zeros(shape, device=dev)
-    for _ in range(10):
-        c = rng.uniform(-0.5, 0.5, 3)
-        a = rng.uniform(0.05, 0.4, 3)
-        ang = np.deg2rad(rng.uniform(0, 180))
-        dens = float(rng.uniform(0.1, 1.0))
-        ca, sa = float(np.cos(ang)), float(np.sin(ang))
-        xr = ca * (X - c[0]) + sa * (Y - c[1])
-        yr = -sa * (X - c[0]) + ca * (Y - c[1])
-        xy = (xr / a[0]) ** 2 + (yr / a[1]) ** 2
-        z = ((gz - c[2]) / a[2]) ** 2
-        vol += dens * ((xy[:, :, None] + z[None, None, :]) <= 1).float()
-    return vol
-
-
-def cone_large_extra(mb, torch, iters=ITERS):
-    """The mixed-precision cone configuration: 512 x 512 x 256 ellipsoid
-    phantom, 720 views on [0, 2 pi), curved 320 x 768 detector (pitch 2),
-    SID 1024, SDD 2048, Poisson counts at I0 = 1e4, 20 VCD iterations; one
-    recon each with FP32, float16 and bfloat16 storage, their recons/s and
-    each 16-bit result's relative L2 to the FP32 result.  (The FP64 oracle
-    is out of reach at this size on the host; the tests hold the 16-bit
-    paths to the FP64 oracle at smaller sizes.)"""
-    dev = torch.device("cuda", 0)
-    Vl, Rl, Cl, Nl, Sl = 720, 320, 768, 512, 256
-    m = mb.ConeBeamModel((Vl, Rl, Cl), np.linspace(0, 2 * np.pi, Vl, endpoint=False),
-                         source_detector_dist=SDD, source_iso_dist=SID,
-                         use_curved_detector=True)
-    m.set_params(no_warning=True, verbose=0, delta_det_channel=2.0, delta_det_row=2.0)
-    m.auto_set_recon_geometry(no_warning=True)
-    m.set_params(no_warning=True, recon_shape=(Nl, Nl, Sl))
-    vol = phantom_torch(torch, (Nl, Nl, Sl), 5, dev)
-    clean = m.forward_project(vol, output_sharded=True)
-    del vol
-    mu = 3.0 / float(clean.max())
-    gen = torch.Generator(device=dev).manual_seed(2)
-    counts = torch.poisson(I0 * torch.exp(-mu * clean), generator=gen)
-    del clean
-    y = (-torch.log(torch.clamp(counts, min=1.0) / I0) / mu).to(torch.float32).contiguous()
-    del counts
-    out = {"workload": f"cone curved {Nl}x{Nl}x{Sl} volume, {Vl} views on [0, 2pi), "
-                       f"{Rl}x{Cl} detector (pitch 2), SID 1024, SDD 2048, Poisson I0=1e4, "
-                       f"{iters} VCD iterations",
-           "voxel_views_full_projection": int(m.full_indices_device().shape[0]) * Sl * Vl}
-    ref = None
-    for st in ("float32", "float16", "bfloat16"):
-        m.set_storage_precision(st)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        np.random.seed(0)
-        r, _ = m.recon(y, max_iterations=iters, stop_threshold_change_pct=0,
-                       logfile_path=None, print_logs=False, output_sharded=True)
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        entry = {"recons_per_s": 1.0 / dt, "seconds": dt}
-        if ref is None:
-            ref = r.double()
-        else:
-            entry["rel_l2_vs_f32_recon"] = float((r.double() - ref).norm() / ref.norm())
-        out[st] = entry
-        del r
     return out
 
 
@@ -480,279 +707,6 @@ def autograd_extra(mb, torch, steps=3):
     return out
 
 
-def shadow_fraction(m, mb):
-    """Fraction of (view, channel) columns that the ROR pixels' channel taps
-    reach (the part of the sinogram a subset step must touch)."""
-    import oracle  # noqa: F401  (numpy geometry only)
-    rs = m.get_params('recon_shape')
-    idx = mb.gen_full_indices(rs).astype(np.int64)
-    g = m._geometry()
-    Cm = g.num_det_channels
-    row, col = idx // rs[1], idx % rs[1]
-    yt = g.delta_voxel_row * (row - (rs[0] - 1) / 2.0)
-    xt = g.delta_voxel * (col - (rs[1] - 1) / 2.0)
-    tot = 0
-    vp = m._view_params_array()
-    angles = vp[:, 0] if vp.ndim == 2 else vp
-    for a in angles[::12]:
-        x = np.cos(a) * xt - np.sin(a) * yt
-        y = np.sin(a) * xt + np.cos(a) * yt
-        mag = 1.0 / (1.0 / g.magnification - y / g.source_detector_dist) \
-            if g.geometry == 1 else 1.0
-        n = np.rint((mag * x + g.det_channel_offset) / g.delta_det_channel
-                    + (Cm - 1) / 2.0).astype(int)
-        hit = np.zeros(Cm + 8, bool)
-        for t in range(-g.psf_radius, g.psf_radius + 1):
-            hit[np.clip(n + t, 0, Cm - 1)] = True
-        tot += hit[:Cm].mean()
-    return tot / len(angles[::12])
-
-
-def main():
-    args = parse()
-    if args.warmup < 3:
-        args.warmup = 3
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-
-    if args.impl == "reference":
-        return main_reference(args, rank, world)
-
-    import torch
-    import torch.distributed as dist
-    import mbirtorch_b200 as mb
-    from mbirtorch_b200 import _lib
-    from mbirtorch_b200.replicas import max_over_ranks, replica_rate
-
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        dist.init_process_group("nccl", init_method="env://",
-                                timeout=__import__("datetime").timedelta(seconds=600))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    if args.profile_case == "subset-cone64":
-        cone64_pass(mb, torch)
-        return
-    if args.profile_case == "subset-parallel":
-        # one 128-subset partition pass of the parallel 512^2 x 256 workload
-        _, upd, flat, err, part, order, acc = parallel_pass_setup(mb, torch)
-        upd.engine.partition_pass(flat, err, part, order, acc)
-        torch.cuda.synchronize()
-        return
-    m = make_model(mb)
-    m.set_storage_precision(args.storage)
-    vol, y = make_data(mb, m, torch, dev)
-    if args.profile_case:
-        return profile_case(args.profile_case, m, mb, torch, y)
-    y_host = y.cpu().numpy()
-
-    def one_recon(sino):
-        np.random.seed(0)
-        return m.recon(sino, max_iterations=ITERS, stop_threshold_change_pct=0,
-                       logfile_path=None, print_logs=False, output_sharded=True)
-
-    for _ in range(args.warmup):
-        rec, rd = one_recon(y)
-    barrier()
-    # ── value: device-resident sinogram ──
-    launches0 = _lib.launch_count()
-    with Clocks(local) as clk:
-        barrier()
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
-        t0.record()
-        for _ in range(args.steps):
-            rec, rd = one_recon(y)
-        t1.record()
-        barrier()
-    launches = _lib.launch_count() - launches0
-    ms = max_over_ranks(t0.elapsed_time(t1), dev)
-    ms_per_step = ms / args.steps
-    value = replica_rate(args.steps, ms / 1e3, world)
-    clocks = clk.summary()
-    rec_ref = rec.detach().clone()
-
-    # ── e2e: host numpy in, host numpy out ──
-    barrier()
-    t0e = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        np.random.seed(0)
-        rec_np, _ = m.recon(y_host, max_iterations=ITERS, stop_threshold_change_pct=0,
-                            logfile_path=None, print_logs=False)
-    e1.record()
-    barrier()
-    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dev)
-    wall_e2e = time.perf_counter() - t0e
-    e2e = {"value": replica_rate(args.steps, ms_e2e / 1e3, world), "unit": "recons/s",
-           "h2d_bytes_per_step": int(y_host.nbytes), "d2h_bytes_per_step": int(rec_np.nbytes),
-           "wall_s": wall_e2e}
-
-    out = {"metric": METRIC, "value": value, "unit": "recons/s", "n_gpus": world,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": {"float32": "f32", "bfloat16": "bf16 storage, f32 math",
-                     "float16": "f16 storage, f32 math"}.get(args.storage, args.storage),
-           "data": "synthetic (seeded ellipsoid phantom, Poisson noise)",
-           "config": {"workload": WORKLOAD, "volume": [NVOX] * 3, "views": V,
-                      "detector_rows_channels": [R, C], "iterations": ITERS,
-                      "storage": args.storage, "parallelism": f"replicas x{world}",
-                      "l2": "inputs larger than L2 (141.6 MB f32 sinogram vs 126 MB L2)"},
-           "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks}
-
-    if rank == 0 and not args.no_extras:
-        # N > 1: the roofline and kernel shares only (the CPU baseline and the
-        # other extras are single-GPU measurements, taken at N = 1)
-        out.update(extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd, full=world == 1))
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(out), flush=True)
-
-
-def extras(args, m, mb, torch, dev, y, y_host, rec_ref, rd, full=True):
-    from mbirtorch_b200 import _lib
-    res = {}
-    # ── per-kernel timing over one timed recon -> roofline of the top kernel
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
-    _lib.timing_collect()
-    _lib.timing_enable(True)
-    np.random.seed(0)
-    m.recon(y, max_iterations=ITERS, stop_threshold_change_pct=0, logfile_path=None,
-            print_logs=False, output_sharded=True)
-    torch.cuda.synchronize()
-    _lib.timing_enable(False)
-    kt = _lib.timing_collect()
-    total = sum(v[0] for v in kt.values())
-    top = max(kt, key=lambda k: kt[k][0])
-    b_e = {"float32": 4, "bfloat16": 2, "float16": 2}[args.storage]
-    frac = shadow_fraction(m, mb)
-    sino = V * R * C
-    bytes_per_launch = {
-        "vcd gradient (back projection)": frac * sino * b_e,
-        "vcd forward + line search": 2 * frac * sino * b_e,
-        # the tail's tile role: read e and A delta, write e, over the reached tiles
-        "vcd pixel + sinogram update": 3 * frac * sino * b_e,
-    }
-    # DRAM bytes of one forward + line-search launch at this workload (FP32
-    # storage), measured by ncu on one launch of the 399-pixel subset step:
-    # 103.9 MB read + 58.3 MB written.
-    traffic = {("vcd forward + line search", "float32"): (103.9e6 + 58.3e6)}
-    tms, tcnt = kt[top]
-    alg = bytes_per_launch.get(top)
-    if alg is not None:
-        ach = alg / (tms / tcnt / 1e3) / 1e9
-        res["roofline"] = {"kernel": top, "bound": "hbm", "achieved": ach, "peak": hbm,
-                           "unit": "GB/s", "frac": ach / hbm,
-                           "traffic": traffic.get((top, args.storage)),
-                           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
-                                             "one launch of the subset-step capture",
-                           "algorithmic_bytes_per_launch": alg,
-                           "avg_launch_ms": tms / tcnt, "launches": tcnt,
-                           "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
-    res["kernel_time_share"] = {k: {"ms": v[0], "launches": v[1], "share": v[0] / total}
-                                for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
-    if not full:
-        return res
-    # ── projector throughput (full volume, f32, device-resident) ──
-    idx = m.full_indices_device()
-    vals = torch.rand(idx.shape[0], NVOX, device=dev)
-    for _ in range(3):
-        s = m.projector.forward(vals, idx)
-        b = m.projector.back(s, idx)
-    torch.cuda.synchronize()
-    vv = idx.shape[0] * NVOX * V
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    ev[0].record()
-    for _ in range(5):
-        s = m.projector.forward(vals, idx)
-    ev[1].record()
-    for _ in range(5):
-        b = m.projector.back(s, idx)
-    ev[2].record()
-    torch.cuda.synchronize()
-    tf = ev[0].elapsed_time(ev[1]) / 5 / 1e3
-    tb = ev[1].elapsed_time(ev[2]) / 5 / 1e3
-    res["projectors"] = {"voxel_views": vv, "forward_gvox_views_per_s": vv / tf / 1e9,
-                         "back_gvox_views_per_s": vv / tb / 1e9, "forward_ms": tf * 1e3,
-                         "back_ms": tb * 1e3, "pixels_ror": int(idx.shape[0])}
-    # ── mixed precision: same recon with bf16 / f16 storage ──
-    mp = {}
-    ref = rec_ref.double()
-    for st in ("bfloat16", "float16"):
-        m.set_storage_precision(st)
-        np.random.seed(0)
-        r2, _ = m.recon(y, max_iterations=ITERS, stop_threshold_change_pct=0,
-                        logfile_path=None, print_logs=False, output_sharded=True)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        np.random.seed(0)
-        r2, _ = m.recon(y, max_iterations=ITERS, stop_threshold_change_pct=0,
-                        logfile_path=None, print_logs=False, output_sharded=True)
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        rel = float((r2.double() - ref).norm() / ref.norm())
-        mp[st] = {"recons_per_s": 1.0 / dt, "rel_l2_vs_f32_recon": rel}
-    m.set_storage_precision(args.storage)
-    res["mixed_precision"] = mp
-    res["serving"] = serving_extra(mb, torch, y_host, rec_ref)
-    res["serving_mix"] = serving_mix_extra(mb, torch)
-    res["parallel_subset"] = parallel_subset_extra(mb, torch, hbm)
-    res["cone_large"] = cone_large_extra(mb, torch)
-    res["autograd"] = autograd_extra(mb, torch)
-    res["fm_rmse_final"] = rd["recon_params"]["fm_rmse"][-1]
-    # ── CPU baseline ──
-    try:
-        res["cpu_baseline"] = cpu_baseline(m, y_host, rd["recon_params"]["regularization_params"],
-                                           mb)
-    except Exception as exc:  # reported, never fatal to the GPU line
-        res["cpu_baseline"] = {"value": None, "error": repr(exc)[:200]}
-    return res
-
-
-def serving_extra(mb, torch, y_host, rec_ref, jobs=4):
-    """The batched mixed-precision form: `jobs` reconstructions of this
-    workload submitted together to a ReconServer (float16 storage, all jobs
-    resident and advancing concurrently on their own streams).  Job 0 draws
-    its partitions like the timed FP32 recon (seed 0), so its relative L2
-    against that recon is the storage precision's error alone."""
-    from mbirtorch_b200.serving import ReconServer
-    out = {"jobs": jobs, "storage": "float16"}
-    for warm in (True, False):
-        srv = ReconServer(storage_dtype="float16", max_active=jobs)
-        reqs = []
-        t0 = time.perf_counter()
-        for j in range(jobs):
-            mj = make_model(mb)
-            reqs.append(srv.submit(mj, y_host, max_iterations=ITERS, seed=j, arrival=t0))
-        srv.run_until_idle(timeout_s=600)
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-    st = srv.stats()
-    ref = rec_ref.double().cpu()
-    r0 = torch.as_tensor(reqs[0].recon).double()
-    out.update({"recons_per_s": jobs / wall, "wall_s": wall,
-                "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
-                "max_concurrent": st["max_concurrent"],
-                "rel_l2_job0_vs_f32_recon": float((r0 - ref).norm() / ref.norm()),
-                "failed": st["failed"]})
-    return out
-
-
 def mix_jobs(mb, torch, n_jobs=16, seed=7):
     """A seeded sample of the serving mix, scaled to run in seconds: 40%
     parallel, 40% cone, 20% helical cone (2 turns); slices in {16, 64},
@@ -805,11 +759,11 @@ def serving_mix_extra(mb, torch, n_jobs=16):
     form (each job alone, FP32, one after another through model.recon) vs
     the served form (all jobs submitted at once to a ReconServer with
     float16 storage: resident, admitted against the memory ledger, advancing
-    concurrently, recurring partition passes replayed as CUDA graphs; the
-    served form with direct launches is timed beside it).  Both with 10 VCD
-    iterations and the same per-job seeds, so each served result is compared
-    with its own plain result.  Each arm is timed three times (interleaved)
-    and the median run is reported, with all samples."""
+    concurrently; recurring partition passes replayed as CUDA graphs, and
+    the same with direct launches).  Both with 10 VCD iterations and the
+    same per-job seeds, so each served result is compared with its own plain
+    result.  Each arm is timed three times (interleaved) and the median run
+    is reported, with all samples."""
     from mbirtorch_b200.serving import ReconServer
     jobs = mix_jobs(mb, torch, n_jobs)
     iters = 10
@@ -835,9 +789,6 @@ def serving_mix_extra(mb, torch, n_jobs=16):
 
     plain()        # warm-up (library load, allocator)
     served()
-    # Three timed runs of each arm, interleaved; the median is reported (the
-    # served arm's host-side scheduling makes single runs noisy on a shared
-    # host) with every sample beside it.
     t_plains, t_srvs, t_ngs, runs = [], [], [], []
     for _ in range(3):
         ref, tp = plain()
@@ -870,37 +821,355 @@ def serving_mix_extra(mb, torch, n_jobs=16):
             "served_p50_latency_s": st["p50_latency_s"],
             "served_p99_latency_s": st["p99_latency_s"],
             "max_concurrent": st["max_concurrent"], "failed": st["failed"],
-            "max_rel_l2_served_vs_plain": max(rel)}
+            "max_rel_l2_served_vs_plain_f32": max(rel)}
+
+
+# ── the reference's own GPU kernels on this GPU ────────────────────────────
+def _time_cuda(torch, fn, reps=3):
+    fn()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for _ in range(reps):
+        fn()
+    ev[1].record()
+    torch.cuda.synchronize()
+    return ev[0].elapsed_time(ev[1]) / reps
+
+
+def triton_reference_extra(mb, torch):
+    """The reference's own GPU path (mbirtorch 0.0.2 from baseline/_ref: its
+    Triton projector bodies selected by _view_batch_bodies after its own
+    availability self-checks, its view-batch driver, its subset updater) on
+    this GPU, against this package on identical device-resident inputs:
+    full-volume sparse_forward_project / sparse_back_project and one VCD
+    subset step of a 128-subset partition, for the 256^3 flat-cone and the
+    headline curved-cone configurations, plus the parallel 512^2 x 256 /
+    720-view case.  Times are CUDA-event milliseconds after a warm-up call
+    (Triton compiles on first use)."""
+    ref = import_reference()
+    if ref is None:
+        return {"unavailable": "reference not installed under baseline/_ref"}
+    from mbirtorch import kernel_availability as ka
+    dev = torch.device("cuda", 0)
+    out = {"reference": f"mbirtorch {ref.__version__} (baseline/_ref), compile_mode='off'",
+           "triton_probe": list(ka.triton_available())}
+    cases = [("cone256_flat", None), ("cone512_curved", None), ("parallel512_720v", None)]
+    for name, _ in cases:
+        res = {}
+        try:
+            if name == "parallel512_720v":
+                ang = np.linspace(0, np.pi, PAR_V, endpoint=False)
+                rm = ref.ParallelBeamModel((PAR_V, PAR_R, PAR_C), ang, compile_mode='off')
+                mm = mb.ParallelBeamModel((PAR_V, PAR_R, PAR_C), ang)
+                for x in (rm, mm):
+                    x.set_params(no_warning=True, verbose=0, recon_shape=(PAR_N, PAR_N, PAR_R))
+            else:
+                rm = cone_model(ref, name, compile_mode='off')
+                mm = cone_model(mb, name)
+            rm.configure_devices(devices=['cuda:0'])
+            bodies = rm._view_batch_bodies()
+            res["reference_bodies"] = [b.__name__ for b in bodies]
+            rs = mm.get_params('recon_shape')
+            V, R, C = mm.get_params('sinogram_shape')
+            idx = torch.as_tensor(mb.gen_full_indices(rs).astype(np.int64), device=dev)
+            gen = torch.Generator(device=dev).manual_seed(5)
+            vals = torch.rand(idx.shape[0], rs[2], generator=gen, device=dev)
+            sino = torch.rand((V, R, C), generator=gen, device=dev)
+            vv = int(idx.shape[0]) * rs[2] * V
+            for who, model in (("reference", rm), ("mbirtorch_b200", mm)):
+                tf = _time_cuda(torch, lambda: model.sparse_forward_project(vals, idx))
+                tb = _time_cuda(torch, lambda: model.sparse_back_project(sino, idx))
+                res[who] = {"forward_ms": tf, "back_ms": tb,
+                            "forward_gvox_views_per_s": vv / tf / 1e6,
+                            "back_gvox_views_per_s": vv / tb / 1e6}
+            f_r = rm.sparse_forward_project(vals, idx)
+            f_m = mm.sparse_forward_project(vals, idx)
+            b_r = rm.sparse_back_project(sino, idx)
+            b_m = mm.sparse_back_project(sino, idx)
+            res["forward_rel_l2_mine_vs_reference"] = float((f_m - f_r).norm() / f_r.norm())
+            res["back_rel_l2_mine_vs_reference"] = float((b_m - b_r).norm() / b_r.norm())
+            del f_r, f_m, b_r, b_m
+            # one VCD subset step (128-subset partition) from a zero volume
+            rng = np.random.RandomState(0)
+            sub = torch.as_tensor(mb.gen_pixel_partition(rs, 128, rng=rng)[0].astype(np.int64),
+                                  device=dev)
+            H = torch.ones(rs[0] * rs[1], rs[2], device=dev)
+            for x in (rm, mm):
+                x.set_params(no_warning=True, sigma_y=1.0, sigma_x=0.1)
+            r_upd = rm.create_vcd_subset_updater(rm._as_shards(H, rm.recon_placement), weights=1)
+            r_flat = rm._as_shards(torch.zeros_like(H), rm.recon_placement)
+            r_err = rm._as_shards(sino.clone(), rm.sino_placement)
+            m_upd = mm.create_vcd_subset_updater(H, weights=1)
+            from mbirtorch_b200 import _lib
+            from mbirtorch_b200.vcd_engine import ResidentSinogram
+            m_flat = torch.zeros_like(H)
+            m_err = ResidentSinogram.from_vrc(sino, _lib.MBIR_F32)
+            t_r = _time_cuda(torch, lambda: r_upd(r_flat, r_err, sub))
+            t_m = _time_cuda(torch, lambda: m_upd.engine.subset_update(m_flat, m_err, sub))
+            res["subset_step"] = {"pixels": int(sub.shape[0]), "reference_ms": t_r,
+                                  "mbirtorch_b200_ms": t_m}
+            res["ratio_forward"] = res["reference"]["forward_ms"] / res["mbirtorch_b200"]["forward_ms"]
+            res["ratio_back"] = res["reference"]["back_ms"] / res["mbirtorch_b200"]["back_ms"]
+            res["ratio_subset_step"] = t_r / t_m
+            del r_err, m_err, sino, vals
+        except Exception as exc:
+            res["error"] = repr(exc)[:400]
+        torch.cuda.empty_cache()
+        out[name] = res
+    return out
+
+
+# ── main ────────────────────────────────────────────────────────────────────
+def main():
+    args = parse()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return main_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    import mbirtorch_b200 as mb
+    from mbirtorch_b200 import _lib
+    from mbirtorch_b200.replicas import max_over_ranks, replica_rate
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    if args.profile_case:
+        return profile_case(args.profile_case, mb, torch, dev)
+    m = cone_model(mb, HEAD)
+    m.set_storage_precision(args.storage)
+    y = make_data(m, torch, dev, 5)
+    y_pinned = y.cpu().pin_memory()
+
+    for _ in range(args.warmup):
+        rec, rd = recon(m, y, output_sharded=True)
+    barrier()
+    # ── value: device-resident sinogram ──
+    launches0 = _lib.launch_count()
+    with Clocks(local) as clk:
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(args.steps):
+            rec, rd = recon(m, y, output_sharded=True)
+        t1.record()
+        barrier()
+    launches = _lib.launch_count() - launches0
+    ms = max_over_ranks(t0.elapsed_time(t1), dev)
+    ms_per_step = ms / args.steps
+    value = replica_rate(args.steps, ms / 1e3, world)
+    clocks = clk.summary()
+    rec_ref = rec.detach().clone()
+
+    # ── e2e: pinned host sinogram in, host volume out, through model.recon ──
+    k_e2e = min(args.steps, 3)
+    barrier()
+    t0e = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(k_e2e):
+        rec_np, _ = recon(m, y_pinned)
+    e1.record()
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), dev)
+    e2e = {"value": replica_rate(k_e2e, ms_e2e / 1e3, world), "unit": "recons/s",
+           "steps": k_e2e, "h2d_bytes_per_step": int(y_pinned.numel() * 4),
+           "d2h_bytes_per_step": int(rec_np.nbytes), "wall_s": time.perf_counter() - t0e}
+
+    out = {"metric": METRIC, "value": value, "unit": "recons/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": {"float32": "f32", "bfloat16": "bf16 storage, f32 math",
+                     "float16": "f16 storage, f32 math"}.get(args.storage, args.storage),
+           "data": "synthetic (seeded ellipsoid phantom, Poisson noise)",
+           "config": config_block(args.storage, world),
+           "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+           "fm_rmse_final": rd["recon_params"]["fm_rmse"][-1]}
+
+    if rank == 0 and not args.no_extras:
+        out.update(extras(args, m, mb, torch, dev, y, rec_ref, full=world == 1))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+EXTRAS = ("roofline", "cpu_baseline", "projectors", "mixed_precision", "cone256_flat",
+          "parallel_subset", "serving_mix", "autograd", "triton_reference")
+
+
+def extras(args, m, mb, torch, dev, y, rec_ref, full=True):
+    res = {}
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    want = set(EXTRAS) if args.only_extra is None else {args.only_extra}
+
+    def run(name, fn):
+        if name not in want:
+            return
+        try:
+            res[name] = fn()
+        except Exception as exc:  # reported, never fatal to the headline line
+            res[name] = {"error": repr(exc)[:400]}
+
+    if "roofline" in want:
+        kt = kernel_timing(m, torch, y, args.storage)
+        total = sum(v[0] for v in kt.values())
+        res["roofline"] = roofline_block(m, torch, y, kt, args.storage, hbm)
+        res["kernel_time_share"] = {
+            "mode": "timing mode: per-launch CUDA events, no programmatic dependent launch "
+                    "(so kernels do not overlap their neighbours' tails, and the sum exceeds "
+                    "ms_per_step)",
+            "kernels": {k: {"ms": v[0], "launches": v[1], "share": v[0] / total}
+                        for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}}
+    if not full:
+        return res
+    if "cpu_baseline" in want:
+        res.update(cpu_baseline_leg(m, mb, torch, y, rec_ref))
+    run("projectors", lambda: projector_block(m, torch, dev))
+    run("mixed_precision", lambda: precision_block(m, torch, y, rec_ref))
+    m.set_storage_precision(args.storage)
+    run("cone256_flat", lambda: cone256_extra(mb, torch, dev))
+    run("parallel_subset", lambda: parallel_subset_extra(mb, torch, hbm))
+    run("serving_mix", lambda: serving_mix_extra(mb, torch))
+    run("autograd", lambda: autograd_extra(mb, torch))
+    run("triton_reference", lambda: triton_reference_extra(mb, torch))
+    return res
+
+
+def profile_case(case, mb, torch, dev):
+    """One pass for a profiler (no JSON line).  'recon' is one whole headline
+    reconstruction; 'subset' is three VCD subset steps of its 128-subset
+    partition from a zero volume; 'subset-small' the same on the 256^3
+    flat-cone configuration; 'projectors' one full-volume forward and back
+    projection; 'subset-parallel' one partition pass of the parallel
+    512^2 x 256 workload; 'subset-cone64' one of a 64-slice serving-mix
+    cone job, with per-kernel averages printed."""
+    from mbirtorch_b200.vcd_engine import ResidentSinogram, storage_code
+    if case == "subset-parallel":
+        _, upd, flat, err, part, order, acc, _ = parallel_pass_setup(mb, torch)
+        upd.engine.partition_pass(flat, err, part, order, acc)
+        torch.cuda.synchronize()
+        return
+    if case == "subset-cone64":
+        return cone64_pass(mb, torch)
+    m = cone_model(mb, "cone256_flat" if case == "subset-small" else HEAD)
+    y = make_data(m, torch, dev, 5)
+    if case == "recon":
+        recon(m, y, output_sharded=True)
+    elif case in ("subset", "subset-small"):
+        m.auto_set_regularization_params(y)
+        H = m.compute_hessian_diagonal(output_sharded=True)
+        upd = m.create_vcd_subset_updater(H, weights=1)
+        rs = m.get_params('recon_shape')
+        flat = torch.zeros(rs[0] * rs[1], rs[2], device=dev)
+        err = ResidentSinogram.from_vrc(y, storage_code(m.storage_dtype))
+        rng = np.random.RandomState(0)
+        parts = torch.as_tensor(mb.gen_pixel_partition(rs, 128, rng=rng), device=dev)
+        for i in range(3):
+            upd.engine.subset_update(flat, err, parts[i])
+    else:
+        idx = m.full_indices_device()
+        vals = torch.rand(idx.shape[0], m.get_params('recon_shape')[2], device=dev)
+        s = m.projector.forward(vals, idx)
+        m.projector.back(s, idx)
+    torch.cuda.synchronize()
+
+
+def cone64_pass(mb, torch):
+    """One 128-subset partition pass of the serving mix's largest cone jobs
+    (256^2 x 64 volume, 360 views, 64 x 384 flat detector of pitch 2, SID
+    512, SDD 1024; FP32 storage on a seeded stand-in error sinogram), then
+    a second pass with per-launch CUDA events, whose per-kernel averages
+    are printed (one line each)."""
+    from mbirtorch_b200 import _lib
+    from mbirtorch_b200.vcd_engine import ResidentSinogram
+    dev = torch.device("cuda", 0)
+    Vc, Sc, Cc, Nc = 360, 64, 384, 256
+    m = mb.ConeBeamModel((Vc, Sc, Cc), np.linspace(0, 2 * np.pi, Vc, endpoint=False),
+                         source_detector_dist=4.0 * Nc, source_iso_dist=2.0 * Nc)
+    m.set_params(no_warning=True, delta_det_channel=2.0, delta_det_row=2.0)
+    m.auto_set_recon_geometry(no_warning=True)
+    m.set_params(no_warning=True, verbose=0, recon_shape=(Nc, Nc, Sc))
+    y = torch.rand((Vc, Sc, Cc), generator=torch.Generator(device=dev).manual_seed(1),
+                   device=dev)
+    m.auto_set_regularization_params(y)
+    H = m.compute_hessian_diagonal(output_sharded=True)
+    upd = m.create_vcd_subset_updater(H, weights=1)
+    rs = m.get_params("recon_shape")
+    flat = torch.zeros(rs[0] * rs[1], rs[2], device=dev)
+    err = ResidentSinogram.from_vrc(y, _lib.MBIR_F32)
+    rng = np.random.RandomState(0)
+    part = torch.as_tensor(mb.gen_pixel_partition(rs, 128, rng=rng), device=dev)
+    order = rng.permutation(part.shape[0]).astype(np.int32)
+    acc = torch.zeros(2 + rs[2], dtype=torch.float64, device=dev)
+    upd.engine.partition_pass(flat, err, part, order, acc)
+    torch.cuda.synchronize()
+    _lib.timing_collect()
+    _lib.timing_enable(True)
+    upd.engine.partition_pass(flat, err, part, order, acc)
+    torch.cuda.synchronize()
+    _lib.timing_enable(False)
+    for k, v in sorted(_lib.timing_collect().items(), key=lambda kv: -kv[1][0]):
+        print(f"{k}: {1e3 * v[0] / v[1]:.1f} us x {v[1]}")
 
 
 def main_reference(args, rank, world):
-    """The reference algorithm on the host cores (FP64 C oracle, OpenMP):
-    each step is one bounded sample (a 128-subset VCD step), reported as the
-    extrapolated whole-recon rate."""
+    """The reference's own CPU implementation on the host cores, rank 0 only:
+    each step is one bounded sample (ReferenceCpu), reported as the
+    extrapolated whole-recon rate on the headline workload; its
+    recon_simple_parallel on its CPU configuration is timed whole beside it."""
     if rank != 0:
         return
     import torch
-    import mbirtorch_b200 as mb
-    torch.set_num_threads(os.cpu_count())
-    m = make_model(mb)
-    # data made on the host with the oracle is too slow at this size; the
-    # step's cost does not depend on the values, so use a seeded stand-in
-    rng = np.random.default_rng(0)
-    y_host = rng.random((V, R, C)).astype(np.float32)
-    reg = {"sigma_y": 1.0, "sigma_x": 0.1}
+    rc = ReferenceCpu(torch)
+    if not rc.available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "mbirtorch 0.0.2 is not installed under baseline/_ref"}),
+              flush=True)
+        return
     vals = []
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(m, y_host, reg, mb)
+        # the first sample also takes the 180-view step that fits the
+        # per-view slope; every later one is a single 90-view step
+        cb = rc.sample()
         if i >= args.warmup:
             vals.append(cb["value"])
     v = float(np.mean(vals))
     cb["value"] = v
+    small = reference_cpu_recon_cfg1(torch)
+    small.pop("sino", None)
     out = {"metric": METRIC, "value": v, "unit": "recons/s", "n_gpus": 0, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
-           "data": "synthetic", "config": {"workload": WORKLOAD},
-           "cpu_baseline": cb, "e2e": {"value": v, "unit": "recons/s",
-                                       "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
+           "data": "synthetic (seeded stand-in error sinogram; a step's cost does not depend "
+                   "on the values)",
+           "config": config_block("float32", world),
+           "cpu_baseline": cb, "reference_cpu_recon_small": small,
+           "e2e": {"value": v, "unit": "recons/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
 

@@ -154,6 +154,29 @@ def check(rc):
         raise MbirError(load().mbir_last_error().decode(errors="replace"))
 
 
+def call(device, name, *args):
+    """Call the ABI function ``name`` with ``device`` current and raise on a
+    nonzero return.  The C side launches on the CURRENT device, so every
+    call is bracketed by the device of the tensors it is given, whatever
+    device the calling thread has current (the reference brackets its
+    launches the same way, triton_cone.py:433-445)."""
+    fn = getattr(load(), name)
+    with torch.cuda.device(device):
+        check(fn(*args))
+
+
+def query(device, name, *args):
+    """A size query (``*_workspace_size``) answered for ``device``: launch
+    shapes, and so workspace sizes, follow that device's SM count.  Without
+    a CUDA device the library answers for a B200."""
+    fn = getattr(load(), name)
+    device = None if device is None else torch.device(device)
+    if device is None or device.type != 'cuda' or not torch.cuda.is_available():
+        return fn(*args)
+    with torch.cuda.device(device):
+        return fn(*args)
+
+
 def launch_count():
     return int(load().mbir_launch_count())
 

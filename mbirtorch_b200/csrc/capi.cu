@@ -73,6 +73,62 @@ int fail(int code, const char *fmt, ...) {
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Attributes of the current device, cached per device.  Launch shapes and
+// workspace sizes follow the SM count; shared-memory requests are checked
+// against the opt-in limit before a launch.  Without a device to query (a
+// workspace-size query on a host without a GPU) the B200 values stand in.
+constexpr int kMaxDevices = 64;
+struct DevAttrs {
+  int sms = 148;
+  int smem_optin = 227 * 1024;
+};
+std::atomic<int> g_attr_sms[kMaxDevices];
+std::atomic<int> g_attr_smem[kMaxDevices];
+
+DevAttrs device_attrs() {
+  DevAttrs a;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return a;
+  }
+  int sms = g_attr_sms[dev].load(std::memory_order_relaxed);
+  int smem = g_attr_smem[dev].load(std::memory_order_relaxed);
+  if (sms <= 0 || smem <= 0) {
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+            cudaSuccess ||
+        sms <= 0 || smem <= 0) {
+      cudaGetLastError();
+      return a;
+    }
+    g_attr_sms[dev].store(sms, std::memory_order_relaxed);
+    g_attr_smem[dev].store(smem, std::memory_order_relaxed);
+  }
+  a.sms = sms;
+  a.smem_optin = smem;
+  return a;
+}
+
+inline int device_sms() { return device_attrs().sms; }
+
+// Opt a kernel into `smem` bytes of dynamic shared memory (above the 48 KB
+// default), refusing requests beyond the device's per-block limit.
+template <typename K>
+int request_smem(K *k, size_t smem, const char *what) {
+  if (smem <= 48 * 1024) return MBIR_OK;
+  const int limit = device_attrs().smem_optin;
+  if (smem > (size_t)limit)
+    return fail(MBIR_ERR_INVALID, "%s: needs %zu bytes of shared memory per block, above the "
+                "device's %d", what, smem, limit);
+  const cudaError_t e =
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess)
+    return fail(MBIR_ERR_CUDA, "%s: shared memory request of %zu bytes refused: %s", what, smem,
+                cudaGetErrorString(e));
+  return MBIR_OK;
+}
+
 // Programmatic dependent launch inside a VCD step or denoise pass: while a
 // PdlScope is open on this thread, launch() lets each kernel begin as the
 // stream's previous kernel winds down (the kernels open with
@@ -126,6 +182,9 @@ struct Carver {
   }
 };
 
+// Views index grid y (forward projections) and grid z (layout changes).
+constexpr int kMaxViews = 65535;
+
 int validate_geometry(const mbir_geometry *g) {
   if (!g) return fail(MBIR_ERR_INVALID, "geometry is NULL");
   if (g->geometry != MBIR_PARALLEL && g->geometry != MBIR_CONE)
@@ -133,6 +192,9 @@ int validate_geometry(const mbir_geometry *g) {
   if (g->num_views <= 0 || g->num_det_rows <= 0 || g->num_det_channels <= 0 ||
       g->num_recon_rows <= 0 || g->num_recon_cols <= 0 || g->num_slices <= 0)
     return fail(MBIR_ERR_INVALID, "geometry sizes must be positive");
+  if (g->num_views > kMaxViews)
+    return fail(MBIR_ERR_INVALID, "at most %d views per geometry (got %d): split the scan into "
+                "several geometries of consecutive views", kMaxViews, g->num_views);
   if ((long long)g->num_recon_rows * g->num_recon_cols >= (1LL << 31))
     return fail(MBIR_ERR_INVALID, "recon grid too large for 32-bit pixel indices");
   if (g->psf_radius < 0 || g->psf_radius > MBIR_MAX_TAP_RADIUS || g->bp_psf_radius < 0 ||
@@ -187,9 +249,9 @@ BackShape back_shape(const mbir_geometry *g, int view_count, long long P, int ba
   const long long teams = P * s.slice_chunks;
   const int teams_per_block = kThreads / s.T;
   s.blocks_x = (int)((teams + teams_per_block - 1) / teams_per_block);
-  // Enough warps for ~2 full waves of the 148 SMs; split views otherwise.
+  // Enough warps for ~2 full waves of the device's SMs; split views otherwise.
   const long long warps = (teams * s.T + 31) / 32;
-  const long long target = 148LL * 64;
+  const long long target = (long long)device_sms() * 64;
   long long nch = warps >= target ? 1 : (target + warps - 1) / warps;
   nch = std::min<long long>(nch, std::max(1, view_count / 4));
   if (l2_views) {
@@ -221,7 +283,8 @@ int launch_back_t(const Geo &geo, const mbir_geometry *g, const float *vp, int v
   dim3 grid(s.blocks_x, s.nchunks);
   if (g->geometry == MBIR_CONE) {
     auto k = back_cone_kernel<CP, SPL, NT, RD>;
-    if (s.smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    const int rc = request_smem(k, s.smem, what);
+    if (rc) return rc;
     tpre(st);
     launch(k, grid, kThreads, s.smem, st, geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P,
            slice_start, band, s.slice_chunks, dst, recs);
@@ -289,7 +352,7 @@ int run_back(const mbir_geometry *g, const float *vp, int v_start, int v_count, 
   if (rc) return rc;
   if (s.nchunks > 1 && reduce_into_out) {
     const size_t n = (size_t)P * band;
-    const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)device_sms() * 16);
     tpre(st);
     launch(reduce_chunks_kernel, blocks, 256, 0, st, (const float *)partials, s.nchunks, n, out);
     MBIR_CHECK_LAUNCH("chunk reduction");
@@ -319,11 +382,9 @@ int launch_forward(const mbir_geometry *g, const float *vp, int v_start, int v_c
   const Geo geo = make_geo(*g);
   const size_t smem = fs.smem_bytes();
   auto k = forward_kernel<CONE, NT, EPI>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-      return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s", smem,
-                  cudaGetErrorString(e));
+  {
+    const int rc_smem = request_smem(k, smem, "forward");
+    if (rc_smem) return rc_smem;
   }
   dim3 grid((g->num_det_channels + fs.CB - 1) / fs.CB, v_count);
   tpre(st);
@@ -356,11 +417,9 @@ int launch_cone_rt(const mbir_geometry *g, const float *vp, int v_start, int v_c
   const Geo geo = make_geo(*g);
   const size_t smem = cone_rt_smem(g, band);
   auto k = forward_cone_rt_kernel<EPI>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-      return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s", smem,
-                  cudaGetErrorString(e));
+  {
+    const int rc_smem = request_smem(k, smem, "forward");
+    if (rc_smem) return rc_smem;
   }
   dim3 grid((g->num_det_channels + kFwdCB - 1) / kFwdCB, v_count);
   tpre(st);
@@ -413,12 +472,9 @@ int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count
                const int64_t *pix, long long P, const FwdBins &b, cudaStream_t st) {
   const Geo geo = make_geo(*g);
   const size_t smem = bin_smem(g);
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(cone_bin_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-      return fail(MBIR_ERR_CUDA, "forward binning: shared memory request of %zu bytes refused: %s",
-                  smem, cudaGetErrorString(e));
+  {
+    const int rc_smem = request_smem(cone_bin_kernel, smem, "forward binning");
+    if (rc_smem) return rc_smem;
   }
   tpre(st);
   launch(cone_bin_kernel, v_count, kThreads, smem, st, geo, vp, v_start, pix, (int)P, 0, b.recs,
@@ -434,11 +490,9 @@ int launch_binned(const mbir_geometry *g, int v_start, int v_count, const float 
   const Geo geo = make_geo(*g);
   const size_t smem = cone_rt_smem(g, band);
   auto k = forward_cone_binned_kernel<EPI>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-      return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s", smem,
-                  cudaGetErrorString(e));
+  {
+    const int rc_smem = request_smem(k, smem, "forward");
+    if (rc_smem) return rc_smem;
   }
   dim3 grid(fwd_nblk(g), v_count);
   tpre(st);
@@ -461,12 +515,9 @@ int launch_par_binned(const mbir_geometry *g, int v_start, int v_count, const fl
     const int nthr4 = (band / 4 + 31) / 32 * 32;
     const size_t smem4 = par_binned4_smem(nthr4);
     auto k4 = forward_parallel_binned4_kernel<EPI>;
-    if (smem4 > 48 * 1024) {
-      cudaError_t e =
-          cudaFuncSetAttribute(k4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem4);
-      if (e != cudaSuccess)
-        return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s",
-                    smem4, cudaGetErrorString(e));
+    {
+      const int rc_smem = request_smem(k4, smem4, "forward");
+      if (rc_smem) return rc_smem;
     }
     dim3 grid(fwd_nblk(g), v_count);
     tpre(st);
@@ -478,11 +529,9 @@ int launch_par_binned(const mbir_geometry *g, int v_start, int v_count, const fl
   const int nthr = cone_rt_threads(g);
   const size_t smem = par_binned_smem(nthr);
   auto k = forward_parallel_binned_kernel<EPI>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-      return fail(MBIR_ERR_CUDA, "forward: shared memory request of %zu bytes refused: %s", smem,
-                  cudaGetErrorString(e));
+  {
+    const int rc_smem = request_smem(k, smem, "forward");
+    if (rc_smem) return rc_smem;
   }
   dim3 grid(fwd_nblk(g), v_count);
   tpre(st);
@@ -553,7 +602,6 @@ struct VcdWs {
 };
 
 constexpr int kUpdChunk = 16;   // pixels per update tile (two load batches)
-constexpr int kDcChunk = 32;    // pixels per DC-sum chunk
 
 size_t storage_size(int storage) { return storage == MBIR_F32 ? 4 : 2; }
 
@@ -572,7 +620,9 @@ VcdWs vcd_layout(const mbir_geometry *g, long long Ps, const mbir_vcd_params *pr
   w.dc_chunks = (int)((Ps + kDcChunk - 1) / kDcChunk);
   w.dc_sums = c.take<double>((size_t)w.dc_chunks * S * 2);
   w.prior_blocks = (int)((PS + kThreads - 1) / kThreads);
-  w.prior_part = c.take<double>((size_t)w.prior_blocks * 2);
+  // (the damped direction writes one pair per (pixel block, slice block))
+  const size_t dc_dir_ctas = (size_t)((Ps + kDcDirPixels - 1) / kDcDirPixels) * ((S + 31) / 32);
+  w.prior_part = c.take<double>(std::max<size_t>(w.prior_blocks, dc_dir_ctas) * 2);
   w.fwd_blocks = fwd_blocks(g, S, V);
   w.fwd_part = c.take<double>((size_t)w.fwd_blocks * 2);
   w.upd_chunks = (int)((Ps + kUpdChunk - 1) / kUpdChunk);
@@ -631,6 +681,7 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   if (rc) return rc;
   // 2. direction (reduces the chunk slabs in order)
   const int nb = w.prior_blocks;
+  int nprior = nb;  // prior line-term partials the alpha kernel folds
   if (!DCon) {
     tpre(st);
     launch(vcd_direction_kernel<false>, nb, kThreads, 0, st, (int)Ps, S, pix, g->num_recon_rows,
@@ -643,13 +694,16 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
            g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H, sc, nullptr, w.gbuf, w.hinv,
            w.gpbuf, w.hpbuf, nullptr);
     MBIR_CHECK_LAUNCH("vcd direction (damped)");
-    dim3 gs((S + 31) / 32, w.dc_chunks);
+    dim3 gs(w.dc_chunks, (S + 31) / 32);
     tpre(st);
-    launch(vcd_dc_sums_kernel, gs, dim3(32, kDcGroups), 0, st, (int)Ps, S, kDcChunk, w.gbuf, w.hinv, w.dc_sums);
+    launch(vcd_dc_sums_kernel, gs, dim3(32, kDcGroups), 0, st, (int)Ps, S, w.gbuf, w.hinv,
+           w.dc_sums);
     MBIR_CHECK_LAUNCH("vcd DC sums");
+    const dim3 gd((unsigned)((Ps + kDcDirPixels - 1) / kDcDirPixels), (S + 31) / 32);
+    nprior = (int)(gd.x * gd.y);
     tpre(st);
-    launch(vcd_dc_direction_kernel, nb, kThreads, 0, st, (int)Ps, S, w.dc_chunks, w.dc_sums, dc,
-           w.gbuf, w.hinv, w.gpbuf, w.hpbuf, w.delta, w.prior_part);
+    launch(vcd_dc_direction_kernel, gd, dim3(32, 8), 0, st, (int)Ps, S, w.dc_chunks, w.dc_sums,
+           dc, w.gbuf, w.hinv, w.gpbuf, w.hpbuf, w.delta, w.prior_part);
     MBIR_CHECK_LAUNCH("vcd DC direction");
   }
   // 3. forward A delta + line-search partials
@@ -662,7 +716,7 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   if (rc) return rc;
   // 4. alpha
   tpre(st);
-  launch(vcd_alpha_kernel, 1, kAlphaThreads, 0, st, w.prior_part, nb, w.fwd_part, w.fwd_blocks,
+  launch(vcd_alpha_kernel, 1, kAlphaThreads, 0, st, w.prior_part, nprior, w.fwd_part, w.fwd_blocks,
          sc.fmc, sc.max_alpha, w.alpha, alpha_user);
   MBIR_CHECK_LAUNCH("vcd alpha");
   if (prm->positivity) {
@@ -689,12 +743,9 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
                       w.bins.offs};
     const size_t smem = nbin ? bin_smem(g) : 0;
     auto k = vcd_tail_kernel<T>;
-    if (smem > 48 * 1024) {
-      const cudaError_t e =
-          cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess)
-        return fail(MBIR_ERR_CUDA, "VCD update: shared memory request of %zu bytes refused: %s",
-                    smem, cudaGetErrorString(e));
+    {
+      const int rc_smem = request_smem(k, smem, "VCD update");
+      if (rc_smem) return rc_smem;
     }
     // tiles per tile-role CTA: about 4096 cells each
     const int tpc = std::max(1, std::min(nblk, 4096 / (kFwdCB * R)));
@@ -715,7 +766,7 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
          w.alpha, flat, w.sq_part, w.l1_part, w.counters + 1, accum);
   MBIR_CHECK_LAUNCH("vcd pixel update");
   const size_t n = (size_t)V * C * R;
-  const int blocks = (int)std::min<size_t>((n / 4 + 255) / 256 + 1, 148 * 32);
+  const int blocks = (int)std::min<size_t>((n / 4 + 255) / 256 + 1, (size_t)device_sms() * 32);
   tpre(st);
   launch(vcd_sino_update_kernel<T>, blocks, 256, 0, st, n, w.alpha, err,
          static_cast<const T *>(w.ad));
@@ -960,6 +1011,8 @@ int32_t mbir_sino_convert(int32_t direction, int32_t views, int32_t rows, int32_
                           const void *src, void *dst, int32_t dtype, float *scale,
                           int32_t compute_scale, void *stream) {
   if (views <= 0 || rows <= 0 || channels <= 0) return fail(MBIR_ERR_INVALID, "bad sinogram shape");
+  if (views > kMaxViews)
+    return fail(MBIR_ERR_INVALID, "at most %d views per sinogram (got %d)", kMaxViews, views);
   if (!src || !dst || !scale) return fail(MBIR_ERR_INVALID, "NULL array argument");
   if (dtype != MBIR_F32 && dtype != MBIR_BF16 && dtype != MBIR_F16)
     return fail(MBIR_ERR_INVALID, "unknown dtype %d", dtype);
@@ -1005,9 +1058,16 @@ int32_t mbir_sino_convert(int32_t direction, int32_t views, int32_t rows, int32_
   return MBIR_OK;
 }
 
+// Partial-sum blocks of the error-init and statistics reductions: a few
+// per SM, capped so that the workspace size does not depend on the device.
+constexpr int kInitMaxBlocks = 4096;
+constexpr int kStatsMaxBlocks = 2048;
+int init_blocks() { return std::min(kInitMaxBlocks, device_sms() * 8); }
+int stats_blocks() { return std::min(kStatsMaxBlocks, device_sms() * 4); }
+
 size_t mbir_error_init_workspace_size(int64_t count) {
   (void)count;
-  return align_up(sizeof(double) * 2 * 148 * 8) + 256;
+  return align_up(sizeof(double) * 2 * kInitMaxBlocks) + 256;
 }
 
 int32_t mbir_error_init(int64_t count, const float *y, const float *ax, const float *weights,
@@ -1019,7 +1079,7 @@ int32_t mbir_error_init(int64_t count, const float *y, const float *ax, const fl
     return fail(MBIR_ERR_WORKSPACE, "error init needs %zu workspace bytes",
                 mbir_error_init_workspace_size(count));
   cudaStream_t st = as_stream(stream);
-  const int nb = 148 * 8;
+  const int nb = init_blocks();
   double *part = static_cast<double *>(workspace);
   tpre(st);
   init_dots_kernel<<<nb, kThreads, 0, st>>>((size_t)count, y, ax, weights, part);
@@ -1200,7 +1260,7 @@ int32_t mbir_denoise_pass(int32_t num_rows, int32_t num_cols, int32_t num_slices
 }
 
 size_t mbir_iteration_stats_workspace_size(void) {
-  return align_up(sizeof(double) * 3 * 148 * 4) + align_up(sizeof(double) * 148 * 4);
+  return align_up(sizeof(double) * 3 * kStatsMaxBlocks) + align_up(sizeof(double) * kStatsMaxBlocks);
 }
 
 int32_t mbir_iteration_stats(int32_t views, int32_t rows, int32_t channels, const void *error_sino,
@@ -1214,10 +1274,10 @@ int32_t mbir_iteration_stats(int32_t views, int32_t rows, int32_t channels, cons
     return fail(MBIR_ERR_WORKSPACE, "statistics need %zu workspace bytes",
                 mbir_iteration_stats_workspace_size());
   cudaStream_t st = as_stream(stream);
-  const int nb = 148 * 4;
+  const int nb = stats_blocks();
   double *sp = static_cast<double *>(workspace);
   double *lp = reinterpret_cast<double *>(static_cast<char *>(workspace) +
-                                          align_up(sizeof(double) * 3 * nb));
+                                          align_up(sizeof(double) * 3 * kStatsMaxBlocks));
   const int CR = rows * channels;
   switch (storage) {
     case MBIR_F32:
@@ -1265,7 +1325,6 @@ constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;  // 32 MiB
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 namespace {
-constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 void *g_noalloc_ptr[kMaxDevices] = {};
 
@@ -1298,7 +1357,14 @@ extern "C" int32_t mbir_back_project_noalloc(const mbir_geometry *geom,
                                              const int64_t *pixel_indices, int64_t num_pixels,
                                              int32_t coeff_power, int32_t slice_start,
                                              int32_t band_len, float *out, void *stream) {
-  if (geom && sino_layout == MBIR_LAYOUT_VRC && view_count > 0) {
+  // Arguments first, so that a bad size reports itself as such and not as a
+  // scratch overflow.
+  int rc = validate_geometry(geom);
+  if (rc) return rc;
+  if (view_start < 0 || view_count < 0 || view_start + view_count > geom->num_views)
+    return fail(MBIR_ERR_INVALID, "view range [%d, %d) outside [0, %d)", view_start,
+                view_start + view_count, geom->num_views);
+  if (sino_layout == MBIR_LAYOUT_VRC && view_count > 0) {
     const size_t need = align_up((size_t)view_count * geom->num_det_rows *
                                  geom->num_det_channels * sizeof(float));
     if (need > kNoAllocScratchBytes)
@@ -1308,7 +1374,7 @@ extern "C" int32_t mbir_back_project_noalloc(const mbir_geometry *geom,
                   "use mbir_back_project with a workspace", need, kNoAllocScratchBytes);
   }
   void *scratch = nullptr;
-  const int rc = noalloc_scratch(&scratch);
+  rc = noalloc_scratch(&scratch);
   if (rc) return rc;
   return mbir_back_project(geom, view_params, view_start, view_count, sino, sino_layout,
                            pixel_indices, num_pixels, coeff_power, slice_start, band_len, out,

@@ -762,6 +762,7 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
 // channel's sum is a fixed sequence of FMAs in pixel order.
 constexpr int kFwdCB = 16;   // channels per CTA
 constexpr int kFwdEB = 16;   // pixels staged per batch
+static_assert(kFwdEB <= 32, "fwd_rt_batch tests a batch's pixels one per lane");
 constexpr int kFwdVPad = 8;  // zero slices either side of a staged cylinder (>= 2 bp + 1)
 
 // Record capacity of one round (at least one scan chunk); the shared memory
@@ -813,12 +814,49 @@ __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec,
                                              int c0, float *__restrict__ acc_s, int &cj,
                                              float &q0, float &q1, float &q2) {
   const int tid = threadIdx.x, nthr = blockDim.x;
+  // A row m reaches the band only when its centre slice (m - m0) / w_r lies
+  // within [kc_lo, kc_hi], i.e. m in [m0 + w_r kc_lo, m0 + w_r kc_hi]
+  // (widened here by a row either side).  Outside, every tap meets the zero
+  // padding and adds an exact zero, so a warp whose rows [wr0, wr0 + 31] all
+  // lie outside skips the pixel, with the same result.  Lane e tests pixel
+  // e of the batch (nb <= kFwdEB <= 32); bit e of `skip` is the answer.
+  unsigned skip;
+  {
+    const int lane = tid & 31;
+    const float wr0 = (float)(tid - lane), wr1 = wr0 + 31.f;
+    bool out = false;
+    if (lane < nb) {
+      const float4 ra = rec[lane].a;
+      out = fmaf(ra.y, kc_hi, ra.x) + 1.f < wr0 || fmaf(ra.y, kc_lo, ra.x) - 1.f > wr1;
+    }
+    skip = __ballot_sync(__activemask(), out);
+  }
 #pragma unroll 1
   for (int e = 0; e < nb; ++e) {
     const ConeFwdRec *r = rec + e;
     const float4 ra = r->a, rb = r->b;
     const int j = __float_as_int(r->c.z) - c0 + 1;  // in [0, kFwdCB + 1]
     const float m0 = ra.x, w_r = ra.y, hw1r = ra.z, lmaxr = ra.w;
+    if (SORTED && j != cj) {  // uniform over the CTA; j > cj
+      float *a = acc_s + cj * nthr + tid;
+      a[0] += q0;
+      if (j == cj + 1) {
+        q0 = q1;
+        q1 = q2;
+      } else {
+        a[nthr] += q1;
+        if (j == cj + 2) {
+          q0 = q2;
+        } else {
+          a[2 * nthr] += q2;
+          q0 = 0.f;
+        }
+        q1 = 0.f;
+      }
+      q2 = 0.f;
+      cj = j;
+    }
+    if ((skip >> e) & 1u) continue;  // uniform over the warp
     const float k_m = (mf - m0) * rb.x;
     const float kc = fminf(fmaxf(rintf(k_m), kc_lo), kc_hi);
     const float d = w_r * (kc - k_m);
@@ -839,25 +877,6 @@ __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec,
     // Thread-private accumulator column in shared memory: row r holds
     // channel c0 + r - 2, so tap t of centre slot j lands on row j + t.
     if (SORTED) {
-      if (j != cj) {  // uniform over the CTA; j > cj
-        float *a = acc_s + cj * nthr + tid;
-        a[0] += q0;
-        if (j == cj + 1) {
-          q0 = q1;
-          q1 = q2;
-        } else {
-          a[nthr] += q1;
-          if (j == cj + 2) {
-            q0 = q2;
-          } else {
-            a[2 * nthr] += q2;
-            q0 = 0.f;
-          }
-          q1 = 0.f;
-        }
-        q2 = 0.f;
-        cj = j;
-      }
       q0 = fmaf(rb.y, det, q0);
       q1 = fmaf(rb.z, det, q1);
       q2 = fmaf(rb.w, det, q2);

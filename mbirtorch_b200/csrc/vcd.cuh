@@ -184,21 +184,25 @@ vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int 
 
 // ── 2'. DC damping ───────────────────────────────────────────────────────
 // Per-slice sums over pixel chunks: part[chunk][l] = (sum h^-1 g, sum h^-1).
-// A CTA of (32 slices, 8 groups) covers one chunk of pchunk <= 32 pixels:
+// A CTA of (32 slices, 8 groups) covers one chunk of kDcChunk pixels:
 // group y sums the pixels y, y + 8, ... of the chunk with all its loads in
-// flight, then the 8 group sums fold in a fixed order.
+// flight, then the 8 group sums fold in a fixed order.  The pixel chunks run
+// along grid x (up to 2^31 - 1 of them), the 32-slice blocks along grid y.
 constexpr int kDcGroups = 8;
+constexpr int kDcPerGroup = 4;                       // pixels per group
+constexpr int kDcChunk = kDcGroups * kDcPerGroup;    // pixels per chunk
+static_assert(kDcChunk == 32, "one DC-sum CTA covers 32 pixels");
 
 __global__ void __launch_bounds__(32 * kDcGroups)
-vcd_dc_sums_kernel(int P, int S, int pchunk, const float *__restrict__ gbuf,
+vcd_dc_sums_kernel(int P, int S, const float *__restrict__ gbuf,
                    const float *__restrict__ hinv, double *__restrict__ part) {
   MBIR_PDL_ENTRY();
   __shared__ double s_num[kDcGroups][32], s_den[kDcGroups][32];
-  constexpr int U = 32 / kDcGroups;  // pixels per group (pchunk <= 32)
+  constexpr int U = kDcPerGroup;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int l = blockIdx.x * 32 + tx;
-  const int chunk = blockIdx.y;
-  const int p0 = chunk * pchunk, p1 = min(P, p0 + pchunk);
+  const int l = blockIdx.y * 32 + tx;
+  const int chunk = blockIdx.x;
+  const int p0 = chunk * kDcChunk, p1 = min(P, p0 + kDcChunk);
   double num = 0.0, den = 0.0;
   if (l < S) {
     float hv[U], gv[U];
@@ -233,36 +237,80 @@ vcd_dc_sums_kernel(int P, int S, int pchunk, const float *__restrict__ gbuf,
 }
 
 // delta = -(g - (1 - s_l) * gbar_l) * h^-1, plus the prior line-term partials.
-__global__ void __launch_bounds__(kThreads)
+// A CTA of (32 slices, 8 rows) owns slices [32 y, 32 y + 32) of the pixels
+// [kDcDirPixels x, kDcDirPixels (x + 1)): it folds its slices' chunk sums
+// once (row r takes the chunks r, r + 8, ...; the 8 row sums fold in a fixed
+// order), then row r updates the pixels r, r + 8, ... of its block.  The
+// CTA's prior partials go to slot y * gridDim.x + x.
+constexpr int kDcDirPixels = 64;
+
+__global__ void __launch_bounds__(256)
 vcd_dc_direction_kernel(int P, int S, int nchunks, const double *__restrict__ sums,
                         const float *__restrict__ s_prof, const float *__restrict__ gbuf,
                         const float *__restrict__ hinv, const float *__restrict__ gpbuf,
                         const float *__restrict__ hpbuf, float *__restrict__ delta,
                         double *__restrict__ partials) {
   MBIR_PDL_ENTRY();
-  const size_t n = (size_t)P * S;
-  const size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x;
-  double pl = 0.0, pq = 0.0;
-  if (i < n) {
-    const int l = (int)(i % S);
-    double num = 0.0, den = 0.0;
-#pragma unroll 8
-    for (int c = 0; c < nchunks; ++c) {
+  __shared__ double s_a[8][32], s_b[8][32];
+  __shared__ float s_fac[32];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int l = blockIdx.y * 32 + tx;
+  double num = 0.0, den = 0.0;
+  if (l < S) {
+    for (int c = ty; c < nchunks; c += 8) {
       num += sums[((size_t)c * S + l) * 2];
       den += sums[((size_t)c * S + l) * 2 + 1];
     }
-    const float gbar = (float)(num / den);
-    const float damp = __fmul_rn(__fsub_rn(1.f, s_prof[l]), gbar);
-    const float dl = __fmul_rn(-__fsub_rn(gbuf[i], damp), hinv[i]);
-    delta[i] = dl;
-    const float g_p = gpbuf[i], h_p = hpbuf[i];
-    pl = (double)__fmul_rn(g_p, dl);
-    pq = (double)__fmul_rn(__fmul_rn(h_p, dl), dl);
   }
-  block_sum2(pl, pq);
-  if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = pl;
-    partials[2 * blockIdx.x + 1] = pq;
+  s_a[ty][tx] = num;
+  s_b[ty][tx] = den;
+  __syncthreads();
+  if (ty == 0) {
+    double a = 0.0, b = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      a += s_a[k][tx];
+      b += s_b[k][tx];
+    }
+    // (1 - s_l) * gbar_l, gbar_l = sum h^-1 g / sum h^-1
+    s_fac[tx] = l < S ? __fmul_rn(__fsub_rn(1.f, s_prof[l]), (float)(a / b)) : 0.f;
+  }
+  __syncthreads();
+  double pl = 0.0, pq = 0.0;
+  if (l < S) {
+    const float damp = s_fac[tx];
+    const int p1 = min(P, (int)(blockIdx.x + 1) * kDcDirPixels);
+    for (int p = blockIdx.x * kDcDirPixels + ty; p < p1; p += 8) {
+      const size_t i = (size_t)p * S + l;
+      const float dl = __fmul_rn(-__fsub_rn(gbuf[i], damp), hinv[i]);
+      delta[i] = dl;
+      const float g_p = gpbuf[i], h_p = hpbuf[i];
+      pl += (double)__fmul_rn(g_p, dl);
+      pq += (double)__fmul_rn(__fmul_rn(h_p, dl), dl);
+    }
+  }
+  // fixed-order CTA reduction: the 8 rows of each slice lane, then the lanes
+  __syncthreads();
+  s_a[ty][tx] = pl;
+  s_b[ty][tx] = pq;
+  __syncthreads();
+  if (ty == 0) {
+    double a = 0.0, b = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      a += s_a[k][tx];
+      b += s_b[k][tx];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if (tx == 0) {
+      const size_t slot = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+      partials[2 * slot] = a;
+      partials[2 * slot + 1] = b;
+    }
   }
 }
 
@@ -337,6 +385,8 @@ struct LineSearchEpi {
   // A row's cells at channels c0 .. c0 + ncb - 1 at once: every load of e
   // and w goes out before the first store of Ad, which the compiler could
   // not otherwise move past (the pointers may alias as far as it knows).
+  // The row's products are summed in FP32 (at most N terms, in channel
+  // order) and added to the FP64 sums once per row.
   template <int N>
   __device__ __forceinline__ void cells(int v, int c0, int ncb, int m, const float (&acc)[N]) {
     const size_t i0 = ((size_t)v * C + c0) * R + m;
@@ -350,6 +400,7 @@ struct LineSearchEpi {
         if (w != nullptr) wv[j] = to_f32(w[i0 + (size_t)j * R]);
       }
     }
+    float rl = 0.f, rq = 0.f;
 #pragma unroll
     for (int j = 0; j < N; ++j) {
       if (j < ncb) {
@@ -360,15 +411,17 @@ struct LineSearchEpi {
           const float evs = __fmul_rn(ev[j], scale);
           if (w != nullptr) {
             const float wvs = __fmul_rn(wv[j], wscale);
-            fl += (double)__fmul_rn(__fmul_rn(wvs, evs), adv);
-            fq += (double)__fmul_rn(__fmul_rn(adv, adv), wvs);
+            rl = __fadd_rn(rl, __fmul_rn(__fmul_rn(wvs, evs), adv));
+            rq = __fadd_rn(rq, __fmul_rn(__fmul_rn(adv, adv), wvs));
           } else {
-            fl += (double)__fmul_rn(evs, adv);
-            fq += (double)__fmul_rn(adv, adv);
+            rl = __fadd_rn(rl, __fmul_rn(evs, adv));
+            rq = __fadd_rn(rq, __fmul_rn(adv, adv));
           }
         }
       }
     }
+    fl += (double)rl;
+    fq += (double)rq;
   }
   // Four consecutive rows m0 .. m0 + 3 of channels c0 .. c0 + ncb - 1 (R and
   // m0 multiples of 4, so each channel's four cells are one aligned 16-byte

@@ -22,7 +22,7 @@ import torch
 
 from . import _lib, vcd_utils
 from . import qggmrf as _qggmrf
-from ._lib import check, ptr, require_cuda, stream_of
+from ._lib import ptr, require_cuda, stream_of
 from ._utils import recon_param_names
 from .tomography_model import TomographyModel
 from .vcd_engine import make_vcd_params
@@ -165,9 +165,8 @@ class QGGMRFDenoiser(TomographyModel):
         flat_err = (image_t.reshape(-1, S) - flat).contiguous()
         require_cuda(flat, flat_err, partition)
         K, n = partition.shape
-        lib = _lib.load()
-        ws = torch.empty(int(lib.mbir_denoise_workspace_size(S, n)), dtype=torch.uint8,
-                         device=flat.device)
+        ws = torch.empty(int(_lib.query(flat.device, 'mbir_denoise_workspace_size', S, n)),
+                         dtype=torch.uint8, device=flat.device)
         accum = torch.zeros(2, dtype=torch.float64, device=flat.device)
         host = torch.empty(3, dtype=torch.float64, pin_memory=True)
         nmae_update = np.zeros(max_iterations)
@@ -177,10 +176,9 @@ class QGGMRFDenoiser(TomographyModel):
         with torch.no_grad():
             for i in range(max_iterations):
                 accum.zero_()
-                check(lib.mbir_denoise_pass(
-                    int(image_shape[0]), int(image_shape[1]), S, prm, ptr(flat), ptr(flat_err),
-                    ptr(partition), K, n, ptr(accum), ptr(ws), ws.numel(),
-                    stream_of(flat.device)))
+                _lib.call(flat.device, 'mbir_denoise_pass', int(image_shape[0]),
+                          int(image_shape[1]), S, prm, ptr(flat), ptr(flat_err), ptr(partition),
+                          K, n, ptr(accum), ptr(ws), ws.numel(), stream_of(flat.device))
                 l1 = torch.sum(torch.abs(flat)).to(torch.float64)
                 host.copy_(torch.cat([accum, l1.reshape(1)]), non_blocking=True)
                 torch.cuda.current_stream(flat.device).synchronize()

@@ -22,7 +22,7 @@ import torch
 
 from . import _lib
 from ._lib import (MBIR_CONE, MBIR_LAYOUT_VCR, MBIR_LAYOUT_VRC, MBIR_PARALLEL, Geometry,
-                   as_f32_contig, as_i64_contig, check, ptr, require_cuda, stream_of)
+                   as_f32_contig, as_i64_contig, ptr, require_cuda, stream_of)
 
 
 def make_geometry(kind, num_views, num_det_rows, num_det_channels, num_recon_rows,
@@ -79,10 +79,9 @@ class DeviceProjector:
                  else (vc, g.num_det_channels, g.num_det_rows))
         if out is None:
             out = torch.empty(shape, dtype=torch.float32, device=values.device)
-        lib = _lib.load()
-        check(lib.mbir_forward_project(g, ptr(self.view_params), view_start, vc, ptr(values),
-                                       idx.shape[0], L, slice_start, ptr(idx), ptr(out), layout,
-                                       stream_of(values.device)))
+        _lib.call(values.device, 'mbir_forward_project', g, ptr(self.view_params), view_start,
+                  vc, ptr(values), idx.shape[0], L, slice_start, ptr(idx), ptr(out), layout,
+                  stream_of(values.device))
         return out
 
     def forward_volume(self, flat_volume, pixel_indices, layout=MBIR_LAYOUT_VRC, out=None):
@@ -99,9 +98,9 @@ class DeviceProjector:
                  else (g.num_views, g.num_det_channels, g.num_det_rows))
         if out is None:
             out = torch.empty(shape, dtype=torch.float32, device=flat.device)
-        check(_lib.load().mbir_forward_project_volume(
-            g, ptr(self.view_params), 0, g.num_views, ptr(flat), ptr(idx), idx.shape[0],
-            ptr(out), layout, stream_of(flat.device)))
+        _lib.call(flat.device, 'mbir_forward_project_volume', g, ptr(self.view_params), 0,
+                  g.num_views, ptr(flat), ptr(idx), idx.shape[0], ptr(out), layout,
+                  stream_of(flat.device))
         return out
 
     def back(self, sino, pixel_indices, coeff_power=1, slice_start=0, band_slices=None,
@@ -114,13 +113,12 @@ class DeviceProjector:
         vc = sino.shape[0]
         band = g.num_slices - slice_start if band_slices is None else int(band_slices)
         out = torch.empty((idx.shape[0], band), dtype=torch.float32, device=sino.device)
-        lib = _lib.load()
-        nbytes = lib.mbir_back_project_workspace_size(g, vc, idx.shape[0], band)
+        nbytes = _lib.query(sino.device, 'mbir_back_project_workspace_size', g, vc,
+                            idx.shape[0], band)
         ws = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=sino.device)
-        check(lib.mbir_back_project(g, ptr(self.view_params), view_start, vc, ptr(sino), layout,
-                                    ptr(idx), idx.shape[0], int(coeff_power), int(slice_start),
-                                    band, ptr(out), ptr(ws), ws.numel(),
-                                    stream_of(sino.device)))
+        _lib.call(sino.device, 'mbir_back_project', g, ptr(self.view_params), view_start, vc,
+                  ptr(sino), layout, ptr(idx), idx.shape[0], int(coeff_power), int(slice_start),
+                  band, ptr(out), ptr(ws), ws.numel(), stream_of(sino.device))
         return out
 
 

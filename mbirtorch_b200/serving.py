@@ -70,8 +70,8 @@ class MemoryLedger:
         code = storage_code(storage_dtype)
         s = 4 if code == _lib.MBIR_F32 else 2
         prm = make_vcd_params(1.0, 1.0, 2.0, 1.2, 1.0, [1 / 6] * 6, 1.5, False, code)
-        ws = int(_lib.load().mbir_vcd_workspace_size(model._geometry(), int(max_subset_pixels),
-                                                     prm))
+        ws = int(_lib.query(getattr(model, 'torch_device', None), 'mbir_vcd_workspace_size',
+                            model._geometry(), int(max_subset_pixels), prm))
         y = 4 * n_sino if code != _lib.MBIR_F32 else 0
         resident = y + (2 if weighted else 1) * s * n_sino + ws + 8 * n_vol
         init = 4 * 4 * n_sino + 3 * 4 * n_vol + y + (4 * n_sino if weighted else 0)

@@ -20,8 +20,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import (STORAGE_CODES, STORAGE_DTYPES, VcdParams, check, host_int32, ptr,
-                   require_cuda, stream_of)
+from ._lib import (STORAGE_CODES, STORAGE_DTYPES, VcdParams, host_int32, ptr, require_cuda,
+                   stream_of)
 
 
 def storage_code(storage_dtype):
@@ -53,8 +53,8 @@ class ResidentSinogram:
         V, R, C = sino.shape
         data = torch.empty((V, C, R), dtype=STORAGE_DTYPES[storage], device=sino.device)
         scale = torch.empty(V, dtype=torch.float32, device=sino.device)
-        check(_lib.load().mbir_sino_convert(0, V, R, C, ptr(sino), ptr(data), storage,
-                                            ptr(scale), 1, stream_of(sino.device)))
+        _lib.call(sino.device, 'mbir_sino_convert', 0, V, R, C, ptr(sino), ptr(data), storage,
+                  ptr(scale), 1, stream_of(sino.device))
         return cls(data, scale, R, storage)
 
     @property
@@ -69,8 +69,8 @@ class ResidentSinogram:
     def to_vrc(self):
         V, C, R = self.data.shape
         out = torch.empty((V, R, C), dtype=torch.float32, device=self.data.device)
-        check(_lib.load().mbir_sino_convert(1, V, R, C, ptr(self.data), ptr(out), self.storage,
-                                            ptr(self.scale), 0, stream_of(self.data.device)))
+        _lib.call(self.data.device, 'mbir_sino_convert', 1, V, R, C, ptr(self.data), ptr(out),
+                  self.storage, ptr(self.scale), 0, stream_of(self.data.device))
         return out
 
     def nbytes(self):
@@ -118,7 +118,8 @@ class VcdEngine:
     def reserve(self, max_subset_pixels):
         if max_subset_pixels <= self._ws_pixels:
             return
-        n = _lib.load().mbir_vcd_workspace_size(self.geom, int(max_subset_pixels), self.params)
+        n = _lib.query(self.device, 'mbir_vcd_workspace_size', self.geom,
+                       int(max_subset_pixels), self.params)
         self._ws = torch.empty(int(n), dtype=torch.uint8, device=self.device)
         self._ws_pixels = int(max_subset_pixels)
 
@@ -140,10 +141,10 @@ class VcdEngine:
         self.reserve(idx.shape[0])
         acc = torch.zeros(2 + self.num_slices, dtype=torch.float64, device=self.device)
         e, es, w, wsc = self._common(err)
-        check(_lib.load().mbir_vcd_subset_update(
-            self.geom, ptr(self.view_params), self.params, ptr(flat_recon), e, es, w, wsc,
-            ptr(self.H), ptr(self.dc), ptr(idx), idx.shape[0], ptr(acc), ptr(self.alpha_buf),
-            ptr(self._ws), self._ws.numel(), stream_of(self.device)))
+        _lib.call(self.device, 'mbir_vcd_subset_update', self.geom, ptr(self.view_params),
+                  self.params, ptr(flat_recon), e, es, w, wsc, ptr(self.H), ptr(self.dc),
+                  ptr(idx), idx.shape[0], ptr(acc), ptr(self.alpha_buf), ptr(self._ws),
+                  self._ws.numel(), stream_of(self.device))
         return acc[0], self.alpha_buf[0].clone(), acc[2:]
 
     def partition_pass(self, flat_recon, err, partition, order, accum=None):
@@ -156,10 +157,10 @@ class VcdEngine:
         accum = self.accum if accum is None else accum
         order_np, order_p = host_int32(order)
         e, es, w, wsc = self._common(err)
-        check(_lib.load().mbir_vcd_partition_pass(
-            self.geom, ptr(self.view_params), self.params, ptr(flat_recon), e, es, w, wsc,
-            ptr(self.H), ptr(self.dc), ptr(part), K, n, order_p, ptr(accum), ptr(self._ws),
-            self._ws.numel(), stream_of(self.device)))
+        _lib.call(self.device, 'mbir_vcd_partition_pass', self.geom, ptr(self.view_params),
+                  self.params, ptr(flat_recon), e, es, w, wsc, ptr(self.H), ptr(self.dc),
+                  ptr(part), K, n, order_p, ptr(accum), ptr(self._ws), self._ws.numel(),
+                  stream_of(self.device))
         del order_np
         return accum
 
@@ -167,9 +168,9 @@ class VcdEngine:
 def _refresh(engine, flat_recon, err, pixel_indices, y_vcr):
     idx = _lib.as_i64_contig(pixel_indices)
     require_cuda(flat_recon, idx, y_vcr)
-    check(_lib.load().mbir_vcd_refresh_error(
-        engine.geom, ptr(engine.view_params), ptr(flat_recon), ptr(idx), idx.shape[0],
-        ptr(y_vcr), ptr(err.data), ptr(err.scale), err.storage, stream_of(engine.device)))
+    _lib.call(engine.device, 'mbir_vcd_refresh_error', engine.geom, ptr(engine.view_params),
+              ptr(flat_recon), ptr(idx), idx.shape[0], ptr(y_vcr), ptr(err.data),
+              ptr(err.scale), err.storage, stream_of(engine.device))
 
 
 VcdEngine.refresh_error = _refresh
@@ -180,14 +181,13 @@ VcdEngine.refresh_error.__doc__ = (
 def iteration_stats(err, weights, flat_recon):
     """FP64 [sum w e^2, sum w, sum e^2, sum |x|] as a device tensor."""
     V, C, R = err.data.shape
-    lib = _lib.load()
     out = torch.empty(4, dtype=torch.float64, device=err.device)
-    ws = torch.empty(int(lib.mbir_iteration_stats_workspace_size()), dtype=torch.uint8,
-                     device=err.device)
-    check(lib.mbir_iteration_stats(
-        V, R, C, ptr(err.data), ptr(err.scale), None if weights is None else ptr(weights.data),
-        None if weights is None else ptr(weights.scale), err.storage, ptr(flat_recon),
-        flat_recon.numel(), ptr(out), ptr(ws), ws.numel(), stream_of(err.device)))
+    ws = torch.empty(int(_lib.query(err.device, 'mbir_iteration_stats_workspace_size')),
+                     dtype=torch.uint8, device=err.device)
+    _lib.call(err.device, 'mbir_iteration_stats', V, R, C, ptr(err.data), ptr(err.scale),
+              None if weights is None else ptr(weights.data),
+              None if weights is None else ptr(weights.scale), err.storage, ptr(flat_recon),
+              flat_recon.numel(), ptr(out), ptr(ws), ws.numel(), stream_of(err.device))
     return out
 
 
@@ -198,13 +198,13 @@ def error_init(y, ax, weights, scale_to_data):
     ax = _lib.as_f32_contig(ax)
     w = None if weights is None else _lib.as_f32_contig(weights)
     require_cuda(y, ax, w)
-    lib = _lib.load()
     err = torch.empty_like(y)
     alpha = torch.empty(1, dtype=torch.float64, device=y.device)
-    ws = torch.empty(int(lib.mbir_error_init_workspace_size(y.numel())), dtype=torch.uint8,
-                     device=y.device)
-    check(lib.mbir_error_init(y.numel(), ptr(y), ptr(ax), ptr(w), int(bool(scale_to_data)),
-                              ptr(err), ptr(alpha), ptr(ws), ws.numel(), stream_of(y.device)))
+    ws = torch.empty(int(_lib.query(y.device, 'mbir_error_init_workspace_size', y.numel())),
+                     dtype=torch.uint8, device=y.device)
+    _lib.call(y.device, 'mbir_error_init', y.numel(), ptr(y), ptr(ax), ptr(w),
+              int(bool(scale_to_data)), ptr(err), ptr(alpha), ptr(ws), ws.numel(),
+              stream_of(y.device))
     return err, alpha
 
 

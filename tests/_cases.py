@@ -90,3 +90,25 @@ def build_model(d, **extra):
     if spec['set_params']:
         m.set_params(no_warning=True, **spec['set_params'])
     return m
+
+
+def oracle_problem(m):
+    """The oracle's view of an mbirtorch_b200 model: same geometry scalars,
+    view parameters and recon shape."""
+    from oracle import OracleGeometry, vcd
+    g = m._geometry()
+    og = OracleGeometry(
+        num_det_rows=g.num_det_rows, num_det_channels=g.num_det_channels,
+        num_recon_rows=g.num_recon_rows, num_recon_cols=g.num_recon_cols,
+        num_slices=g.num_slices, delta_det_channel=g.delta_det_channel,
+        delta_det_row=g.delta_det_row, det_channel_offset=g.det_channel_offset,
+        det_row_offset=g.det_row_offset, delta_voxel=g.delta_voxel,
+        delta_voxel_row=g.delta_voxel_row, delta_voxel_slice=g.delta_voxel_slice,
+        recon_slice_offset=g.recon_slice_offset, magnification=g.magnification,
+        source_detector_dist=g.source_detector_dist,
+        use_curved_detector=bool(g.use_curved_detector), psf_radius=g.psf_radius,
+        bp_psf_radius=g.bp_psf_radius)
+    kind = 'cone' if g.geometry == 1 else 'parallel'
+    return vcd.Problem(kind, og, m._view_params_array(), m.get_params('recon_shape'),
+                       source_iso_dist=m.get_params('source_iso_dist') if kind == 'cone'
+                       else None)

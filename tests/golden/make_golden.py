@@ -1,9 +1,10 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container where the reference package (mbirtorch 0.0.2) is
-importable, e.g.:
+Run where the reference package (mbirtorch 0.0.2) source tree is at hand,
+naming its directory in MBIRTORCH_REFERENCE:
 
-    PYTHONPATH=/root/reference python tests/golden/make_golden.py
+    MBIRTORCH_REFERENCE=<path to the mbirtorch checkout> \
+        python tests/golden/make_golden.py
 
 The script calls the reference's OWN torch bodies and public methods on
 small seeded inputs (CPU, compile_mode='off') and stores inputs and outputs
@@ -24,9 +25,14 @@ Cases
                     (automatic sigma_prox) and cone (given sigma_prox)
   denoise.npz       QGGMRFDenoiser: noise estimate and seeded denoise runs
                     (given and estimated sigma_noise)
+  recon_simple_parallel_128.npz
+                    the one-call parallel recon at the reference's CPU
+                    configuration: a 128 x 128 x 16 ellipsoid phantom, 180
+                    views on [0, pi), 16 x 192 detector, Gaussian noise at 1%
+                    of the largest projection, 10 VCD iterations
 
 Pass case-function names to regenerate only those, e.g.
-    PYTHONPATH=/root/reference python tests/golden/make_golden.py prox_cases
+    MBIRTORCH_REFERENCE=... python tests/golden/make_golden.py prox_cases
 """
 
 import json
@@ -37,7 +43,9 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("MBIRTORCH_REFERENCE", "/root/reference")
+REF = os.environ.get("MBIRTORCH_REFERENCE")
+if not REF:
+    sys.exit("set MBIRTORCH_REFERENCE to the directory of the mbirtorch 0.0.2 checkout")
 if REF not in sys.path:
     sys.path.insert(0, REF)
 
@@ -382,8 +390,44 @@ def denoise_case():
     print('wrote denoise')
 
 
+def recon_simple_parallel_case():
+    """recon_simple_parallel at the reference's CPU configuration.  The
+    phantom (128 x 128 x 16, unit voxels) is projected by a model of that
+    recon shape; the one-call recon then runs at its default grid."""
+    shape = (180, 16, 192)
+    ang = np.linspace(0, np.pi, shape[0], endpoint=False)
+    mp = _quiet(mbirtorch.ParallelBeamModel(shape, ang, compile_mode='off'))
+    mp.set_params(no_warning=True, recon_shape=(128, 128, 16))
+    ph = phantom((128, 128, 16), 61)
+    clean = mp.forward_project(ph)
+    rng = np.random.default_rng(62)
+    sino = (clean + rng.normal(0, 0.01 * clean.max(), clean.shape)).astype(np.float32)
+    # the data are rounded to float16 values (stored as float32 here), so the
+    # fixture can hold them in half the bytes and still reproduce the input
+    sino = sino.astype(np.float16).astype(np.float32)
+    np.random.seed(63)
+    import time
+    t = time.perf_counter()
+    rec, d = mbirtorch.recon_simple_parallel(sino, ang, max_iterations=10)
+    secs = time.perf_counter() - t
+    rp = d['recon_params']
+    mask = vcd_utils.get_2d_ror_mask(rec.shape[:2]).astype(bool)
+    np.savez_compressed(os.path.join(HERE, 'recon_simple_parallel_128.npz'),
+                        sino_f16=sino.astype(np.float16), angles=ang,
+                        recon_shape=np.array(rec.shape),
+                        recon_ror=rec[mask].astype(np.float32),
+                        fm_rmse=np.array(rp['fm_rmse']), alpha=np.array(rp['alpha_values']),
+                        num_iterations=np.array(rp['num_iterations']),
+                        reg=np.array([rp['regularization_params'][k]
+                                      for k in ('sigma_y', 'sigma_x', 'sigma_prox')]),
+                        seed=np.array(63), max_iterations=np.array(10),
+                        reference_cpu_seconds=np.array(secs),
+                        reference_cpu_threads=np.array(torch.get_num_threads()))
+    print(f'wrote recon_simple_parallel_128 ({secs:.1f} s on the CPU)')
+
+
 CASES = ['projector_cases', 'qggmrf_case', 'partition_case', 'autoreg_and_direct_cases',
-         'recon_cases', 'prox_cases', 'denoise_case']
+         'recon_cases', 'prox_cases', 'denoise_case', 'recon_simple_parallel_case']
 
 if __name__ == '__main__':
     for name in (sys.argv[1:] or CASES):
