@@ -81,7 +81,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip every extra measurement (headline value and e2e only)")
     ap.add_argument("--only-extra", default=None,
-                    help="run one extra by name after the headline (e.g. triton_reference)")
+                    help="run only these extras (comma-separated names, e.g. "
+                         "triton_reference,mixed_precision) after the headline")
     ap.add_argument("--profile-case", choices=["recon", "subset", "projectors",
                                                "subset-parallel", "subset-cone64",
                                                "subset-small"], default=None,
@@ -1024,7 +1025,7 @@ def extras(args, m, mb, torch, dev, y, rec_ref, full=True):
     except Exception:
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    want = set(EXTRAS) if args.only_extra is None else {args.only_extra}
+    want = set(EXTRAS) if args.only_extra is None else set(args.only_extra.split(","))
 
     def run(name, fn):
         if name not in want:

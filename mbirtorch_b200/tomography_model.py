@@ -87,6 +87,9 @@ class TomographyModel(ParameterHandler):
         # keeps the drift of in-place updates below the quantization error
         # over 5 iterations; every iteration for bfloat16 (8 bits).
         self.error_refresh_interval = None
+        # bfloat16 storage: the last iterations run with the error sinogram
+        # re-formed in float16 (same bytes, 3 more significand bits)
+        self.bf16_finish_iterations = 3
         self._torch_device = None
         self._projector = None
         self._full_indices_cache = None

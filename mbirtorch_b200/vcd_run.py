@@ -105,7 +105,7 @@ class VcdRun:
         sino = None if self.init_error_sinogram is not None else m._sino_device(self.sinogram)
         refresh = m.error_refresh_interval
         if refresh is None:
-            refresh = {_lib.MBIR_F32: 0, _lib.MBIR_F16: 5, _lib.MBIR_BF16: 1}[self.storage]
+            refresh = {_lib.MBIR_F32: 0, _lib.MBIR_F16: 5, _lib.MBIR_BF16: 5}[self.storage]
         self.refresh = refresh
         self.y_vcr = None
         if refresh and sino is not None:
@@ -160,8 +160,46 @@ class VcdRun:
                                      prox_flat=self.prox_flat)
         self.host = torch.empty(2 + self.recon_shape[2] + 4, dtype=torch.float64,
                                 pin_memory=True)
+        self._set_finish()
         self._graph_setup()
         log.info('Starting VCD iterations')
+
+    # ── the float16 finish of a bfloat16 run ─────────────────────────────
+    def _set_finish(self):
+        """Iteration at which a bfloat16 run re-forms its error sinogram in
+        float16 (None: no switch).  bfloat16's 8-bit significand quantizes
+        e to about 2^-9 of its size; the last iterations' updates carry that
+        noise into the volume.  Re-forming e = y - A x in float16 (an 11-bit
+        significand with power-of-two per-view scales, the same two bytes a
+        cell) for the last ``model.bf16_finish_iterations`` iterations
+        removes most of it."""
+        self.finish_at = None
+        k = int(getattr(self.model, 'bf16_finish_iterations', 0) or 0)
+        if self.storage == _lib.MBIR_BF16 and self.y_vcr is not None and k > 0:
+            self.finish_at = max(self.done, len(self.seq) - k)
+
+    def _finish_in_float16(self):
+        m = self.model
+        V, R, C = self.sinogram_shape
+        dev = m.torch_device
+        m.logger.info('Re-forming the error sinogram in float16 for the last {} iterations'
+                      .format(len(self.seq) - self.done))
+        e32 = ResidentSinogram(torch.empty((V, C, R), dtype=torch.float32, device=dev),
+                               torch.ones(V, dtype=torch.float32, device=dev), R, _lib.MBIR_F32)
+        self.engine.refresh_error(self.flat, e32, m.full_indices_device(), self.y_vcr)
+        e_vrc = e32.to_vrc()
+        del e32
+        self.err = ResidentSinogram.from_vrc(e_vrc, _lib.MBIR_F16)
+        del e_vrc
+        if self.w_res is not None:
+            self.w_res = ResidentSinogram.from_vrc(self.w_res.to_vrc(), _lib.MBIR_F16)
+        self.storage = _lib.MBIR_F16
+        H = self.fm_hessian.reshape(-1, self.fm_hessian.shape[-1]).contiguous()
+        self.engine = m._make_engine(H, self.w_res, self.storage,
+                                     max_subset_pixels=self.engine._ws_pixels,
+                                     prox_flat=self.prox_flat)
+        self.release_graphs()
+        self.finish_at = None
 
     def _graph_setup(self):
         """Pick the pass shapes worth a graph -- those used at least twice
@@ -226,6 +264,8 @@ class VcdRun:
             raise RuntimeError('no iteration can be enqueued now')
         i = self.done
         with torch.cuda.stream(self.stream):
+            if self.finish_at is not None and i >= self.finish_at:
+                self._finish_in_float16()
             part = self.parts_dev[int(self.seq[i])]
             order = order_array(part.shape[0], self.rng)
             self.engine.accum.zero_()
@@ -434,6 +474,7 @@ class VcdRun:
                                             prox_flat=run.prox_flat)
             run.host = torch.empty(2 + run.recon_shape[2] + 4, dtype=torch.float64,
                                    pin_memory=True)
+            run._set_finish()
             run._graph_setup()
         return run
 
