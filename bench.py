@@ -83,6 +83,9 @@ def parse():
     ap.add_argument("--only-extra", default=None,
                     help="run only these extras (comma-separated names, e.g. "
                          "triton_reference,mixed_precision) after the headline")
+    ap.add_argument("--serving-config5", action="store_true",
+                    help="run the serving configuration (200 Poisson arrivals) against "
+                         "sequential plain FP32 solves and print its JSON (minutes)")
     ap.add_argument("--profile-case", choices=["recon", "subset", "projectors",
                                                "subset-parallel", "subset-cone64",
                                                "subset-small"], default=None,
@@ -825,6 +828,142 @@ def serving_mix_extra(mb, torch, n_jobs=16):
             "max_rel_l2_served_vs_plain_f32": max(rel)}
 
 
+# ── serving configuration: 200 requests with Poisson arrivals ──────────────
+def config5_jobs(mb, torch, n_jobs=200, rate=5.0, seed=11):
+    """The serving configuration: n_jobs requests with Poisson arrivals at
+    `rate` per second (seeded exponential gaps); 40% parallel, 40% cone, 20%
+    helical cone (pitch 1, 2 turns of 720 views: the source rises two
+    detector heights at iso over the scan, the volume centred); slices
+    uniform in {16, 64, 128, 256} (= detector rows), in-plane size in {128,
+    256, 512}, views in {180, 360, 720} (not helical), channels 1.5x the
+    in-plane size; cone magnification 2 with a pitch-2 detector; ellipsoid
+    phantoms (largest line integral 3) with Poisson counts at I0 = 1e4.
+    Returns [(arrival offset s, kind, model factory, sinogram on the host,
+    seed)]."""
+    rng = np.random.default_rng(seed)
+    dev = torch.device("cuda", 0)
+    t = 0.0
+    jobs = []
+    for j in range(n_jobs):
+        t += float(rng.exponential(1.0 / rate))
+        kind = str(rng.choice(["parallel", "cone", "helical"], p=[0.4, 0.4, 0.2]))
+        S = int(rng.choice([16, 64, 128, 256]))
+        N = int(rng.choice([128, 256, 512]))
+        Vj = 1440 if kind == "helical" else int(rng.choice([180, 360, 720]))
+        Cj = int(1.5 * N)
+
+        def make(kind=kind, S=S, N=N, Vj=Vj, Cj=Cj):
+            if kind == "parallel":
+                mj = mb.ParallelBeamModel((Vj, S, Cj), np.linspace(0, np.pi, Vj, endpoint=False))
+            else:
+                sdd, sid = 4.0 * N, 2.0 * N
+                if kind == "helical":
+                    # 720 views per turn; z rises by pitch x detector height at
+                    # iso (S rows of 2 / magnification 2) per turn
+                    ang = (2 * np.pi / 720) * np.arange(Vj)
+                    z_range = 2 * 1.0 * S
+                    zs = np.linspace(-0.5 * z_range, 0.5 * z_range, Vj)
+                else:
+                    ang, zs = np.linspace(0, 2 * np.pi, Vj, endpoint=False), None
+                mj = mb.ConeBeamModel((Vj, S, Cj), ang, source_detector_dist=sdd,
+                                      source_iso_dist=sid, helical_z_shifts=zs)
+                mj.set_params(no_warning=True, delta_det_channel=2.0, delta_det_row=2.0)
+                mj.auto_set_recon_geometry(no_warning=True)
+            mj.set_params(no_warning=True, verbose=0, recon_shape=(N, N, S))
+            return mj
+
+        mj = make()
+        with torch.no_grad():
+            vol = phantom_torch(torch, (N, N, S), 1000 + j, dev)
+            clean = mj.forward_project(vol, output_sharded=True)
+            del vol
+            mu = 3.0 / max(float(clean.max()), 1e-6)
+            gen = torch.Generator(device=dev).manual_seed(2000 + j)
+            counts = torch.poisson(I0 * torch.exp(-mu * clean), generator=gen)
+            del clean
+            sino = (-torch.log(torch.clamp(counts, min=1.0) / I0) / mu).cpu().numpy()
+            del counts
+        jobs.append((t, kind, make, sino, 3000 + j))
+    return jobs
+
+
+def serving_config5(mb, torch, n_jobs=200, iters=10,
+                    arms=(("bfloat16", "shortest"), ("float32", "shortest"), ("bfloat16", "fifo")),
+                    max_active=8):
+    """The served form against sequential plain FP32 solves on the same
+    requests.  Plain: each job alone through model.recon (FP32), one after
+    another in arrival order; its latencies are those of a FIFO single-job
+    server fed the same arrivals (start = max(arrival, previous finish),
+    from the measured per-job times).  Served: the requests submitted at
+    their real arrival times to a ReconServer (bfloat16 storage, admission
+    against the memory ledger, up to `max_active` jobs resident), once per
+    (storage precision, admission policy) arm.  Each served result is
+    compared with its own plain result."""
+    from mbirtorch_b200.serving import ReconServer
+    t_gen = time.perf_counter()
+    jobs = config5_jobs(mb, torch, n_jobs)
+    t_gen = time.perf_counter() - t_gen
+    torch.cuda.empty_cache()
+    # warm-up of both paths on the smallest two jobs
+    small = sorted(jobs, key=lambda j: j[3].size)[:2]
+    for _, _, make, sino, seed in small:
+        np.random.seed(seed)
+        make().recon(sino, max_iterations=2, stop_threshold_change_pct=0, logfile_path=None,
+                     print_logs=False)
+    srv = ReconServer(storage_dtype=arms[0][0], max_active=max_active)
+    for _, _, make, sino, seed in small:
+        srv.submit(make(), sino, max_iterations=2, seed=seed)
+    srv.run_until_idle(timeout_s=600)
+    # plain FP32, sequential
+    plain, durations = [], []
+    for _, _, make, sino, seed in jobs:
+        t0 = time.perf_counter()
+        np.random.seed(seed)
+        r, _ = make().recon(sino, max_iterations=iters, stop_threshold_change_pct=0,
+                            logfile_path=None, print_logs=False)
+        durations.append(time.perf_counter() - t0)
+        plain.append(r)
+    finish, lat = 0.0, []
+    for (arr, _, _, _, _), d in zip(jobs, durations):
+        finish = max(arr, finish) + d
+        lat.append(finish - arr)
+    plain_span = finish - jobs[0][0]
+    torch.cuda.empty_cache()
+    out = {"requests": n_jobs, "arrival_rate_per_s": 5.0, "iterations": iters,
+           "max_active": max_active, "arrivals_span_s": jobs[-1][0] - jobs[0][0],
+           "data_generation_s": t_gen,
+           "plain_f32": {"recons_per_s": n_jobs / plain_span,
+                         "busy_recons_per_s": n_jobs / sum(durations),
+                         "p50_latency_s": float(np.percentile(lat, 50)),
+                         "p99_latency_s": float(np.percentile(lat, 99)),
+                         "span_s": plain_span}}
+    kinds = {}
+    for _, kind, _, _, _ in jobs:
+        kinds[kind] = kinds.get(kind, 0) + 1
+    out["kinds"] = kinds
+    # served, at the real arrival times, once per storage precision
+    for storage, admission in arms:
+        srv = ReconServer(storage_dtype=storage, max_active=max_active, admission=admission)
+        schedule = [(arr, dict(model=make(), sinogram=sino, max_iterations=iters, seed=seed))
+                    for arr, _, make, sino, seed in jobs]
+        done = srv.serve_schedule(schedule, timeout_s=3600)
+        st = srv.stats()
+        by_id = {r.id: r for r in done}
+        rel = [float(np.linalg.norm(by_id[k].recon.astype(np.float64) - p) / np.linalg.norm(p))
+               for k, p in enumerate(plain)]
+        out[f"served_{storage}_{admission}"] = {
+            "recons_per_s": st["recons_per_s"], "p50_latency_s": st["p50_latency_s"],
+            "p99_latency_s": st["p99_latency_s"], "span_s": st["span_s"],
+            "max_concurrent": st["max_concurrent"], "failed": st["failed"],
+            "deferred_admissions": srv.deferred,
+            "ledger_high_water_gb": srv.ledger.high_water / 1e9,
+            "over_plain_recons_per_s": st["recons_per_s"] / (n_jobs / plain_span),
+            "rel_l2_vs_plain_f32": {"max": max(rel), "median": float(np.median(rel))}}
+        del srv, done
+        torch.cuda.empty_cache()
+    return out
+
+
 # ── the reference's own GPU kernels on this GPU ────────────────────────────
 def _time_cuda(torch, fn, reps=3):
     fn()
@@ -951,7 +1090,10 @@ def main():
         torch.cuda.synchronize()
 
     if args.profile_case:
-        return profile_case(args.profile_case, mb, torch, dev)
+        return profile_case(args.profile_case, mb, torch, dev, args.storage)
+    if args.serving_config5:
+        print(json.dumps({"serving_config5": serving_config5(mb, torch)}), flush=True)
+        return
     m = cone_model(mb, HEAD)
     m.set_storage_precision(args.storage)
     y = make_data(m, torch, dev, 5)
@@ -1060,7 +1202,7 @@ def extras(args, m, mb, torch, dev, y, rec_ref, full=True):
     return res
 
 
-def profile_case(case, mb, torch, dev):
+def profile_case(case, mb, torch, dev, storage="float32"):
     """One pass for a profiler (no JSON line).  'recon' is one whole headline
     reconstruction; 'subset' is three VCD subset steps of its 128-subset
     partition from a zero volume; 'subset-small' the same on the 256^3
@@ -1077,6 +1219,7 @@ def profile_case(case, mb, torch, dev):
     if case == "subset-cone64":
         return cone64_pass(mb, torch)
     m = cone_model(mb, "cone256_flat" if case == "subset-small" else HEAD)
+    m.set_storage_precision(storage)
     y = make_data(m, torch, dev, 5)
     if case == "recon":
         recon(m, y, output_sharded=True)

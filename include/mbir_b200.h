@@ -282,6 +282,27 @@ int32_t mbir_vcd_partition_pass(const mbir_geometry *geom,
                                 double *accum, void *workspace,
                                 size_t workspace_bytes, void *stream);
 
+/* Up to MBIR_MAX_BATCH reconstructions that share a geometry, stepped
+ * together (no counterpart in the reference, which reconstructs one job at
+ * a time; the serving layer's cross-job batching): each subset index i
+ * updates subset order[j][i] of job j, exactly as mbir_vcd_partition_pass
+ * would for that job alone, but each kernel of the subset step is launched
+ * once for all jobs (job index on grid z).  The arguments are HOST arrays
+ * of num_jobs entries -- params and the per-job device pointers -- plus
+ * order, a HOST (num_jobs, num_subsets) int32 array.  The jobs must agree
+ * in storage, positivity, prior kind and weighting; their regularization
+ * scalars may differ.  Each job has its own workspace (workspace_bytes
+ * each) and its own accumulators.  Geometries that the binned subset path
+ * does not cover step their jobs one after another. */
+#define MBIR_MAX_BATCH 16
+int32_t mbir_vcd_partition_pass_batched(
+    int32_t num_jobs, const mbir_geometry *geom, const float *view_params,
+    const mbir_vcd_params *params, float *const *flat_recon, void *const *error_sino,
+    const float *const *err_scale, const void *const *weights, const float *const *w_scale,
+    const float *const *fm_hessian, const float *dc_profile, const int64_t *const *partition,
+    int32_t num_subsets, int64_t subset_pixels, const int32_t *order, double *const *accum,
+    void *const *workspace, size_t workspace_bytes, void *stream);
+
 /* Workspace bytes for mbir_denoise_pass with subsets of subset_pixels
  * pixels of an image with num_slices slices. */
 size_t mbir_denoise_workspace_size(int32_t num_slices, int64_t subset_pixels);

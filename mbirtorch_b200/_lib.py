@@ -21,6 +21,7 @@ MBIR_PARALLEL, MBIR_CONE = 0, 1
 MBIR_LAYOUT_VRC, MBIR_LAYOUT_VCR = 0, 1
 MBIR_F32, MBIR_BF16, MBIR_F16 = 0, 1, 2
 MAX_TAP_RADIUS = 3
+MAX_BATCH = 16
 
 STORAGE_CODES = {'float32': MBIR_F32, 'bfloat16': MBIR_BF16, 'float16': MBIR_F16}
 STORAGE_DTYPES = {MBIR_F32: torch.float32, MBIR_BF16: torch.bfloat16, MBIR_F16: torch.float16}
@@ -104,6 +105,9 @@ SIGNATURES = {
                                       _i64, _vp, _vp, _vp, _sz, _vp]),
     "mbir_vcd_partition_pass": (_i32, [_GP, _vp, _PP, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                        _i32, _i64, _vp, _vp, _vp, _sz, _vp]),
+    "mbir_vcd_partition_pass_batched": (_i32, [_i32, _GP, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                               _vp, _vp, _vp, _i32, _i64, _vp, _vp, _vp, _sz,
+                                               _vp]),
     "mbir_iteration_stats": (_i32, [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _i32, _vp, _i64,
                                     _vp, _vp, _sz, _vp]),
     "mbir_iteration_stats_workspace_size": (_sz, []),

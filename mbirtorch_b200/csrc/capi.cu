@@ -13,7 +13,7 @@
 #include <string>
 #include <vector>
 
-#include "vcd.cuh"
+#include "batch.cuh"
 
 using namespace mbir;
 
@@ -35,9 +35,12 @@ std::vector<TimedLaunch> g_timed;
 thread_local cudaEvent_t t_pending = nullptr;
 thread_local cudaStream_t t_stream = nullptr;
 
+struct BatchRecorder;
+thread_local BatchRecorder *t_batch = nullptr;  // see launchb
+
 void tpre(cudaStream_t st) {
   t_stream = st;
-  if (!g_timing.load(std::memory_order_relaxed)) return;
+  if (!g_timing.load(std::memory_order_relaxed) || t_batch) return;
   cudaEventCreate(&t_pending);
   cudaEventRecord(t_pending, st);
 }
@@ -64,7 +67,7 @@ int fail(int code, const char *fmt, ...) {
 
 #define MBIR_CHECK_LAUNCH(what)                                                     \
   do {                                                                              \
-    g_launches.fetch_add(1, std::memory_order_relaxed);                             \
+    if (!t_batch) g_launches.fetch_add(1, std::memory_order_relaxed);               \
     tpost(what);                                                                    \
     cudaError_t _e = cudaGetLastError();                                            \
     if (_e != cudaSuccess)                                                          \
@@ -162,6 +165,88 @@ void launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_
   (void)cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
 }
 
+// ── cross-job batching (batch.cuh) ─────────────────────────────────────────
+// While a BatchRecorder is installed on this thread, launchb<B>(...) records
+// the launch's arguments for the recorder's current job instead of
+// launching; BatchRecorder::replay then issues each recorded launch once,
+// for every job, as batched_kernel<B, ...> with the job on grid z.
+struct BatchRecorder {
+  struct Launch {
+    int (*replay)(const Launch &, int jobs, cudaStream_t);
+    dim3 grid, block;
+    size_t smem;
+    const char *what;
+    size_t blob;                 // bytes of one job's argument pack
+    std::vector<char> args;      // the jobs' packs, one after another
+  };
+  std::vector<Launch> launches;
+  int job = 0;
+  size_t cursor = 0;
+  bool mismatch = false;
+
+  void begin_job(int j) {
+    job = j;
+    cursor = 0;
+  }
+  void record(int (*replay)(const Launch &, int, cudaStream_t), dim3 grid, dim3 block,
+              size_t smem, const char *what, const void *pack, size_t bytes) {
+    if (job == 0) {
+      Launch l{replay, grid, block, smem, what, bytes, {}};
+      l.args.resize(bytes * kMaxBatch);
+      launches.push_back(std::move(l));
+    }
+    if (cursor >= launches.size()) {
+      mismatch = true;
+      return;
+    }
+    Launch &l = launches[cursor++];
+    if (l.replay != replay || l.blob != bytes || l.smem != smem || l.grid.x != grid.x ||
+        l.grid.y != grid.y || l.block.x != block.x || l.block.y != block.y) {
+      mismatch = true;
+      return;
+    }
+    memcpy(l.args.data() + (size_t)job * bytes, pack, bytes);
+  }
+};
+template <typename B, typename... K>
+int replay_batched(const BatchRecorder::Launch &l, int jobs, cudaStream_t st);
+
+template <typename B, typename... KArgs, typename... Args>
+void launchb_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+               const char *what, Args... args) {
+  if (!t_batch) {
+    launch(k, grid, block, smem, st, args...);
+    return;
+  }
+  const ArgPack<KArgs...> pack = make_pack(static_cast<KArgs>(args)...);
+  t_batch->record(&replay_batched<B, KArgs...>, grid, block, smem, what, &pack, sizeof(pack));
+}
+
+// A launch of the subset step's kernel B (batch.cuh) that a BatchRecorder
+// can take over.
+template <typename B, typename... Args>
+void launchb(dim3 grid, dim3 block, size_t smem, cudaStream_t st, const char *what,
+             Args... args) {
+  launchb_k<B>(B::kernel(), grid, block, smem, st, what, args...);
+}
+
+template <typename B, typename... K>
+int replay_batched(const BatchRecorder::Launch &l, int jobs, cudaStream_t st) {
+  BatchTable<K...> t;
+  for (int j = 0; j < jobs; ++j) memcpy(&t.job[j], l.args.data() + (size_t)j * l.blob, l.blob);
+  auto k = batched_kernel<B, K...>;
+  {
+    const int rc_smem = request_smem(k, l.smem, l.what);
+    if (rc_smem) return rc_smem;
+  }
+  dim3 grid = l.grid;
+  grid.z = (unsigned)jobs;
+  tpre(st);
+  launch(k, grid, l.block, l.smem, st, t);
+  MBIR_CHECK_LAUNCH(l.what);
+  return MBIR_OK;
+}
+
 inline int next_pow2(int x) {
   int p = 1;
   while (p < x) p <<= 1;
@@ -199,8 +284,13 @@ int validate_geometry(const mbir_geometry *g) {
     return fail(MBIR_ERR_INVALID, "recon grid too large for 32-bit pixel indices");
   if (g->psf_radius < 0 || g->psf_radius > MBIR_MAX_TAP_RADIUS || g->bp_psf_radius < 0 ||
       g->bp_psf_radius > MBIR_MAX_TAP_RADIUS)
-    return fail(MBIR_ERR_INVALID, "tap radii must lie in [0, %d] (psf %d, bp %d)",
-                MBIR_MAX_TAP_RADIUS, g->psf_radius, g->bp_psf_radius);
+    return fail(MBIR_ERR_INVALID,
+                "tap radii must lie in [0, %d] (psf %d, bp %d): the kernels unroll at most "
+                "%d taps a side, where the reference's torch bodies take any radius.  A psf "
+                "radius ceil(ceil(voxel pitch x magnification / detector pitch) / 2) above %d "
+                "means voxels wider than %d detector cells; use finer voxels or a coarser "
+                "detector binning", MBIR_MAX_TAP_RADIUS, g->psf_radius, g->bp_psf_radius,
+                MBIR_MAX_TAP_RADIUS, MBIR_MAX_TAP_RADIUS, 2 * MBIR_MAX_TAP_RADIUS);
   if (!(g->delta_det_channel > 0.f) || !(g->delta_voxel > 0.f) || !(g->delta_voxel_row > 0.f))
     return fail(MBIR_ERR_INVALID, "detector and voxel pitches must be positive");
   if (g->geometry == MBIR_PARALLEL && g->num_det_rows != g->num_slices)
@@ -286,21 +376,25 @@ int launch_back_t(const Geo &geo, const mbir_geometry *g, const float *vp, int v
     const int rc = request_smem(k, s.smem, what);
     if (rc) return rc;
     tpre(st);
-    launch(k, grid, kThreads, s.smem, st, geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P,
-           slice_start, band, s.slice_chunks, dst, recs);
+    launchb<BackConeB<CP, SPL, NT, RD>>(grid, kThreads, s.smem, st, what, geo, vp, v_start,
+                                        v_count, s.vpc, rd, pix, (int)P, slice_start, band,
+                                        s.slice_chunks, dst, recs);
   } else if (NT == 3 && SPL == 4 && band % 4 == 0 && rd.aligned16() && is_aligned16(dst)) {
     // four consecutive slices per lane: the same teams, one 16-byte load per tap
-    auto k4 = s.T == 32 ? back_parallel4_kernel<CP, 32, RD>
-            : s.T == 16 ? back_parallel4_kernel<CP, 16, RD>
-            : s.T == 8  ? back_parallel4_kernel<CP, 8, RD>
-                        : back_parallel4_kernel<CP, 4, RD>;
     tpre(st);
-    launch(k4, grid, kThreads, 0, st, geo, vp, v_start, v_count, s.vpc, rd, pix, (int)P, band,
-           s.slice_chunks, dst);
+#define MBIR_BACK4(TV)                                                                       \
+  launchb<BackParallel4B<CP, TV, RD>>(grid, kThreads, 0, st, what, geo, vp, v_start, v_count, \
+                                      s.vpc, rd, pix, (int)P, band, s.slice_chunks, dst)
+    if (s.T == 32) MBIR_BACK4(32);
+    else if (s.T == 16) MBIR_BACK4(16);
+    else if (s.T == 8) MBIR_BACK4(8);
+    else MBIR_BACK4(4);
+#undef MBIR_BACK4
   } else {
     tpre(st);
-    launch(back_parallel_kernel<CP, SPL, NT, RD>, grid, kThreads, 0, st, geo, vp, v_start,
-           v_count, s.vpc, rd, pix, (int)P, band, s.T, s.slice_chunks, dst);
+    launchb<BackParallelB<CP, SPL, NT, RD>>(grid, kThreads, 0, st, what, geo, vp, v_start,
+                                            v_count, s.vpc, rd, pix, (int)P, band, s.T,
+                                            s.slice_chunks, dst);
   }
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
@@ -477,8 +571,8 @@ int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count
     if (rc_smem) return rc_smem;
   }
   tpre(st);
-  launch(cone_bin_kernel, v_count, kThreads, smem, st, geo, vp, v_start, pix, (int)P, 0, b.recs,
-         b.list, b.offs);
+  launchb<ConeBinB>(v_count, kThreads, smem, st, "vcd forward binning", geo, vp, v_start, pix,
+                    (int)P, 0, b.recs, b.list, b.offs);
   MBIR_CHECK_LAUNCH("vcd forward binning");
   return MBIR_OK;
 }
@@ -496,8 +590,9 @@ int launch_binned(const mbir_geometry *g, int v_start, int v_count, const float 
   }
   dim3 grid(fwd_nblk(g), v_count);
   tpre(st);
-  launch(k, grid, cone_rt_threads(g), smem, st, geo, v_start, values, (int)P, band, 0,
-         (const ConeFwdRec *)b.recs, (const int *)b.list, (const int *)b.offs, b.touched, epi);
+  launchb<FwdConeBinnedB<EPI>>(grid, cone_rt_threads(g), smem, st, what, geo, v_start, values,
+                               (int)P, band, 0, (const ConeFwdRec *)b.recs, (const int *)b.list,
+                               (const int *)b.offs, b.touched, epi);
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
 }
@@ -521,8 +616,9 @@ int launch_par_binned(const mbir_geometry *g, int v_start, int v_count, const fl
     }
     dim3 grid(fwd_nblk(g), v_count);
     tpre(st);
-    launch(k4, grid, nthr4, smem4, st, geo, v_start, values, (int)P, band,
-           (const ConeFwdRec *)b.recs, (const int *)b.list, (const int *)b.offs, b.touched, epi);
+    launchb<FwdParBinned4B<EPI>>(grid, nthr4, smem4, st, what, geo, v_start, values, (int)P,
+                                 band, (const ConeFwdRec *)b.recs, (const int *)b.list,
+                                 (const int *)b.offs, b.touched, epi);
     MBIR_CHECK_LAUNCH(what);
     return MBIR_OK;
   }
@@ -535,8 +631,9 @@ int launch_par_binned(const mbir_geometry *g, int v_start, int v_count, const fl
   }
   dim3 grid(fwd_nblk(g), v_count);
   tpre(st);
-  launch(k, grid, nthr, smem, st, geo, v_start, values, (int)P, band, (const ConeFwdRec *)b.recs,
-         (const int *)b.list, (const int *)b.offs, b.touched, epi);
+  launchb<FwdParBinnedB<EPI>>(grid, nthr, smem, st, what, geo, v_start, values, (int)P, band,
+                              (const ConeFwdRec *)b.recs, (const int *)b.list,
+                              (const int *)b.offs, b.touched, epi);
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
 }
@@ -684,26 +781,27 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   int nprior = nb;  // prior line-term partials the alpha kernel folds
   if (!DCon) {
     tpre(st);
-    launch(vcd_direction_kernel<false>, nb, kThreads, 0, st, (int)Ps, S, pix, g->num_recon_rows,
-           g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H, sc, w.delta, nullptr, nullptr,
-           nullptr, nullptr, w.prior_part);
+    launchb<DirectionB<false>>(nb, kThreads, 0, st, "vcd direction", (int)Ps, S, pix,
+                               g->num_recon_rows, g->num_recon_cols, w.grad_part, w.bs.nchunks,
+                               flat, H, sc, w.delta, nullptr, nullptr, nullptr, nullptr,
+                               w.prior_part);
     MBIR_CHECK_LAUNCH("vcd direction");
   } else {
     tpre(st);
-    launch(vcd_direction_kernel<true>, nb, kThreads, 0, st, (int)Ps, S, pix, g->num_recon_rows,
-           g->num_recon_cols, w.grad_part, w.bs.nchunks, flat, H, sc, nullptr, w.gbuf, w.hinv,
-           w.gpbuf, w.hpbuf, nullptr);
+    launchb<DirectionB<true>>(nb, kThreads, 0, st, "vcd direction (damped)", (int)Ps, S, pix,
+                              g->num_recon_rows, g->num_recon_cols, w.grad_part, w.bs.nchunks,
+                              flat, H, sc, nullptr, w.gbuf, w.hinv, w.gpbuf, w.hpbuf, nullptr);
     MBIR_CHECK_LAUNCH("vcd direction (damped)");
     dim3 gs(w.dc_chunks, (S + 31) / 32);
     tpre(st);
-    launch(vcd_dc_sums_kernel, gs, dim3(32, kDcGroups), 0, st, (int)Ps, S, w.gbuf, w.hinv,
-           w.dc_sums);
+    launchb<DcSumsB>(gs, dim3(32, kDcGroups), 0, st, "vcd DC sums", (int)Ps, S, w.gbuf, w.hinv,
+                     w.dc_sums);
     MBIR_CHECK_LAUNCH("vcd DC sums");
     const dim3 gd((unsigned)((Ps + kDcDirPixels - 1) / kDcDirPixels), (S + 31) / 32);
     nprior = (int)(gd.x * gd.y);
     tpre(st);
-    launch(vcd_dc_direction_kernel, gd, dim3(32, 8), 0, st, (int)Ps, S, w.dc_chunks, w.dc_sums,
-           dc, w.gbuf, w.hinv, w.gpbuf, w.hpbuf, w.delta, w.prior_part);
+    launchb<DcDirectionB>(gd, dim3(32, 8), 0, st, "vcd DC direction", (int)Ps, S, w.dc_chunks,
+                          w.dc_sums, dc, w.gbuf, w.hinv, w.gpbuf, w.hpbuf, w.delta, w.prior_part);
     MBIR_CHECK_LAUNCH("vcd DC direction");
   }
   // 3. forward A delta + line-search partials
@@ -716,13 +814,13 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
   if (rc) return rc;
   // 4. alpha
   tpre(st);
-  launch(vcd_alpha_kernel, 1, kAlphaThreads, 0, st, w.prior_part, nprior, w.fwd_part, w.fwd_blocks,
-         sc.fmc, sc.max_alpha, w.alpha, alpha_user);
+  launchb<AlphaB>(1, kAlphaThreads, 0, st, "vcd alpha", w.prior_part, nprior, w.fwd_part,
+                  w.fwd_blocks, sc.fmc, sc.max_alpha, w.alpha, alpha_user);
   MBIR_CHECK_LAUNCH("vcd alpha");
   if (prm->positivity) {
     tpre(st);
-    launch(vcd_positivity_kernel, (unsigned)((PS + 255) / 256), 256, 0, st, (int)Ps, S, pix,
-           flat, w.alpha, w.delta);
+    launchb<PositivityB>((unsigned)((PS + 255) / 256), 256, 0, st, "vcd positivity", (int)Ps, S,
+                         pix, flat, w.alpha, w.delta);
     MBIR_CHECK_LAUNCH("vcd positivity");
     LineSearchEpi<T> epi2{err, es, wts, wsc, static_cast<T *>(w.ad), C, R, nullptr, 0, 0.0, 0.0};
     if (w.binned)
@@ -752,10 +850,10 @@ int vcd_subset_t(const mbir_geometry *g, const float *vp, const mbir_vcd_params 
     const long long ctas = (long long)nbin + (long long)w.upd_chunks * w.upd_yblocks +
                            (long long)((nblk + tpc - 1) / tpc) * V;
     tpre(st);
-    launch(k, (unsigned)ctas, 256, smem, st, nbin, tb, (int)Ps, S, kUpdChunk, pix, w.delta,
-           w.alpha, flat, w.sq_part, w.l1_part, w.counters + 1, accum, w.upd_chunks,
-           w.upd_yblocks, C, R, kFwdCB, w.bins.touched, err, static_cast<const T *>(w.ad), nblk,
-           tpc);
+    launchb<TailB<T>>((unsigned)ctas, 256, smem, st, "vcd pixel + sinogram update", nbin, tb,
+                      (int)Ps, S, kUpdChunk, pix, w.delta, w.alpha, flat, w.sq_part, w.l1_part,
+                      w.counters + 1, accum, w.upd_chunks, w.upd_yblocks, C, R, kFwdCB,
+                      w.bins.touched, err, static_cast<const T *>(w.ad), nblk, tpc);
     MBIR_CHECK_LAUNCH("vcd pixel + sinogram update");
     if (binned_next) *binned_next = nbin > 0;
     return MBIR_OK;
@@ -1183,6 +1281,81 @@ int32_t mbir_vcd_partition_pass(const mbir_geometry *geom, const float *view_par
         fm_hessian, dc_profile, partition + (size_t)order[i] * subset_pixels, subset_pixels, accum,
         nullptr, workspace, workspace_bytes, stream, i == 0, next, prebinned, &binned_next);
     if (rc) return rc;
+    prebinned = binned_next;
+  }
+  return MBIR_OK;
+}
+
+int32_t mbir_vcd_partition_pass_batched(
+    int32_t num_jobs, const mbir_geometry *geom, const float *view_params,
+    const mbir_vcd_params *params, float *const *flat_recon, void *const *error_sino,
+    const float *const *err_scale, const void *const *weights, const float *const *w_scale,
+    const float *const *fm_hessian, const float *dc_profile, const int64_t *const *partition,
+    int32_t num_subsets, int64_t subset_pixels, const int32_t *order, double *const *accum,
+    void *const *workspace, size_t workspace_bytes, void *stream) {
+  if (num_jobs < 1 || num_jobs > kMaxBatch)
+    return fail(MBIR_ERR_INVALID, "a batch holds 1 to %d jobs, got %d", kMaxBatch, num_jobs);
+  if (!params || !flat_recon || !error_sino || !err_scale || !weights || !w_scale ||
+      !fm_hessian || !partition || !order || !accum || !workspace)
+    return fail(MBIR_ERR_INVALID, "batched partition pass: NULL argument array");
+  if (num_subsets <= 0 || subset_pixels <= 0)
+    return fail(MBIR_ERR_INVALID, "partition pass needs subsets, a partition and an order");
+  for (int j = 0; j < num_jobs; ++j) {
+    // Every job of a batch takes the same branches of the subset step.
+    const mbir_vcd_params &a = params[0], &b = params[j];
+    if (b.storage != a.storage || b.positivity != a.positivity ||
+        (b.prox_input == nullptr) != (a.prox_input == nullptr) ||
+        (weights[j] == nullptr) != (weights[0] == nullptr))
+      return fail(MBIR_ERR_INVALID, "job %d of the batch differs from job 0 in storage, "
+                  "positivity, prior or weighting", j);
+    for (int i = 0; i < num_subsets; ++i) {
+      const int o = order[(size_t)j * num_subsets + i];
+      if (o < 0 || o >= num_subsets)
+        return fail(MBIR_ERR_INVALID, "order[%d][%d] = %d outside [0, %d)", j, i, o,
+                    num_subsets);
+    }
+  }
+  const int rc0 = validate_geometry(geom);
+  if (rc0) return rc0;
+  if (!use_binned(geom)) {
+    // The batched chain covers the binned subset step; other shapes step
+    // their jobs one after another.
+    for (int j = 0; j < num_jobs; ++j) {
+      const int rc = mbir_vcd_partition_pass(
+          geom, view_params, &params[j], flat_recon[j], error_sino[j], err_scale[j], weights[j],
+          w_scale[j], fm_hessian[j], dc_profile, partition[j], num_subsets, subset_pixels,
+          order + (size_t)j * num_subsets, accum[j], workspace[j], workspace_bytes, stream);
+      if (rc) return rc;
+    }
+    return MBIR_OK;
+  }
+  cudaStream_t st = as_stream(stream);
+  const PdlScope pdl;
+  bool prebinned = false;
+  for (int i = 0; i < num_subsets; ++i) {
+    BatchRecorder rec;
+    bool binned_next = false;
+    for (int j = 0; j < num_jobs; ++j) {
+      const int32_t *oj = order + (size_t)j * num_subsets;
+      const int64_t *pj = partition[j];
+      const int64_t *next = i + 1 < num_subsets ? pj + (size_t)oj[i + 1] * subset_pixels : nullptr;
+      rec.begin_job(j);
+      t_batch = &rec;
+      const int rc = subset_update(geom, view_params, &params[j], flat_recon[j], error_sino[j],
+                                   err_scale[j], weights[j], w_scale[j], fm_hessian[j],
+                                   dc_profile, pj + (size_t)oj[i] * subset_pixels, subset_pixels,
+                                   accum[j], nullptr, workspace[j], workspace_bytes, stream, i == 0,
+                                   next, prebinned, &binned_next);
+      t_batch = nullptr;
+      if (rc) return rc;
+      if (rec.mismatch || rec.cursor != rec.launches.size())
+        return fail(MBIR_ERR_INVALID, "job %d's subset step does not match job 0's launch "
+                    "for launch", j);
+    }
+    for (const BatchRecorder::Launch &l : rec.launches) {
+      const int rc = l.replay(l, num_jobs, st);
+      if (rc) return rc;
+    }
     prebinned = binned_next;
   }
   return MBIR_OK;

@@ -126,8 +126,7 @@ struct __align__(16) ConeFwdRec {
 
 // ── back projection: parallel ─────────────────────────────────────────────
 template <int CP, int SPL, int NT, typename RD>
-__global__ void __launch_bounds__(kThreads)
-back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
+__device__ __forceinline__ void back_parallel_kernel_body(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
                      RD rd, const int64_t *__restrict__ pix, int P, int band, int T,
                      int slice_chunks, float *__restrict__ out) {
   MBIR_PDL_ENTRY();
@@ -219,6 +218,15 @@ back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_cou
   }
 }
 
+template <int CP, int SPL, int NT, typename RD>
+__global__ void __launch_bounds__(kThreads)
+
+back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
+                     RD rd, const int64_t *__restrict__ pix, int P, int band, int T,
+                     int slice_chunks, float *__restrict__ out) {
+  back_parallel_kernel_body<CP, SPL, NT, RD>(g, vp, v_start, v_count, vpc, rd, pix, P, band, T, slice_chunks, out);
+}
+
 // The parallel back projector at psf radius 1 with four consecutive slices
 // per lane (a team of T lanes covers 4 T slices, as SPL = 4 does):
 // each tap of a view is one 16-byte load per lane, and two views' taps are
@@ -226,8 +234,7 @@ back_parallel_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_cou
 // of FMAs as in back_parallel_kernel.  Needs band a multiple of 4 and the
 // operands 16-byte aligned (checked on the host).
 template <int CP, int T, typename RD>
-__global__ void __launch_bounds__(kThreads)
-back_parallel4_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
+__device__ __forceinline__ void back_parallel4_kernel_body(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
                       RD rd, const int64_t *__restrict__ pix, int P, int band, int slice_chunks,
                       float *__restrict__ out) {
   MBIR_PDL_ENTRY();
@@ -298,6 +305,15 @@ back_parallel4_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_co
     float *o = out + (size_t)chunk * P * band + (size_t)p * band + l;
     *reinterpret_cast<float4 *>(o) = make_float4(acc[0], acc[1], acc[2], acc[3]);
   }
+}
+
+template <int CP, int T, typename RD>
+__global__ void __launch_bounds__(kThreads)
+
+back_parallel4_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc,
+                      RD rd, const int64_t *__restrict__ pix, int P, int band, int slice_chunks,
+                      float *__restrict__ out) {
+  back_parallel4_kernel_body<CP, T, RD>(g, vp, v_start, v_count, vpc, rd, pix, P, band, slice_chunks, out);
 }
 
 // Trapezoid tap weight min(max(x, 0), lmax) (cone_beam.py:203-226,
@@ -377,8 +393,7 @@ __device__ __forceinline__ void column_batch(const RD &rd, const size_t (&base)[
 // One warp per (pixel, chunk of 32*SPL slices).  Dynamic shared memory:
 // 8 warps x (R + 2 kPad) floats of column buffer, then 8 x 32 ConeRec.
 template <int CP, int SPL, int NT, typename RD>
-__global__ void __launch_bounds__(kThreads)
-back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc, RD rd,
+__device__ __forceinline__ void back_cone_kernel_body(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc, RD rd,
                  const int64_t *__restrict__ pix, int P, int slice_start, int band,
                  int slice_chunks, float *__restrict__ out,
                  const ConeFwdRec *__restrict__ recs) {
@@ -525,6 +540,16 @@ back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, 
     const int l = l0 + lane + 32 * j;
     if (l < band) o[l] = acc[j];
   }
+}
+
+template <int CP, int SPL, int NT, typename RD>
+__global__ void __launch_bounds__(kThreads)
+
+back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc, RD rd,
+                 const int64_t *__restrict__ pix, int P, int slice_start, int band,
+                 int slice_chunks, float *__restrict__ out,
+                 const ConeFwdRec *__restrict__ recs) {
+  back_cone_kernel_body<CP, SPL, NT, RD>(g, vp, v_start, v_count, vpc, rd, pix, P, slice_start, band, slice_chunks, out, recs);
 }
 
 // out[i] = sum over chunks of part[chunk * n + i], in chunk order.
@@ -1192,8 +1217,7 @@ __device__ __forceinline__ void cone_bin_view(const Geo &g, const float *__restr
   }
 }
 
-__global__ void __launch_bounds__(256)
-cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
+__device__ __forceinline__ void cone_bin_kernel_body(Geo g, const float *__restrict__ vp, int v_start,
                 const int64_t *__restrict__ pix, int P, int by_pixel,
                 ConeFwdRec *__restrict__ recs, int *__restrict__ list, int *__restrict__ offs) {
   MBIR_PDL_ENTRY();
@@ -1201,13 +1225,20 @@ cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
   cone_bin_view(g, vp, v_start, blockIdx.x, pix, P, by_pixel, recs, list, offs, bsm);
 }
 
+__global__ void __launch_bounds__(256)
+
+cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
+                const int64_t *__restrict__ pix, int P, int by_pixel,
+                ConeFwdRec *__restrict__ recs, int *__restrict__ list, int *__restrict__ offs) {
+  cone_bin_kernel_body(g, vp, v_start, pix, P, by_pixel, recs, list, offs);
+}
+
 // Forward CTA (channel block, view of the chunk) over its bucket.  The
 // epilogue sees the absolute view v_start + vl and partial slot
 // (v_start + vl) * nblk + block; touched[view * nblk + block] records
 // whether any pixel reached the tile.
 template <typename EPI>
-__global__ void __launch_bounds__(1024)
-forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values, int P, int band,
+__device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_start, const float *__restrict__ values, int P, int band,
                            int slice_start, const ConeFwdRec *__restrict__ recs,
                            const int *__restrict__ list, const int *__restrict__ offs,
                            unsigned char *__restrict__ touched, EPI epi) {
@@ -1275,6 +1306,16 @@ forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values,
   epi.end(v * nblk + blk);
 }
 
+template <typename EPI>
+__global__ void __launch_bounds__(1024)
+
+forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values, int P, int band,
+                           int slice_start, const ConeFwdRec *__restrict__ recs,
+                           const int *__restrict__ list, const int *__restrict__ offs,
+                           unsigned char *__restrict__ touched, EPI epi) {
+  forward_cone_binned_kernel_body<EPI>(g, v_start, values, P, band, slice_start, recs, list, offs, touched, epi);
+}
+
 // ── forward projection, parallel, binned ───────────────────────────────────
 // The parallel-beam counterpart of forward_cone_binned_kernel for a VCD
 // subset: one CTA per (channel block of kFwdCB, view), thread m owns
@@ -1312,8 +1353,7 @@ __host__ __device__ inline size_t par_binned_smem(int nthr) {
 }
 
 template <typename EPI>
-__global__ void __launch_bounds__(1024)
-forward_parallel_binned_kernel(Geo g, int v_start, const float *__restrict__ values, int P,
+__device__ __forceinline__ void forward_parallel_binned_kernel_body(Geo g, int v_start, const float *__restrict__ values, int P,
                                int band, const ConeFwdRec *__restrict__ recs,
                                const int *__restrict__ list, const int *__restrict__ offs,
                                unsigned char *__restrict__ touched, EPI epi) {
@@ -1407,6 +1447,16 @@ forward_parallel_binned_kernel(Geo g, int v_start, const float *__restrict__ val
   epi.end(v * nblk + blk);
 }
 
+template <typename EPI>
+__global__ void __launch_bounds__(1024)
+
+forward_parallel_binned_kernel(Geo g, int v_start, const float *__restrict__ values, int P,
+                               int band, const ConeFwdRec *__restrict__ recs,
+                               const int *__restrict__ list, const int *__restrict__ offs,
+                               unsigned char *__restrict__ touched, EPI epi) {
+  forward_parallel_binned_kernel_body<EPI>(g, v_start, values, P, band, recs, list, offs, touched, epi);
+}
+
 // Four rows per thread (band a multiple of 4, at least 128 rows): thread t
 // owns detector rows 4t .. 4t + 3, loads their four values of a pixel as one
 // 16-byte access and keeps four sets of the three channel sums, so that the
@@ -1416,8 +1466,7 @@ forward_parallel_binned_kernel(Geo g, int v_start, const float *__restrict__ val
 // cell's sum is the same sequence of FMAs as in
 // forward_parallel_binned_kernel.
 template <typename EPI>
-__global__ void __launch_bounds__(256)
-forward_parallel_binned4_kernel(Geo g, int v_start, const float *__restrict__ values, int P,
+__device__ __forceinline__ void forward_parallel_binned4_kernel_body(Geo g, int v_start, const float *__restrict__ values, int P,
                                 int band, const ConeFwdRec *__restrict__ recs,
                                 const int *__restrict__ list, const int *__restrict__ offs,
                                 unsigned char *__restrict__ touched, EPI epi) {
@@ -1515,6 +1564,16 @@ forward_parallel_binned4_kernel(Geo g, int v_start, const float *__restrict__ va
   epi.begin(v);
   if (mine) epi.cells4(v, c0, ncb, m0, acc_s + tid, nthr);
   epi.end(v * nblk + blk);
+}
+
+template <typename EPI>
+__global__ void __launch_bounds__(256)
+
+forward_parallel_binned4_kernel(Geo g, int v_start, const float *__restrict__ values, int P,
+                                int band, const ConeFwdRec *__restrict__ recs,
+                                const int *__restrict__ list, const int *__restrict__ offs,
+                                unsigned char *__restrict__ touched, EPI epi) {
+  forward_parallel_binned4_kernel_body<EPI>(g, v_start, values, P, band, recs, list, offs, touched, epi);
 }
 
 }  // namespace mbir

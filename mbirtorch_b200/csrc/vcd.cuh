@@ -131,8 +131,7 @@ __device__ __forceinline__ void qggmrf_terms(const float *__restrict__ flat, int
 // Thread per (pixel p, slice l).  DC = 0: writes delta and the prior
 // line-term partials.  DC = 1: writes g, 1/h, g_p, h_p for the damping pass.
 template <bool DC>
-__global__ void __launch_bounds__(kThreads)
-vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int NC,
+__device__ __forceinline__ void vcd_direction_kernel_body(int P, int S, const int64_t *__restrict__ pix, int NR, int NC,
                      const float *__restrict__ part, int nchunks,
                      const float *__restrict__ flat, const float *__restrict__ H,
                      VcdScalars sc, float *__restrict__ delta, float *__restrict__ gbuf,
@@ -182,6 +181,18 @@ vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int 
   }
 }
 
+template <bool DC>
+__global__ void __launch_bounds__(kThreads)
+
+vcd_direction_kernel(int P, int S, const int64_t *__restrict__ pix, int NR, int NC,
+                     const float *__restrict__ part, int nchunks,
+                     const float *__restrict__ flat, const float *__restrict__ H,
+                     VcdScalars sc, float *__restrict__ delta, float *__restrict__ gbuf,
+                     float *__restrict__ hinv, float *__restrict__ gpbuf,
+                     float *__restrict__ hpbuf, double *__restrict__ partials) {
+  vcd_direction_kernel_body<DC>(P, S, pix, NR, NC, part, nchunks, flat, H, sc, delta, gbuf, hinv, gpbuf, hpbuf, partials);
+}
+
 // ── 2'. DC damping ───────────────────────────────────────────────────────
 // Per-slice sums over pixel chunks: part[chunk][l] = (sum h^-1 g, sum h^-1).
 // A CTA of (32 slices, 8 groups) covers one chunk of kDcChunk pixels:
@@ -193,8 +204,7 @@ constexpr int kDcPerGroup = 4;                       // pixels per group
 constexpr int kDcChunk = kDcGroups * kDcPerGroup;    // pixels per chunk
 static_assert(kDcChunk == 32, "one DC-sum CTA covers 32 pixels");
 
-__global__ void __launch_bounds__(32 * kDcGroups)
-vcd_dc_sums_kernel(int P, int S, const float *__restrict__ gbuf,
+__device__ __forceinline__ void vcd_dc_sums_kernel_body(int P, int S, const float *__restrict__ gbuf,
                    const float *__restrict__ hinv, double *__restrict__ part) {
   MBIR_PDL_ENTRY();
   __shared__ double s_num[kDcGroups][32], s_den[kDcGroups][32];
@@ -236,6 +246,13 @@ vcd_dc_sums_kernel(int P, int S, const float *__restrict__ gbuf,
   }
 }
 
+__global__ void __launch_bounds__(32 * kDcGroups)
+
+vcd_dc_sums_kernel(int P, int S, const float *__restrict__ gbuf,
+                   const float *__restrict__ hinv, double *__restrict__ part) {
+  vcd_dc_sums_kernel_body(P, S, gbuf, hinv, part);
+}
+
 // delta = -(g - (1 - s_l) * gbar_l) * h^-1, plus the prior line-term partials.
 // A CTA of (32 slices, 8 rows) owns slices [32 y, 32 y + 32) of the pixels
 // [kDcDirPixels x, kDcDirPixels (x + 1)): it folds its slices' chunk sums
@@ -244,8 +261,7 @@ vcd_dc_sums_kernel(int P, int S, const float *__restrict__ gbuf,
 // CTA's prior partials go to slot y * gridDim.x + x.
 constexpr int kDcDirPixels = 64;
 
-__global__ void __launch_bounds__(256)
-vcd_dc_direction_kernel(int P, int S, int nchunks, const double *__restrict__ sums,
+__device__ __forceinline__ void vcd_dc_direction_kernel_body(int P, int S, int nchunks, const double *__restrict__ sums,
                         const float *__restrict__ s_prof, const float *__restrict__ gbuf,
                         const float *__restrict__ hinv, const float *__restrict__ gpbuf,
                         const float *__restrict__ hpbuf, float *__restrict__ delta,
@@ -312,6 +328,16 @@ vcd_dc_direction_kernel(int P, int S, int nchunks, const double *__restrict__ su
       partials[2 * slot + 1] = b;
     }
   }
+}
+
+__global__ void __launch_bounds__(256)
+
+vcd_dc_direction_kernel(int P, int S, int nchunks, const double *__restrict__ sums,
+                        const float *__restrict__ s_prof, const float *__restrict__ gbuf,
+                        const float *__restrict__ hinv, const float *__restrict__ gpbuf,
+                        const float *__restrict__ hpbuf, float *__restrict__ delta,
+                        double *__restrict__ partials) {
+  vcd_dc_direction_kernel_body(P, S, nchunks, sums, s_prof, gbuf, hinv, gpbuf, hpbuf, delta, partials);
 }
 
 // Grid-wide "last CTA" election: every CTA calls it once after writing its
@@ -514,8 +540,7 @@ struct RefreshEpi {
 // One CTA of kAlphaThreads.  prior: np pairs (pl, pq); fwd: nf pairs (fl, fq).
 constexpr int kAlphaThreads = 1024;
 
-__global__ void __launch_bounds__(kAlphaThreads)
-vcd_alpha_kernel(const double *__restrict__ prior, int np, const double *__restrict__ fwd, int nf,
+__device__ __forceinline__ void vcd_alpha_kernel_body(const double *__restrict__ prior, int np, const double *__restrict__ fwd, int nf,
                  float fmc, float max_alpha, float *__restrict__ alpha_out,
                  float *__restrict__ alpha_user) {
   MBIR_PDL_ENTRY();
@@ -547,8 +572,16 @@ vcd_alpha_kernel(const double *__restrict__ prior, int np, const double *__restr
   }
 }
 
+__global__ void __launch_bounds__(kAlphaThreads)
+
+vcd_alpha_kernel(const double *__restrict__ prior, int np, const double *__restrict__ fwd, int nf,
+                 float fmc, float max_alpha, float *__restrict__ alpha_out,
+                 float *__restrict__ alpha_user) {
+  vcd_alpha_kernel_body(prior, np, fwd, nf, fmc, max_alpha, alpha_out, alpha_user);
+}
+
 // Positivity: delta = max(-x / (alpha + eps), delta) (tomography_model.py:2624-2633).
-__global__ void vcd_positivity_kernel(int P, int S, const int64_t *__restrict__ pix,
+__device__ __forceinline__ void vcd_positivity_kernel_body(int P, int S, const int64_t *__restrict__ pix,
                                       const float *__restrict__ flat,
                                       const float *__restrict__ alpha, float *__restrict__ delta) {
   MBIR_PDL_ENTRY();
@@ -559,6 +592,13 @@ __global__ void vcd_positivity_kernel(int P, int S, const int64_t *__restrict__ 
   const float pos_c = __fdiv_rn(1.f, __fadd_rn(alpha[0], kF32Eps));
   const float x = flat[(size_t)pix[p] * S + l];
   delta[i] = fmaxf(__fmul_rn(-pos_c, x), delta[i]);
+}
+
+__global__ void 
+vcd_positivity_kernel(int P, int S, const int64_t *__restrict__ pix,
+                                      const float *__restrict__ flat,
+                                      const float *__restrict__ alpha, float *__restrict__ delta) {
+  vcd_positivity_kernel_body(P, S, pix, flat, alpha, delta);
 }
 
 // ── 5. update ────────────────────────────────────────────────────────────
@@ -742,8 +782,7 @@ struct TailBins {
 // per SM (at most 40 registers) keep enough of the tile update's loads in
 // flight to hold the copy bandwidth.
 template <typename T>
-__global__ void __launch_bounds__(256, 6)
-vcd_tail_kernel(int nbin, TailBins tb, int P, int S, int pchunk, const int64_t *__restrict__ pix,
+__device__ __forceinline__ void vcd_tail_kernel_body(int nbin, TailBins tb, int P, int S, int pchunk, const int64_t *__restrict__ pix,
                 const float *__restrict__ delta, const float *__restrict__ alpha,
                 float *__restrict__ flat, double *__restrict__ sq_part,
                 double *__restrict__ l1_part, unsigned int *__restrict__ counter,
@@ -766,6 +805,19 @@ vcd_tail_kernel(int nbin, TailBins tb, int P, int S, int pchunk, const int64_t *
   b -= ux * uy;
   const int ngrp = (nblk + tpc - 1) / tpc;
   sino_tile_cta<T>(C, R, CB, touched, alpha, e, ad, b % ngrp, b / ngrp, nblk, tpc);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 6)
+
+vcd_tail_kernel(int nbin, TailBins tb, int P, int S, int pchunk, const int64_t *__restrict__ pix,
+                const float *__restrict__ delta, const float *__restrict__ alpha,
+                float *__restrict__ flat, double *__restrict__ sq_part,
+                double *__restrict__ l1_part, unsigned int *__restrict__ counter,
+                double *__restrict__ accum, int ux, int uy, int C, int R, int CB,
+                const unsigned char *__restrict__ touched, T *__restrict__ e,
+                const T *__restrict__ ad, int nblk, int tpc) {
+  vcd_tail_kernel_body<T>(nbin, tb, P, S, pchunk, pix, delta, alpha, flat, sq_part, l1_part, counter, accum, ux, uy, C, R, CB, touched, e, ad, nblk, tpc);
 }
 
 // ── QGGMRF denoiser (identity forward model; denoising.py:35-83) ──────────

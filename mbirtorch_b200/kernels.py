@@ -32,8 +32,14 @@ def make_geometry(kind, num_views, num_det_rows, num_det_channels, num_recon_row
                   delta_voxel_row=1.0, delta_voxel_slice=1.0, recon_slice_offset=0.0,
                   magnification=1.0, source_detector_dist=math.inf):
     if psf_radius > _lib.MAX_TAP_RADIUS or bp_psf_radius > _lib.MAX_TAP_RADIUS:
-        raise ValueError(f"tap radius above {_lib.MAX_TAP_RADIUS} is not supported "
-                         f"(psf_radius={psf_radius}, bp_psf_radius={bp_psf_radius})")
+        raise ValueError(
+            f"tap radius above {_lib.MAX_TAP_RADIUS} is not supported (psf_radius="
+            f"{psf_radius}, bp_psf_radius={bp_psf_radius}): the kernels unroll at most "
+            f"{_lib.MAX_TAP_RADIUS} taps a side, where the reference's torch bodies "
+            "(horizontal_fan.py:74-154) take any radius.  The radius is "
+            "ceil(ceil(voxel pitch x magnification / detector pitch) / 2): voxels wider than "
+            f"{2 * _lib.MAX_TAP_RADIUS} detector cells exceed it; use finer voxels or a "
+            "coarser detector binning")
     return Geometry(MBIR_CONE if kind == 'cone' else MBIR_PARALLEL, int(num_views),
                     int(num_det_rows), int(num_det_channels), int(num_recon_rows),
                     int(num_recon_cols), int(num_slices), int(psf_radius), int(bp_psf_radius),

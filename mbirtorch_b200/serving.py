@@ -131,10 +131,24 @@ class ReconServer:
             CUDA graphs (default True; see :class:`VcdRun`).  Results are
             bitwise the same either way; the graphs take the per-kernel
             launch work off the scheduler thread.
+        batching: step the iterations of resident jobs that share a geometry
+            (and storage, options and partition shape) together, each kernel
+            of their subset steps launched once for all of them
+            (:func:`vcd_run.enqueue_batched_iteration`, up to 16 jobs).  A job
+            that becomes ready while a same-geometry partner is still running
+            waits up to ``batch_hold_s`` for it, so that partners fall into
+            step.  Results are bitwise the same batched or not.
+        admission: 'fifo' (the default) admits waiting requests in arrival
+            order; 'shortest' admits the one with the least estimated work
+            first (voxel-views per iteration times iterations), except that a
+            request waiting longer than ``max_wait_s`` goes first, in arrival
+            order (the wait bound caps how long a large job can be passed
+            over).
     """
 
     def __init__(self, device=None, memory_budget_bytes=None, max_active=8,
-                 storage_dtype='float16', cuda_graphs=True):
+                 storage_dtype='float16', cuda_graphs=True, admission='fifo',
+                 max_wait_s=20.0, batching=True, batch_hold_s=0.05):
         self.device = torch.device('cuda', torch.cuda.current_device()) if device is None \
             else torch.device(device)
         if memory_budget_bytes is None:
@@ -142,6 +156,14 @@ class ReconServer:
             memory_budget_bytes = int(0.8 * free)
         self.ledger = MemoryLedger(memory_budget_bytes)
         self.max_active = int(max_active)
+        if admission not in ('fifo', 'shortest'):
+            raise ValueError(f"admission must be 'fifo' or 'shortest', got {admission!r}")
+        self.admission = admission
+        self.max_wait_s = float(max_wait_s)
+        self.batching = bool(batching)
+        self.batch_hold_s = float(batch_hold_s)
+        self._batch_stream = None
+        self.batched_iterations = 0   # job-iterations run inside a batch
         self.storage_dtype = storage_dtype
         self.cuda_graphs = bool(cuda_graphs)
         storage_code(storage_dtype)
@@ -168,6 +190,7 @@ class ReconServer:
             self.t0 = now
         r = Request(self._next_id, model, sinogram, weights, max_iterations,
                     stop_threshold_change_pct, seed, now if arrival is None else arrival)
+        r.work = self.estimated_work(model, max_iterations)
         self._next_id += 1
         self.waiting.append(r)
         return r
@@ -184,6 +207,25 @@ class ReconServer:
                                                max_iterations)
         max_ps = max((-(-n_pix // min(int(gran[int(i)]), n_pix)) for i in seq), default=1)
         return MemoryLedger.job_bytes(model, self.storage_dtype, weighted, max_ps)
+
+    @staticmethod
+    def estimated_work(model, max_iterations):
+        """Voxel-views a request projects: ROR pixels x slices x views per
+        projector pass, times its iterations."""
+        V = model.get_params('sinogram_shape')[0]
+        rs, ror = model.get_params(['recon_shape', 'use_ror_mask'])
+        n_pix = int(vcd_utils.get_2d_ror_mask(rs, use_ror_mask=ror).sum()) \
+            if ror is not False else rs[0] * rs[1]
+        return float(n_pix) * rs[2] * V * max(1, int(max_iterations))
+
+    def _next_waiting(self):
+        """Index in ``waiting`` of the request to admit next."""
+        if self.admission == 'fifo' or len(self.waiting) == 1:
+            return 0
+        now = time.perf_counter()
+        if now - self.waiting[0].arrival > self.max_wait_s:
+            return 0   # the oldest has waited past the bound
+        return min(range(len(self.waiting)), key=lambda k: (self.waiting[k].work, k))
 
     def _admit_state(self, r):
         m = r.model
@@ -295,9 +337,49 @@ class ReconServer:
         r._state = state
         return r
 
+    def _enqueue_ready(self, ready):
+        """Enqueue the next iteration of each ready job: same-key jobs as one
+        batch; a job whose same-geometry partner is still running waits for
+        it (up to batch_hold_s)."""
+        from .vcd_run import enqueue_batched_iteration
+        now = time.perf_counter()
+        groups = {}
+        for r in ready:
+            key = r._run.batch_key() if self.batching else None
+            groups.setdefault(key if key is not None else ('solo', r.id), []).append(r)
+        # jobs with an iteration in flight, by the batch key of the iteration
+        # they will take next
+        running = {}
+        if self.batching:
+            for r in self.active:
+                run = r._run
+                if run is not None and run._event is not None and r._out_event is None and \
+                        run.done + 1 < len(run.seq):
+                    nxt = tuple(run.parts_dev[int(run.seq[run.done + 1])].shape)
+                    running.setdefault((run.batch_key_geometry(), nxt), []).append(r)
+        for key, rs in groups.items():
+            if self.batching and key[0] != 'solo':
+                partners = running.get((key[0], key[2]), [])
+                if partners and len(rs) < 16 and \
+                        now - min(r._ready_since for r in rs) < self.batch_hold_s:
+                    continue   # a partner is finishing its iteration: wait for it
+            for k in range(0, len(rs), 16):
+                chunk = rs[k:k + 16]
+                if len(chunk) == 1:
+                    chunk[0]._run.enqueue_iteration()
+                else:
+                    if self._batch_stream is None:
+                        self._batch_stream = torch.cuda.Stream(self.device)
+                    with torch.cuda.device(self.device):
+                        enqueue_batched_iteration([r._run for r in chunk], self._batch_stream)
+                    self.batched_iterations += len(chunk)
+                for r in chunk:
+                    r._ready_since = None
+
     def step(self):
         """One scheduler pass; returns True if it did anything."""
         busy = False
+        ready = []
         # advance the admitted jobs
         for r in list(self.active):
             if r._out_event is not None:
@@ -318,11 +400,19 @@ class ReconServer:
                 if r._run.collect():
                     self._finish(r)
                 else:
-                    r._run.enqueue_iteration()
+                    r._ready_since = time.perf_counter()
+                    ready.append(r)
                 busy = True
-        # admit waiting requests in arrival order while slots and memory allow
+        # jobs held for a same-geometry partner from an earlier pass
+        ready += [r for r in self.active if r._run is not None and r._out_event is None
+                  and getattr(r, '_ready_since', None) is not None and r not in ready]
+        if ready:
+            self._enqueue_ready(ready)
+        # admit waiting requests (in the admission policy's order) while
+        # slots and memory allow
         while self.waiting and len(self.active) < self.max_active:
-            r = self.waiting[0]
+            k = self._next_waiting()
+            r = self.waiting[k]
             try:
                 if not self._admit(r):
                     break
@@ -336,11 +426,11 @@ class ReconServer:
                 if r._charge:
                     self.ledger.release(r._charge)
                     r._charge = 0
-                self.waiting.pop(0)
+                self.waiting.pop(k)
                 self.completed.append(r)
                 busy = True
                 continue
-            self.waiting.pop(0)
+            self.waiting.pop(k)
             self.active.append(r)
             busy = True
         self.max_concurrent = max(self.max_concurrent, len(self.active))
@@ -387,4 +477,5 @@ class ReconServer:
             'p50_latency_s': float(np.percentile(lat, 50)) if ok else math.nan,
             'p99_latency_s': float(np.percentile(lat, 99)) if ok else math.nan,
             'max_concurrent': self.max_concurrent, 'span_s': span,
+            'batched_iterations': self.batched_iterations,
         }

@@ -16,6 +16,8 @@ lives on the device in the resident form:
   ``vcd_partition_iterator``).
 """
 
+import ctypes
+
 import numpy as np
 import torch
 
@@ -163,6 +165,48 @@ class VcdEngine:
                   stream_of(self.device))
         del order_np
         return accum
+
+
+def partition_pass_batched(engines, flats, errs, partitions, orders, accums=None):
+    """One VCD iteration of several reconstructions that share a geometry,
+    each kernel of the subset step launched once for all of them
+    (``mbir_vcd_partition_pass_batched``): job j updates the subsets of
+    ``partitions[j]`` (all (K, n)) in ``orders[j]``, exactly as its own
+    :meth:`VcdEngine.partition_pass` would."""
+    n = len(engines)
+    if not 1 <= n <= _lib.MAX_BATCH:
+        raise ValueError(f'a batch holds 1 to {_lib.MAX_BATCH} jobs, got {n}')
+    e0 = engines[0]
+    parts = [_lib.as_i64_contig(p) for p in partitions]
+    K, npix = parts[0].shape
+    for p in parts:
+        if tuple(p.shape) != (K, npix):
+            raise ValueError('every job of a batch needs partitions of the same shape')
+    require_cuda(*flats, *parts)
+    for e in engines:
+        e.reserve(npix)
+    accums = [e.accum for e in engines] if accums is None else list(accums)
+    c = ctypes
+
+    keep = []   # the host arrays must outlive the call
+
+    def arr(vals):
+        a = (c.c_void_p * n)(*[None if v is None else v.data_ptr() for v in vals])
+        keep.append(a)
+        return c.cast(a, c.c_void_p)
+
+    params_arr = (VcdParams * n)(*[e.params for e in engines])
+    params = c.cast(params_arr, c.c_void_p)
+    order = np.ascontiguousarray(np.stack([np.asarray(o) for o in orders]).astype(np.int32))
+    ws_bytes = min(e.workspace_bytes() for e in engines)
+    _lib.call(e0.device, 'mbir_vcd_partition_pass_batched', n, e0.geom, ptr(e0.view_params),
+              params, arr(flats), arr([r.data for r in errs]), arr([r.scale for r in errs]),
+              arr([None if e.weights is None else e.weights.data for e in engines]),
+              arr([None if e.weights is None else e.weights.scale for e in engines]),
+              arr([e.H for e in engines]), ptr(e0.dc), arr(parts), K, npix,
+              order.ctypes.data_as(c.c_void_p), arr(accums), arr([e._ws for e in engines]),
+              ws_bytes, stream_of(e0.device))
+    return accums
 
 
 def _refresh(engine, flat_recon, err, pixel_indices, y_vcr):

@@ -88,6 +88,7 @@ class VcdRun:
         self._graphs = {}
         self._graph_shapes = set()
         self.graph_replays = 0
+        self.batched_passes = 0
 
     # ── device preparation ───────────────────────────────────────────────
     def prepare(self):
@@ -262,25 +263,62 @@ class VcdRun:
         """Enqueue iteration ``self.done`` on the run's stream (no sync)."""
         if self.finished or self._event is not None:
             raise RuntimeError('no iteration can be enqueued now')
-        i = self.done
         with torch.cuda.stream(self.stream):
-            if self.finish_at is not None and i >= self.finish_at:
-                self._finish_in_float16()
-            part = self.parts_dev[int(self.seq[i])]
-            order = order_array(part.shape[0], self.rng)
-            self.engine.accum.zero_()
+            part, order = self._begin_iteration()
             if tuple(part.shape) in self._graph_shapes and not _lib.timing_enabled():
                 self._graph_pass(part, order)
             else:
                 self.engine.partition_pass(self.flat, self.err, part, order)
-            if self.y_vcr is not None and (i + 1) % self.refresh == 0:
-                self.engine.refresh_error(self.flat, self.err, self.model.full_indices_device(),
-                                          self.y_vcr)
-            stats = iteration_stats(self.err, self.w_res, self.flat)
-            self.host.copy_(torch.cat([self.engine.accum, stats]), non_blocking=True)
-            self._event = torch.cuda.Event()
-            self._event.record(self.stream)
-            self._pending = part.shape[0]
+            self._end_iteration(part)
+
+    # The pieces of an iteration, on the current stream (a run's own, or the
+    # stream of a batch of runs, enqueue_batched_iteration).
+    def _begin_iteration(self):
+        i = self.done
+        if self.finish_at is not None and i >= self.finish_at:
+            self._finish_in_float16()
+        part = self.parts_dev[int(self.seq[i])]
+        order = order_array(part.shape[0], self.rng)
+        self.engine.accum.zero_()
+        return part, order
+
+    def _end_iteration(self, part):
+        i = self.done
+        # (no refresh after the last iteration, whose error sinogram only
+        # feeds the statistics, nor right before the float16 finish, which
+        # re-forms it anyway)
+        if self.y_vcr is not None and (i + 1) % self.refresh == 0 and \
+                i + 1 < len(self.seq) and i + 1 != self.finish_at:
+            self.engine.refresh_error(self.flat, self.err, self.model.full_indices_device(),
+                                      self.y_vcr)
+        stats = iteration_stats(self.err, self.w_res, self.flat)
+        self.host.copy_(torch.cat([self.engine.accum, stats]), non_blocking=True)
+        self._event = torch.cuda.Event()
+        self._event.record(torch.cuda.current_stream(self.model.torch_device))
+        self._pending = part.shape[0]
+
+    def batch_key_geometry(self):
+        """The part of :meth:`batch_key` that does not change from iteration
+        to iteration (geometry, view parameters, options, device)."""
+        m = self.model
+        g = m._geometry()
+        return (tuple(getattr(g, f) for f, _ in g._fields_),
+                np.asarray(m._view_params_array()).tobytes(),
+                bool(m.get_params('positivity_flag')), self.w_res is None,
+                self.prox_flat is None, str(m.torch_device))
+
+    def batch_key(self):
+        """Runs with equal keys can take their next iteration as one batch
+        (:func:`enqueue_batched_iteration`): the same geometry and view
+        parameters, storage (after a float16 finish due now), options and
+        partition shape.  None when the run cannot be batched."""
+        if self.finished or self._event is not None:
+            return None
+        storage = self.storage
+        if self.finish_at is not None and self.done >= self.finish_at:
+            storage = _lib.MBIR_F16
+        return (self.batch_key_geometry(), storage,
+                tuple(self.parts_dev[int(self.seq[self.done])].shape))
 
     def ready(self):
         return self._event is not None and self._event.query()
@@ -444,6 +482,7 @@ class VcdRun:
         run.cuda_graphs = bool(cuda_graphs)
         run._graphs = {}
         run.graph_replays = 0
+        run.batched_passes = 0
         run.refresh = int(state['refresh'])
         run.constant_weights = bool(state['constant_weights'])
         dev = model.torch_device
@@ -489,3 +528,30 @@ class VcdRun:
         if self._graph_shapes:
             n += (self._ordered.numel() + self._order_dev.numel()) * 8
         return n
+
+
+def enqueue_batched_iteration(runs, stream):
+    """The next iteration of several runs with equal :meth:`VcdRun.batch_key`
+    as one batch on ``stream``: each kernel of each subset step is launched
+    once for all of them (``mbir_vcd_partition_pass_batched``); every run's
+    subsets, orders, statistics and results are its own.  ``stream`` waits
+    for the runs' own streams first, and they wait for it afterwards."""
+    from .vcd_engine import partition_pass_batched
+    if len(runs) == 1:
+        runs[0].enqueue_iteration()
+        return
+    key = runs[0].batch_key()
+    if key is None or any(r.batch_key() != key for r in runs[1:]):
+        raise ValueError('runs of a batch must share batch_key()')
+    with torch.cuda.stream(stream):
+        for r in runs:
+            stream.wait_stream(r.stream)
+        items = [r._begin_iteration() for r in runs]
+        partition_pass_batched([r.engine for r in runs], [r.flat for r in runs],
+                               [r.err for r in runs], [p for p, _ in items],
+                               [o for _, o in items])
+        for r, (part, _) in zip(runs, items):
+            r._end_iteration(part)
+            r.batched_passes += 1
+    for r in runs:
+        r.stream.wait_stream(stream)

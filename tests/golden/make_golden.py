@@ -25,6 +25,9 @@ Cases
                     (automatic sigma_prox) and cone (given sigma_prox)
   denoise.npz       QGGMRFDenoiser: noise estimate and seeded denoise runs
                     (given and estimated sigma_noise)
+  autograd.npz      the reference's autograd gradient of a weighted residual
+                    loss through forward_project_differentiable (parallel,
+                    cone)
   recon_simple_parallel_128.npz
                     the one-call parallel recon at the reference's CPU
                     configuration: a 128 x 128 x 16 ellipsoid phantom, 180
@@ -426,8 +429,42 @@ def recon_simple_parallel_case():
     print(f'wrote recon_simple_parallel_128 ({secs:.1f} s on the CPU)')
 
 
+def autograd_case():
+    """The reference's own autograd (forward_project_differentiable) on a
+    parallel and a cone model: the gradient of sum w (A x - y)^2 at a seeded
+    volume, with its inputs."""
+    out = {}
+    for tag in ('par', 'cone'):
+        shape = (24, 16, 16)
+        if tag == 'par':
+            m = _quiet(mbirtorch.ParallelBeamModel(
+                shape, np.linspace(0, np.pi, shape[0], endpoint=False), compile_mode='off'))
+        else:
+            m = _quiet(mbirtorch.ConeBeamModel(
+                shape, np.linspace(0, 2 * np.pi, shape[0], endpoint=False),
+                source_detector_dist=96.0, source_iso_dist=64.0, compile_mode='off'))
+        m.configure_devices(devices=['cpu'])
+        rs = tuple(m.get_params('recon_shape'))
+        g = torch.Generator().manual_seed(71)
+        x = torch.rand(rs, generator=g, dtype=torch.float32)
+        y = torch.rand(shape, generator=g, dtype=torch.float32)
+        w = torch.rand(shape, generator=g, dtype=torch.float32) + 0.5
+        xr = x.clone().requires_grad_(True)
+        from mbirtorch.autograd import forward_project_differentiable
+        s = forward_project_differentiable(m, xr)
+        loss = (w * (s - y) ** 2).sum()
+        loss.backward()
+        out[f'{tag}_x'], out[f'{tag}_y'], out[f'{tag}_w'] = x.numpy(), y.numpy(), w.numpy()
+        out[f'{tag}_grad'] = xr.grad.numpy()
+        out[f'{tag}_loss'] = np.array(float(loss))
+        out[f'{tag}_recon_shape'] = np.array(rs)
+    np.savez_compressed(os.path.join(HERE, 'autograd.npz'), **out)
+    print('wrote autograd')
+
+
 CASES = ['projector_cases', 'qggmrf_case', 'partition_case', 'autoreg_and_direct_cases',
-         'recon_cases', 'prox_cases', 'denoise_case', 'recon_simple_parallel_case']
+         'recon_cases', 'prox_cases', 'denoise_case', 'recon_simple_parallel_case',
+         'autograd_case']
 
 if __name__ == '__main__':
     for name in (sys.argv[1:] or CASES):

@@ -156,7 +156,7 @@ def test_dc_sum_chunks_run_along_grid_x():
     a subset of every pixel of a 2048 x 2048 volume (131,072 chunks, above
     the 65,535 grid-y limit) is launchable."""
     src = open(os.path.join(ROOT, 'mbirtorch_b200', 'csrc', 'capi.cu')).read()
-    m = re.search(r"dim3 gs\(([^,]+),[^;]*;\s*tpre\(st\);\s*launch\(vcd_dc_sums_kernel", src)
+    m = re.search(r"dim3 gs\(([^,]+),[^;]*;\s*tpre\(st\);\s*launchb<DcSumsB>\(gs", src)
     assert m and m.group(1).strip() == 'w.dc_chunks'
     kern = open(os.path.join(ROOT, 'mbirtorch_b200', 'csrc', 'vcd.cuh')).read()
     assert 'const int chunk = blockIdx.x;' in kern

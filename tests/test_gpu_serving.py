@@ -186,3 +186,62 @@ def test_preempt_checkpoint_resume_equals_uninterrupted(storage, tmp_path):
     assert r2.error is None
     assert np.array_equal(r2.recon, alone[0].recon)
     assert r2.recon_params['fm_rmse'] == alone[0].recon_params['fm_rmse']
+
+
+def test_served_bfloat16_results_against_fp64_oracle():
+    """Served with bfloat16 storage (admission by the ledger, jobs resident
+    together): a parallel, a cone and a two-turn helical cone job, 128^2 x 16
+    with Poisson data and 10 iterations, each within 1e-3 of the FP64
+    oracle's seeded reconstruction of the same data and partitions."""
+    from oracle import vcd as ovcd
+    from _cases import oracle_problem
+    N, S, V = 128, 16, 180
+    C = int(1.5 * N)
+
+    def make(kind):
+        if kind == 'parallel':
+            m = mb.ParallelBeamModel((V, S, C), np.linspace(0, np.pi, V, endpoint=False))
+        else:
+            if kind == 'helical':
+                ang = (2 * np.pi / (V // 2)) * np.arange(V)
+                zs = np.linspace(-S, S, V)
+            else:
+                ang, zs = np.linspace(0, 2 * np.pi, V, endpoint=False), None
+            m = mb.ConeBeamModel((V, S, C), ang, source_detector_dist=4.0 * N,
+                                 source_iso_dist=2.0 * N, helical_z_shifts=zs)
+            m.set_params(no_warning=True, delta_det_channel=2.0, delta_det_row=2.0)
+            m.auto_set_recon_geometry(no_warning=True)
+        m.set_params(no_warning=True, verbose=0, recon_shape=(N, N, S))
+        return m
+
+    jobs = []
+    for i, kind in enumerate(['parallel', 'cone', 'helical']):
+        m = make(kind)
+        clean = m.forward_project(_phantom((N, N, S), 30 + i))
+        mu = 3.0 / float(clean.max())
+        counts = np.random.default_rng(40 + i).poisson(1e4 * np.exp(-mu * clean))
+        jobs.append((kind, (-np.log(np.maximum(counts, 1) / 1e4) / mu).astype(np.float32)))
+    srv = ReconServer(storage_dtype='bfloat16', max_active=3)
+    reqs = [srv.submit(make(kind), sino, max_iterations=10, seed=50 + i)
+            for i, (kind, sino) in enumerate(jobs)]
+    srv.run_until_idle(timeout_s=600)
+    assert srv.stats()['failed'] == 0
+    for i, ((kind, sino), r) in enumerate(zip(jobs, reqs)):
+        m = make(kind)
+        reg = m.auto_set_regularization_params(sino)
+        prob = oracle_problem(m)
+        # the server draws a job's partitions and orders from RandomState(seed)
+        rng = np.random.RandomState(50 + i)
+        state = np.random.get_state()
+        np.random.set_state(rng.get_state())
+        try:
+            parts = [ovcd.pixel_partition(prob.recon_shape, n)
+                     for n in m.get_params('granularity')]
+            seq = ovcd.partition_sequence(m.get_params('partition_sequence'), 10)
+            dc = ovcd.dc_damping_profile(prob) if kind != 'parallel' else None
+            orec, _ = ovcd.recon(prob, sino, reg['sigma_y'], reg['sigma_x'], parts, seq,
+                                 dc_profile=dc)
+        finally:
+            np.random.set_state(state)
+        err = float(np.linalg.norm(r.recon - orec) / np.linalg.norm(orec))
+        assert err <= 1e-3, (kind, err)

@@ -48,3 +48,28 @@ def test_job_charge_matches_drawn_partitions():
         max_ps = max(int(parts[int(i)].shape[1]) for i in seq)
         assert srv.job_charge(m, False, iters) == \
             MemoryLedger.job_bytes(m, 'float16', False, max_ps)
+
+
+def test_admission_policy_shortest_first_with_wait_bound(monkeypatch):
+    """'shortest' admits the waiting request with the least estimated work
+    (pixels x slices x views x iterations); a request waiting past max_wait_s
+    goes first; 'fifo' keeps arrival order."""
+    import time
+    from mbirtorch_b200.serving import ReconServer
+    now = time.perf_counter()
+    big, mid, small = _cone((80, 24, 48)), _cone((40, 12, 24)), _cone((20, 6, 12))
+    srv = ReconServer(device='cuda:0', memory_budget_bytes=1 << 30, storage_dtype='float16',
+                      admission='shortest', max_wait_s=5.0)
+    reqs = [srv.submit(m, None, max_iterations=10, arrival=now) for m in (big, mid, small)]
+    assert reqs[2].work < reqs[1].work < reqs[0].work
+    assert srv._next_waiting() == 2
+    srv.waiting[0].arrival = now - 10.0      # the oldest has waited past the bound
+    assert srv._next_waiting() == 0
+    fifo = ReconServer(device='cuda:0', memory_budget_bytes=1 << 30, storage_dtype='float16',
+                       admission='fifo')
+    for m in (big, small):
+        fifo.submit(m, None, max_iterations=10, arrival=now)
+    assert fifo._next_waiting() == 0
+    rs = small.get_params('recon_shape')
+    n_pix = int(mb.get_2d_ror_mask(rs).sum())
+    assert reqs[2].work == n_pix * rs[2] * 20 * 10
