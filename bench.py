@@ -828,6 +828,73 @@ def serving_mix_extra(mb, torch, n_jobs=16):
             "max_rel_l2_served_vs_plain_f32": max(rel)}
 
 
+def serving_batching_extra(mb, torch, jobs=8, iters=10):
+    """Cross-job batching on a scanner-protocol workload: `jobs` requests of
+    one geometry (own phantoms, noise and seeds) submitted together, served
+    with same-geometry batching (each kernel of a subset step launched once
+    for all of them) and without it (each job on its own stream), float16
+    storage, CUDA graphs on; medians of three interleaved runs per arm.
+    Two protocols: a small parallel scan (128^2 x 16, 180 views, 16 x 192)
+    and a medium cone scan (256^2 x 64, 360 views, 64 x 384 flat, pitch 2,
+    magnification 2)."""
+    from mbirtorch_b200.serving import ReconServer
+    dev = torch.device("cuda", 0)
+
+    def protocols():
+        def par():
+            m = mb.ParallelBeamModel((180, 16, 192), np.linspace(0, np.pi, 180, endpoint=False))
+            m.set_params(no_warning=True, verbose=0, recon_shape=(128, 128, 16))
+            return m
+
+        def cone():
+            m = mb.ConeBeamModel((360, 64, 384), np.linspace(0, 2 * np.pi, 360, endpoint=False),
+                                 source_detector_dist=1024.0, source_iso_dist=512.0)
+            m.set_params(no_warning=True, delta_det_channel=2.0, delta_det_row=2.0)
+            m.auto_set_recon_geometry(no_warning=True)
+            m.set_params(no_warning=True, verbose=0, recon_shape=(256, 256, 64))
+            return m
+        return {"parallel 128^2 x 16, 180 views": par, "cone 256^2 x 64, 360 views": cone}
+
+    out = {"jobs": jobs, "iterations": iters, "storage": "float16"}
+    for name, make in protocols().items():
+        sinos = []
+        for j in range(jobs):
+            m = make()
+            rs = tuple(m.get_params('recon_shape'))
+            with torch.no_grad():
+                vol = phantom_torch(torch, rs, 500 + j, dev)
+                clean = m.forward_project(vol, output_sharded=True)
+                mu = 3.0 / float(clean.max())
+                gen = torch.Generator(device=dev).manual_seed(600 + j)
+                counts = torch.poisson(I0 * torch.exp(-mu * clean), generator=gen)
+                sinos.append((-torch.log(torch.clamp(counts, min=1.0) / I0) / mu).cpu().numpy())
+
+        def serve(batching):
+            srv = ReconServer(storage_dtype="float16", max_active=jobs, batching=batching)
+            t0 = time.perf_counter()
+            reqs = [srv.submit(make(), s, max_iterations=iters, seed=700 + j, arrival=t0)
+                    for j, s in enumerate(sinos)]
+            srv.run_until_idle(timeout_s=600)
+            torch.cuda.synchronize()
+            return time.perf_counter() - t0, reqs, srv.batched_iterations
+
+        serve(True)
+        serve(False)
+        t_b, t_n = [], []
+        for _ in range(3):
+            tb, rb, nb = serve(True)
+            tn, rn, _ = serve(False)
+            t_b.append(tb)
+            t_n.append(tn)
+        same = all(np.array_equal(a.recon, b.recon) for a, b in zip(rb, rn))
+        out[name] = {"batched_recons_per_s": jobs / float(np.median(t_b)),
+                     "per_job_streams_recons_per_s": jobs / float(np.median(t_n)),
+                     "batched_over_streams": float(np.median(t_n)) / float(np.median(t_b)),
+                     "samples_s": {"batched": t_b, "per_job_streams": t_n},
+                     "batched_job_iterations": nb, "results_bitwise_equal": bool(same)}
+    return out
+
+
 # ── serving configuration: 200 requests with Poisson arrivals ──────────────
 def config5_jobs(mb, torch, n_jobs=200, rate=5.0, seed=11):
     """The serving configuration: n_jobs requests with Poisson arrivals at
@@ -1156,7 +1223,7 @@ def main():
 
 
 EXTRAS = ("roofline", "cpu_baseline", "projectors", "mixed_precision", "cone256_flat",
-          "parallel_subset", "serving_mix", "autograd", "triton_reference")
+          "parallel_subset", "serving_mix", "serving_batching", "autograd", "triton_reference")
 
 
 def extras(args, m, mb, torch, dev, y, rec_ref, full=True):
@@ -1197,6 +1264,7 @@ def extras(args, m, mb, torch, dev, y, rec_ref, full=True):
     run("cone256_flat", lambda: cone256_extra(mb, torch, dev))
     run("parallel_subset", lambda: parallel_subset_extra(mb, torch, hbm))
     run("serving_mix", lambda: serving_mix_extra(mb, torch))
+    run("serving_batching", lambda: serving_batching_extra(mb, torch))
     run("autograd", lambda: autograd_extra(mb, torch))
     run("triton_reference", lambda: triton_reference_extra(mb, torch))
     return res
