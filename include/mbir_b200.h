@@ -29,6 +29,9 @@
  *                            and driven by Projectors.
  *                            sparse_forward_project_view_range
  *                            (projectors.py:518-588)
+ *   mbir_forward_project_binned <- the same bodies for whole cylinders, through
+ *                            channel-sorted bins (forward_project,
+ *                            tomography_model.py:1877-1909)
  *   mbir_back_project     <- _parallel_back_view_batch (parallel_beam.py:76-94)
  *                            and _cone_back_view_batch (cone_beam.py:237-299),
  *                            driven by sparse_back_project_view_range
@@ -178,6 +181,33 @@ int32_t mbir_forward_project_volume(const mbir_geometry *geom, const float *view
                                     const float *flat_volume, const int64_t *pixel_indices,
                                     int64_t num_pixels, float *sino_out, int32_t out_layout,
                                     void *stream);
+
+/* Forward projection of whole cylinders through channel-sorted bins: per
+ * chunk of views, every (view, pixel) record is formed once and sorted by
+ * centre channel, and each (view, 16-channel block) CTA walks only the
+ * pixels that reach it (the scanning forward above tests every pixel in
+ * every block).  Same operator as mbir_forward_project_volume (values_by_pixel
+ * 1: values is the flat (N*N, num_slices) volume read at rows
+ * pixel_indices[p]) or mbir_forward_project with slice_start 0 and band_len
+ * num_slices (values_by_pixel 0: values is (num_pixels, num_slices)); the
+ * sums run in another fixed order, so results agree with those to FP32
+ * rounding.  Covers the geometries with psf radius 1 and at most 1024
+ * detector rows (MBIR_ERR_INVALID otherwise).  The workspace (256-byte
+ * aligned) holds the bins of as many views as fit; a larger one means fewer
+ * chunks.  Replaces _parallel_forward_view_batch / _cone_forward_view_batch
+ * (parallel_beam.py:56-73, cone_beam.py:161-234) for whole volumes. */
+int32_t mbir_forward_project_binned(const mbir_geometry *geom, const float *view_params,
+                                    int32_t view_start, int32_t view_count,
+                                    const float *values, int32_t values_by_pixel,
+                                    const int64_t *pixel_indices, int64_t num_pixels,
+                                    float *sino_out, int32_t out_layout, void *workspace,
+                                    size_t workspace_bytes, void *stream);
+
+/* Workspace bytes for mbir_forward_project_binned: the bins of
+ * min(view_count, views whose records fit 1 GiB) views, at least one; 0 when
+ * the geometry is not covered. */
+size_t mbir_forward_project_binned_workspace_size(const mbir_geometry *geom,
+                                                  int32_t view_count, int64_t num_pixels);
 
 /* Workspace bytes mbir_back_project needs for this call shape. */
 size_t mbir_back_project_workspace_size(const mbir_geometry *geom,
@@ -330,11 +360,16 @@ int32_t mbir_denoise_pass(int32_t num_rows, int32_t num_cols, int32_t num_slices
  * in the (V, C, R) layout and x the flat (N*N, S) recon at pixel_indices.
  * Part of the storage-precision layer (no counterpart in the reference,
  * whose error sinogram is FP32 and updated in place only): it bounds the
- * drift that in-place 16-bit updates accumulate. */
+ * drift that in-place 16-bit updates accumulate.  With a workspace of
+ * mbir_forward_project_binned_workspace_size(geom, num_views, num_pixels)
+ * bytes (256-byte aligned; any size holding one view's bins) A x is formed
+ * through the channel-sorted bins; with none (NULL), by the scanning
+ * forward. */
 int32_t mbir_vcd_refresh_error(const mbir_geometry *geom, const float *view_params,
                                const float *flat_recon, const int64_t *pixel_indices,
                                int64_t num_pixels, const float *y_vcr, void *error_sino,
-                               const float *err_scale, int32_t storage, void *stream);
+                               const float *err_scale, int32_t storage, void *workspace,
+                               size_t workspace_bytes, void *stream);
 
 /* Per-iteration statistics in FP64 (device out[4]):
  *   out[0] = sum(w e^2)  (sum(e^2) without weights)

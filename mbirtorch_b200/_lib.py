@@ -17,6 +17,7 @@ import torch
 from . import _build
 
 MBIR_OK = 0
+MBIR_ERR_INVALID, MBIR_ERR_CUDA, MBIR_ERR_WORKSPACE = 1, 2, 3
 MBIR_PARALLEL, MBIR_CONE = 0, 1
 MBIR_LAYOUT_VRC, MBIR_LAYOUT_VCR = 0, 1
 MBIR_F32, MBIR_BF16, MBIR_F16 = 0, 1, 2
@@ -91,7 +92,11 @@ SIGNATURES = {
                                     _i32, _vp]),
     "mbir_forward_project_volume": (_i32, [_GP, _vp, _i32, _i32, _vp, _vp, _i64, _vp, _i32,
                                            _vp]),
-    "mbir_vcd_refresh_error": (_i32, [_GP, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i32, _vp]),
+    "mbir_forward_project_binned": (_i32, [_GP, _vp, _i32, _i32, _vp, _i32, _vp, _i64, _vp,
+                                           _i32, _vp, _sz, _vp]),
+    "mbir_forward_project_binned_workspace_size": (_sz, [_GP, _i32, _i64]),
+    "mbir_vcd_refresh_error": (_i32, [_GP, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i32, _vp, _sz,
+                                      _vp]),
     "mbir_back_project_workspace_size": (_sz, [_GP, _i32, _i64, _i32]),
     "mbir_back_project": (_i32, [_GP, _vp, _i32, _i32, _vp, _i32, _vp, _i64, _i32, _i32, _i32,
                                  _vp, _vp, _sz, _vp]),

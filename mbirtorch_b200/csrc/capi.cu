@@ -542,8 +542,8 @@ struct FwdBins {
   int views;               // views per chunk
 };
 
-size_t bin_smem(const mbir_geometry *g) {
-  return sizeof(int) * (size_t)fwd_nkeys(g->num_det_channels) * (1 + kThreads / 32);
+size_t bin_smem(const mbir_geometry *g, int nthr = kThreads) {
+  return sizeof(int) * (size_t)fwd_nkeys(g->num_det_channels) * (1 + nthr / 32);
 }
 
 // The binned forward where the row-tiled one applies and the binning's
@@ -562,9 +562,23 @@ bool use_par_binned(const mbir_geometry *g) {
 
 bool use_binned(const mbir_geometry *g) { return use_cone_binned(g) || use_par_binned(g); }
 
+// by_pixel: the records name the cylinder's row of `values` as pix[p] (a
+// flat volume) instead of the subset slot p.  wide: whole-volume bins, with
+// kBinWideThreads threads per view where their counters fit shared memory.
 int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count,
-               const int64_t *pix, long long P, const FwdBins &b, cudaStream_t st) {
+               const int64_t *pix, long long P, const FwdBins &b, cudaStream_t st,
+               int by_pixel = 0, bool wide = false) {
   const Geo geo = make_geo(*g);
+  if (wide && bin_smem(g, kBinWideThreads) <= (size_t)device_attrs().smem_optin) {
+    const size_t smem_w = bin_smem(g, kBinWideThreads);
+    const int rc_smem = request_smem(cone_bin_wide_kernel, smem_w, "forward binning");
+    if (rc_smem) return rc_smem;
+    tpre(st);
+    launch(cone_bin_wide_kernel, v_count, kBinWideThreads, smem_w, st, geo, vp, v_start, pix,
+           (int)P, by_pixel, b.recs, b.list, b.offs);
+    MBIR_CHECK_LAUNCH("forward binning");
+    return MBIR_OK;
+  }
   const size_t smem = bin_smem(g);
   {
     const int rc_smem = request_smem(cone_bin_kernel, smem, "forward binning");
@@ -572,7 +586,7 @@ int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count
   }
   tpre(st);
   launchb<ConeBinB>(v_count, kThreads, smem, st, "vcd forward binning", geo, vp, v_start, pix,
-                    (int)P, 0, b.recs, b.list, b.offs);
+                    (int)P, by_pixel, b.recs, b.list, b.offs);
   MBIR_CHECK_LAUNCH("vcd forward binning");
   return MBIR_OK;
 }
@@ -588,7 +602,7 @@ int launch_binned(const mbir_geometry *g, int v_start, int v_count, const float 
     const int rc_smem = request_smem(k, smem, "forward");
     if (rc_smem) return rc_smem;
   }
-  dim3 grid(fwd_nblk(g), v_count);
+  const dim3 grid = EPI::kViewFastest ? dim3(v_count, fwd_nblk(g)) : dim3(fwd_nblk(g), v_count);
   tpre(st);
   launchb<FwdConeBinnedB<EPI>>(grid, cone_rt_threads(g), smem, st, what, geo, v_start, values,
                                (int)P, band, 0, (const ConeFwdRec *)b.recs, (const int *)b.list,
@@ -605,8 +619,8 @@ int launch_par_binned(const mbir_geometry *g, int v_start, int v_count, const fl
     return fail(MBIR_ERR_INVALID, "%s: the binned parallel forward projects whole cylinders "
                 "(band %d, detector rows %d)", what, band, g->num_det_rows);
   const Geo geo = make_geo(*g);
-  if (band % 4 == 0 && band >= 128) {
-    // four rows per thread
+  if (band % 4 == 0 && band >= 128 && (reinterpret_cast<uintptr_t>(values) & 15) == 0) {
+    // four rows per thread (one 16-byte load of a cylinder's four rows)
     const int nthr4 = (band / 4 + 31) / 32 * 32;
     const size_t smem4 = par_binned4_smem(nthr4);
     auto k4 = forward_parallel_binned4_kernel<EPI>;
@@ -614,7 +628,8 @@ int launch_par_binned(const mbir_geometry *g, int v_start, int v_count, const fl
       const int rc_smem = request_smem(k4, smem4, "forward");
       if (rc_smem) return rc_smem;
     }
-    dim3 grid(fwd_nblk(g), v_count);
+    const dim3 grid =
+        EPI::kViewFastest ? dim3(v_count, fwd_nblk(g)) : dim3(fwd_nblk(g), v_count);
     tpre(st);
     launchb<FwdParBinned4B<EPI>>(grid, nthr4, smem4, st, what, geo, v_start, values, (int)P,
                                  band, (const ConeFwdRec *)b.recs, (const int *)b.list,
@@ -629,7 +644,7 @@ int launch_par_binned(const mbir_geometry *g, int v_start, int v_count, const fl
     const int rc_smem = request_smem(k, smem, "forward");
     if (rc_smem) return rc_smem;
   }
-  dim3 grid(fwd_nblk(g), v_count);
+  const dim3 grid = EPI::kViewFastest ? dim3(v_count, fwd_nblk(g)) : dim3(fwd_nblk(g), v_count);
   tpre(st);
   launchb<FwdParBinnedB<EPI>>(grid, nthr, smem, st, what, geo, v_start, values, (int)P, band,
                               (const ConeFwdRec *)b.recs, (const int *)b.list,
@@ -676,6 +691,41 @@ int run_forward(const mbir_geometry *g, const float *vp, int v_start, int v_coun
   if (g->geometry == MBIR_CONE) return r1 ? MBIR_FWD(true, 3) : MBIR_FWD(true, 0);
   return r1 ? MBIR_FWD(false, 3) : MBIR_FWD(false, 0);
 #undef MBIR_FWD
+}
+
+// ── binned forward of whole cylinders (the projector entry points) ─────────
+// The bins of views [v0, v0 + vc) for P pixels, carved from a workspace,
+// with `touched` for every view of the geometry (the kernels index it by
+// absolute view).
+constexpr size_t kFullBinBytes = (size_t)1 << 30;  // default record budget
+
+size_t full_bin_bytes(const mbir_geometry *g, long long P, int vc) {
+  return align_up((size_t)vc * P * sizeof(ConeFwdRec)) + align_up((size_t)vc * P * sizeof(int)) +
+         align_up((size_t)vc * (fwd_nkeys(g->num_det_channels) + 1) * sizeof(int)) +
+         align_up((size_t)g->num_views * fwd_nblk(g));
+}
+
+// Views per chunk that `bytes` of workspace hold (0 when not even one).
+int full_bin_views(const mbir_geometry *g, long long P, int view_count, size_t bytes) {
+  const size_t fixed = align_up((size_t)g->num_views * fwd_nblk(g));
+  if (bytes <= fixed) return 0;
+  const size_t per_view = (size_t)P * (sizeof(ConeFwdRec) + sizeof(int)) +
+                          (size_t)(fwd_nkeys(g->num_det_channels) + 1) * sizeof(int);
+  // an upper bound, then down past the alignment padding (at most 768 bytes)
+  int vc = (int)std::min<size_t>((size_t)view_count, (bytes - fixed) / per_view);
+  while (vc > 0 && full_bin_bytes(g, P, vc) > bytes) --vc;
+  return vc;
+}
+
+FwdBins carve_full_bins(const mbir_geometry *g, long long P, int vc, void *ws) {
+  Carver c(ws);
+  FwdBins b;
+  b.recs = c.take<ConeFwdRec>((size_t)vc * P);
+  b.list = c.take<int>((size_t)vc * P);
+  b.offs = c.take<int>((size_t)vc * (fwd_nkeys(g->num_det_channels) + 1));
+  b.touched = c.take<unsigned char>((size_t)g->num_views * fwd_nblk(g));
+  b.views = vc;
+  return b;
 }
 
 int fwd_blocks(const mbir_geometry *g, int band, int v_count) {
@@ -1009,37 +1059,114 @@ int32_t mbir_forward_project_volume(const mbir_geometry *geom, const float *view
                      geom->num_slices, 0, pixel_indices, epi, st, "forward projection", 1);
 }
 
+size_t mbir_forward_project_binned_workspace_size(const mbir_geometry *geom, int32_t view_count,
+                                                  int64_t num_pixels) {
+  if (!geom || view_count <= 0 || num_pixels <= 0 || num_pixels >= (1LL << 31)) return 0;
+  if (geom->num_views <= 0 || geom->num_det_channels <= 0 || !use_binned(geom)) return 0;
+  const size_t per_view = (size_t)num_pixels * (sizeof(ConeFwdRec) + sizeof(int));
+  const int vc = (int)std::max<size_t>(
+      1, std::min<size_t>((size_t)view_count, kFullBinBytes / std::max<size_t>(per_view, 1)));
+  return full_bin_bytes(geom, num_pixels, vc);
+}
+
+int32_t mbir_forward_project_binned(const mbir_geometry *geom, const float *view_params,
+                                    int32_t view_start, int32_t view_count, const float *values,
+                                    int32_t values_by_pixel, const int64_t *pixel_indices,
+                                    int64_t num_pixels, float *sino_out, int32_t out_layout,
+                                    void *workspace, size_t workspace_bytes, void *stream) {
+  int rc = validate_geometry(geom);
+  if (rc) return rc;
+  if (!use_binned(geom))
+    return fail(MBIR_ERR_INVALID, "the binned forward covers psf radius 1 and up to 1024 "
+                "detector rows; use mbir_forward_project");
+  if (view_start < 0 || view_count < 0 || view_start + view_count > geom->num_views)
+    return fail(MBIR_ERR_INVALID, "view range [%d, %d) outside [0, %d)", view_start,
+                view_start + view_count, geom->num_views);
+  if (num_pixels < 0 || num_pixels >= (1LL << 31)) return fail(MBIR_ERR_INVALID, "bad num_pixels");
+  if (out_layout != MBIR_LAYOUT_VRC && out_layout != MBIR_LAYOUT_VCR)
+    return fail(MBIR_ERR_INVALID, "unknown layout %d", out_layout);
+  if (values_by_pixel != 0 && values_by_pixel != 1)
+    return fail(MBIR_ERR_INVALID, "values_by_pixel must be 0 or 1");
+  if (!view_params || !sino_out || (num_pixels > 0 && (!values || !pixel_indices)))
+    return fail(MBIR_ERR_INVALID, "NULL array argument");
+  if (view_count == 0) return MBIR_OK;
+  cudaStream_t st = as_stream(stream);
+  if (num_pixels == 0) {
+    cudaError_t e = cudaMemsetAsync(sino_out, 0,
+        (size_t)view_count * geom->num_det_rows * geom->num_det_channels * sizeof(float), st);
+    if (e != cudaSuccess) return fail(MBIR_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
+    return MBIR_OK;
+  }
+  if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+    return fail(MBIR_ERR_WORKSPACE, "the binned forward needs a 256-byte aligned workspace");
+  const int vc = full_bin_views(geom, num_pixels, view_count, workspace_bytes);
+  if (vc < 1)
+    return fail(MBIR_ERR_WORKSPACE, "workspace of %zu bytes holds no view's bins (%zu needed "
+                "for one)", workspace_bytes, full_bin_bytes(geom, num_pixels, 1));
+  const FwdBins b = carve_full_bins(geom, num_pixels, vc, workspace);
+  const int band = geom->num_slices;
+  StoreSino epi{sino_out, out_layout, geom->num_det_channels, geom->num_det_rows, view_start};
+  for (int v0 = view_start; v0 < view_start + view_count; v0 += vc) {
+    const int nv = std::min(vc, view_start + view_count - v0);
+    rc = launch_bin(geom, view_params, v0, nv, pixel_indices, num_pixels, b, st, values_by_pixel,
+                    true);
+    if (rc) return rc;
+    rc = geom->geometry == MBIR_CONE
+             ? launch_binned(geom, v0, nv, values, num_pixels, band, b, epi, st,
+                             "forward projection (binned)")
+             : launch_par_binned(geom, v0, nv, values, num_pixels, band, b, epi, st,
+                                 "forward projection (binned)");
+    if (rc) return rc;
+  }
+  return MBIR_OK;
+}
+
 int32_t mbir_vcd_refresh_error(const mbir_geometry *geom, const float *view_params,
                                const float *flat_recon, const int64_t *pixel_indices,
                                int64_t num_pixels, const float *y_vcr, void *error_sino,
-                               const float *err_scale, int32_t storage, void *stream) {
+                               const float *err_scale, int32_t storage, void *workspace,
+                               size_t workspace_bytes, void *stream) {
   int rc = validate_geometry(geom);
   if (rc) return rc;
   if (!view_params || !flat_recon || !pixel_indices || !y_vcr || !error_sino || !err_scale ||
       num_pixels <= 0)
     return fail(MBIR_ERR_INVALID, "bad refresh arguments");
+  if (storage != MBIR_F32 && storage != MBIR_BF16 && storage != MBIR_F16)
+    return fail(MBIR_ERR_INVALID, "unknown storage dtype %d", storage);
   cudaStream_t st = as_stream(stream);
   const int C = geom->num_det_channels, R = geom->num_det_rows, V = geom->num_views;
   const int S = geom->num_slices;
+  // Through the bins when a workspace holds at least one view's.
+  const bool binned = workspace != nullptr &&
+                      (reinterpret_cast<uintptr_t>(workspace) & 255) == 0 && use_binned(geom) &&
+                      full_bin_views(geom, num_pixels, V, workspace_bytes) >= 1;
+  auto run = [&](auto epi) -> int {
+    if (!binned)
+      return run_forward(geom, view_params, 0, V, flat_recon, num_pixels, S, 0, pixel_indices,
+                         epi, st, "vcd error refresh", 1);
+    const int vc = full_bin_views(geom, num_pixels, V, workspace_bytes);
+    const FwdBins b = carve_full_bins(geom, num_pixels, vc, workspace);
+    for (int v0 = 0; v0 < V; v0 += vc) {
+      const int nv = std::min(vc, V - v0);
+      int r = launch_bin(geom, view_params, v0, nv, pixel_indices, num_pixels, b, st, 1, true);
+      if (r) return r;
+      r = geom->geometry == MBIR_CONE
+              ? launch_binned(geom, v0, nv, flat_recon, num_pixels, S, b, epi, st,
+                              "vcd error refresh (binned)")
+              : launch_par_binned(geom, v0, nv, flat_recon, num_pixels, S, b, epi, st,
+                                  "vcd error refresh (binned)");
+      if (r) return r;
+    }
+    return MBIR_OK;
+  };
   switch (storage) {
-    case MBIR_F32: {
-      RefreshEpi<float> epi{y_vcr, static_cast<float *>(error_sino), err_scale, C, R};
-      return run_forward(geom, view_params, 0, V, flat_recon, num_pixels, S, 0, pixel_indices,
-                         epi, st, "vcd error refresh", 1);
-    }
-    case MBIR_BF16: {
-      RefreshEpi<__nv_bfloat16> epi{y_vcr, static_cast<__nv_bfloat16 *>(error_sino), err_scale,
-                                    C, R};
-      return run_forward(geom, view_params, 0, V, flat_recon, num_pixels, S, 0, pixel_indices,
-                         epi, st, "vcd error refresh", 1);
-    }
-    case MBIR_F16: {
-      RefreshEpi<__half> epi{y_vcr, static_cast<__half *>(error_sino), err_scale, C, R};
-      return run_forward(geom, view_params, 0, V, flat_recon, num_pixels, S, 0, pixel_indices,
-                         epi, st, "vcd error refresh", 1);
-    }
+    case MBIR_F32:
+      return run(RefreshEpi<float>{y_vcr, static_cast<float *>(error_sino), err_scale, C, R});
+    case MBIR_BF16:
+      return run(RefreshEpi<__nv_bfloat16>{y_vcr, static_cast<__nv_bfloat16 *>(error_sino),
+                                           err_scale, C, R});
     default:
-      return fail(MBIR_ERR_INVALID, "unknown storage dtype %d", storage);
+      return run(RefreshEpi<__half>{y_vcr, static_cast<__half *>(error_sino), err_scale, C, R});
   }
 }
 

@@ -580,24 +580,57 @@ struct FwdShape {
   }
 };
 
-// Epilogue: plain store in either sinogram layout.
+// Epilogue: plain store in either sinogram layout.  View v lands in slot
+// v - v_base of `out` (the binned kernels hand over absolute views).
 struct StoreSino {
+  static constexpr bool kViewFastest = true;  // binned grids: views on x
   float *out;
   int layout, C, R;
+  int v_base;
   __device__ __forceinline__ bool channel_fastest() const { return layout == MBIR_LAYOUT_VRC; }
   __device__ __forceinline__ void begin(int) {}
   __device__ __forceinline__ void prefetch(int, int, int) {}
   __device__ __forceinline__ void cell(int v, int c, int m, float val) {
+    const size_t vs = (size_t)(v - v_base);
     if (layout == MBIR_LAYOUT_VCR)
-      out[((size_t)v * C + c) * R + m] = val;
+      out[(vs * C + c) * R + m] = val;
     else
-      out[((size_t)v * R + m) * C + c] = val;
+      out[(vs * R + m) * C + c] = val;
   }
   template <int N>
   __device__ __forceinline__ void cells(int v, int c0, int ncb, int m, const float (&acc)[N]) {
 #pragma unroll
     for (int j = 0; j < N; ++j)
       if (j < ncb) cell(v, c0 + j, m, acc[j]);
+  }
+  // Rows m0 .. m0 + 3 of channels c0 .. c0 + ncb - 1; channel j's four sums
+  // are acc[j * stride].  In the (V, C, R) layout with R a multiple of 4 and
+  // a 16-byte aligned `out`, each channel's four cells are one vector store.
+  __device__ __forceinline__ void cells4(int v, int c0, int ncb, int m0,
+                                         const float4 *__restrict__ acc, int stride) {
+    const size_t vs = (size_t)(v - v_base);
+    const bool vec = layout == MBIR_LAYOUT_VCR && (R & 3) == 0 &&
+                     (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+    for (int j = 0; j < ncb; ++j) {
+      const float4 a = acc[j * stride];
+      if (vec) {
+        *reinterpret_cast<float4 *>(out + (vs * C + c0 + j) * R + m0) = a;
+      } else {
+        const float q[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (m0 + k < R) cell(v, c0 + j, m0 + k, q[k]);
+      }
+    }
+  }
+  // A tile that no pixel reaches is zero.
+  __device__ __forceinline__ void empty_tile(int v, int c0, int ncb) {
+    for (int i = threadIdx.x; i < ncb * R; i += blockDim.x) {
+      if (layout == MBIR_LAYOUT_VCR)
+        cell(v, c0 + i / R, i % R, 0.f);
+      else
+        cell(v, c0 + i % ncb, i / ncb, 0.f);
+    }
   }
   __device__ __forceinline__ void end(int) {}
 };
@@ -1081,7 +1114,7 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
 // A pixel whose centre lies outside [-1, C] has no tap on the detector and
 // is in no key.  Channel block b (channels c0 .. c0 + 15) is reached by the
 // centres c0 - 1 .. c0 + 16: the keys c0 .. c0 + 17, one contiguous range.
-// Slots are placed by a deterministic prefix over (chunk, warp, lane): no
+// Slots are placed by a deterministic prefix over (key, warp, lane): no
 // atomics decide an order.
 __host__ __device__ inline int fwd_nkeys(int C) { return C + 2; }
 
@@ -1144,6 +1177,18 @@ __device__ __forceinline__ ConeFwdRec par_fwd_record(const Geo &g, const ParView
 // One CTA's work of cone_bin_kernel: view vl of the chunk, with bsm the
 // (1 + warps) x (C + 2) ints of dynamic shared memory.  Parallel-beam
 // geometries (g.cone = 0) are binned the same way, with par_fwd_record.
+//
+// A stable counting sort in three steps.  Warp w owns the contiguous slots
+// [p0, p1) (slot order = warp order, then lane order), so that:
+//   1. each warp forms its slots' records and counts them per key into its
+//      own row of counters (the leader of each group of equal keys in a
+//      32-slot step adds the group's size: no two lanes write one counter);
+//   2. the per-key totals are scanned, and each warp's row becomes its
+//      starting cursor per key (key-major, then warp order);
+//   3. each warp walks its slots again and places them at its cursors.
+// Only steps 1 -> 2 -> 3 synchronise the CTA; steps 1 and 3 are warp-local.
+// The list is THE stable sort of the slots by key (a stable sort has one
+// result), whatever the CTA size.
 __device__ __forceinline__ void cone_bin_view(const Geo &g, const float *__restrict__ vp,
                                               int v_start, int vl,
                                               const int64_t *__restrict__ pix, int P,
@@ -1154,8 +1199,9 @@ __device__ __forceinline__ void cone_bin_view(const Geo &g, const float *__restr
   const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nw = nthr >> 5;
   const int nkeys = fwd_nkeys(g.C);
-  int *cursor = bsm;        // nkeys
-  int *wc = bsm + nkeys;    // nw x nkeys
+  int *tot = bsm;             // nkeys: per-key totals, then their exclusive prefix
+  int *wc = bsm + nkeys;      // nw x nkeys: per-(warp, key) counts, then cursors
+  int *mywc = wc + warp * nkeys;
   const int v = v_start + vl;
   const float ang = vp[2 * v];
   const float cs = cosf(ang), sn = sinf(ang);
@@ -1165,55 +1211,66 @@ __device__ __forceinline__ void cone_bin_view(const Geo &g, const float *__restr
   ConeFwdRec *vrec = recs + (size_t)vl * P;
   int *vlist = list + (size_t)vl * P;
   int *voffs = offs + (size_t)vl * (nkeys + 1);
+  const int per_warp = (P + nw - 1) / nw;
+  const int p0 = min(P, warp * per_warp), p1 = min(P, p0 + per_warp);
+  const unsigned lt = (1u << lane) - 1u;
 
-  for (int k = tid; k < nkeys; k += nthr) cursor[k] = 0;
+  for (int i = tid; i < nkeys * (1 + nw); i += nthr) bsm[i] = 0;
   __syncthreads();
-  // Pass 1: records and per-key counts (the counts do not depend on the
-  // order of the shared-memory increments).
-  for (int p = tid; p < P; p += nthr) {
-    float xt, yt;
-    pixel_xy(g, (int)pix[p], xt, yt);
-    const int row = by_pixel ? (int)pix[p] : p;
-    int ctr;
-    if (g.cone) {
-      const ConeCenter cc = cone_center(g, cs, sn, xt, yt);
-      vrec[p] = cone_fwd_record(g, ang, z_off, cc, row);
-      ctr = cc.ctr;
-    } else {
-      const float n_p = parallel_np(g, pv, xt, yt);
-      ctr = (int)fminf(fmaxf(rintf(n_p), -1.0e6f), 1.0e6f);
-      vrec[p] = par_fwd_record(g, pv, n_p, ctr, row);
+  // 1. records and per-(warp, key) counts
+  for (int base = p0; base < p1; base += 32) {
+    const int p = base + lane;
+    int key = -1;
+    if (p < p1) {
+      float xt, yt;
+      pixel_xy(g, (int)pix[p], xt, yt);
+      const int row = by_pixel ? (int)pix[p] : p;
+      int ctr;
+      if (g.cone) {
+        const ConeCenter cc = cone_center(g, cs, sn, xt, yt);
+        vrec[p] = cone_fwd_record(g, ang, z_off, cc, row);
+        ctr = cc.ctr;
+      } else {
+        const float n_p = parallel_np(g, pv, xt, yt);
+        ctr = (int)fminf(fmaxf(rintf(n_p), -1.0e6f), 1.0e6f);
+        vrec[p] = par_fwd_record(g, pv, n_p, ctr, row);
+      }
+      key = fwd_key(ctr, g.C);
     }
-    const int key = fwd_key(ctr, g.C);
-    if (key >= 0) atomicAdd(&cursor[key], 1);
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (key >= 0 && (peers & lt) == 0) mywc[key] += __popc(peers);
+    __syncwarp();
   }
   __syncthreads();
-  const int total = block_exclusive_scan(cursor, nkeys, warp_tot);
-  for (int k = tid; k < nkeys; k += nthr) voffs[k] = cursor[k];
-  if (tid == 0) voffs[nkeys] = total;
-  // Pass 2: stable placement, one chunk of nthr slots at a time (a thread
-  // reads back the record it wrote itself in pass 1).
-  const unsigned lt = (1u << lane) - 1u;
-  for (int base = 0; base < P; base += nthr) {
-    const int p = base + tid;
-    const int key = p < P ? fwd_key(__float_as_int(vrec[p].c.z), g.C) : -1;
-    for (int i = tid; i < nw * nkeys; i += nthr) wc[i] = 0;
-    __syncthreads();
-    const unsigned peers = __match_any_sync(0xffffffffu, key);
-    if (key >= 0 && (peers & lt) == 0) wc[warp * nkeys + key] = __popc(peers);
-    __syncthreads();
-    for (int k = tid; k < nkeys; k += nthr) {
-      int s = cursor[k];
-      for (int j = 0; j < nw; ++j) {
-        const int c = wc[j * nkeys + k];
-        wc[j * nkeys + k] = s;
-        s += c;
-      }
-      cursor[k] = s;
+  // 2. key totals, their prefix, and each warp's cursors
+  for (int k = tid; k < nkeys; k += nthr) {
+    int t = 0;
+    for (int w = 0; w < nw; ++w) t += wc[w * nkeys + k];
+    tot[k] = t;
+  }
+  __syncthreads();
+  const int total = block_exclusive_scan(tot, nkeys, warp_tot);
+  for (int k = tid; k < nkeys; k += nthr) {
+    int run = tot[k];
+    voffs[k] = run;
+    for (int w = 0; w < nw; ++w) {
+      const int c = wc[w * nkeys + k];
+      wc[w * nkeys + k] = run;
+      run += c;
     }
-    __syncthreads();
-    if (key >= 0) vlist[wc[warp * nkeys + key] + __popc(peers & lt)] = p;
-    __syncthreads();
+  }
+  if (tid == 0) voffs[nkeys] = total;
+  __syncthreads();
+  // 3. placement (a lane reads back the record it wrote itself in step 1)
+  for (int base = p0; base < p1; base += 32) {
+    const int p = base + lane;
+    const int key = p < p1 ? fwd_key(__float_as_int(vrec[p].c.z), g.C) : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int pos = key >= 0 ? mywc[key] + __popc(peers & lt) : 0;
+    __syncwarp();
+    if (key >= 0 && (peers & lt) == 0) mywc[key] += __popc(peers);
+    __syncwarp();
+    if (key >= 0) vlist[pos] = p;
   }
 }
 
@@ -1230,6 +1287,19 @@ __global__ void __launch_bounds__(256)
 cone_bin_kernel(Geo g, const float *__restrict__ vp, int v_start,
                 const int64_t *__restrict__ pix, int P, int by_pixel,
                 ConeFwdRec *__restrict__ recs, int *__restrict__ list, int *__restrict__ offs) {
+  cone_bin_kernel_body(g, vp, v_start, pix, P, by_pixel, recs, list, offs);
+}
+
+// Whole-volume binning: the same per-view sort with kBinWideThreads threads
+// per view (a view then holds every pixel of the volume, a few hundred slots
+// per thread at 256 threads).  The list is the same stable sort.
+constexpr int kBinWideThreads = 1024;
+
+__global__ void __launch_bounds__(kBinWideThreads)
+cone_bin_wide_kernel(Geo g, const float *__restrict__ vp, int v_start,
+                     const int64_t *__restrict__ pix, int P, int by_pixel,
+                     ConeFwdRec *__restrict__ recs, int *__restrict__ list,
+                     int *__restrict__ offs) {
   cone_bin_kernel_body(g, vp, v_start, pix, P, by_pixel, recs, list, offs);
 }
 
@@ -1250,7 +1320,13 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
   ConeFwdRec *rec = reinterpret_cast<ConeFwdRec *>(sm4);
   float *stage = reinterpret_cast<float *>(rec + cap);
   float *acc_s = stage + kFwdEB * SP;  // (kFwdCB + 4) x nthr
-  const int nblk = gridDim.x, blk = blockIdx.x, vl = blockIdx.y;
+  // (channel block, view) from the grid: views on x for whole-volume
+  // epilogues (EPI::kViewFastest), so that the CTAs in flight are adjacent
+  // views of one channel block, whose pixel strips nearly coincide and whose
+  // cylinder reads hit L2; channel blocks on x otherwise.
+  const bool vf = EPI::kViewFastest;
+  const int nblk = vf ? gridDim.y : gridDim.x, blk = vf ? blockIdx.y : blockIdx.x,
+            vl = vf ? blockIdx.x : blockIdx.y;
   const int c0 = blk * kFwdCB;
   const int ncb = min(kFwdCB, g.C - c0);
   const int bp = g.bp;
@@ -1264,8 +1340,9 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
   const int v = v_start + vl;
   if (tid == 0) touched[(size_t)v * nblk + blk] = end > start;
   if (end == start) {
-    // No pixel reaches the tile: its A x is zero and is not stored (readers
-    // consult `touched`); the epilogue's partials are zero.
+    // No pixel reaches the tile: its A x is zero (the VCD epilogue stores
+    // nothing; its readers consult `touched`) and the partials are zero.
+    epi.empty_tile(v, c0, ncb);
     epi.begin(v);
     epi.end(v * nblk + blk);
     return;
@@ -1364,7 +1441,13 @@ __device__ __forceinline__ void forward_parallel_binned_kernel_body(Geo g, int v
   float4 *wq = sm4;                                   // cap x (w0, w1, w2, ctr)
   int *rows = reinterpret_cast<int *>(wq + cap);      // cap cylinder rows
   float *acc_s = reinterpret_cast<float *>(rows + cap);  // (kFwdCB + 4) x nthr
-  const int nblk = gridDim.x, blk = blockIdx.x, vl = blockIdx.y;
+  // (channel block, view) from the grid: views on x for whole-volume
+  // epilogues (EPI::kViewFastest), so that the CTAs in flight are adjacent
+  // views of one channel block, whose pixel strips nearly coincide and whose
+  // cylinder reads hit L2; channel blocks on x otherwise.
+  const bool vf = EPI::kViewFastest;
+  const int nblk = vf ? gridDim.y : gridDim.x, blk = vf ? blockIdx.y : blockIdx.x,
+            vl = vf ? blockIdx.x : blockIdx.y;
   const int c0 = blk * kFwdCB;
   const int ncb = min(kFwdCB, g.C - c0);
   const ConeFwdRec *vrec = recs + (size_t)vl * P;
@@ -1375,6 +1458,7 @@ __device__ __forceinline__ void forward_parallel_binned_kernel_body(Geo g, int v
   const int v = v_start + vl;
   if (tid == 0) touched[(size_t)v * nblk + blk] = end > start;
   if (end == start) {
+    epi.empty_tile(v, c0, ncb);
     epi.begin(v);
     epi.end(v * nblk + blk);
     return;
@@ -1476,7 +1560,13 @@ __device__ __forceinline__ void forward_parallel_binned4_kernel_body(Geo g, int 
   float4 *wq = sm4;                                            // kPar4Cap x (w0, w1, w2, ctr)
   int *rows = reinterpret_cast<int *>(wq + kPar4Cap);          // kPar4Cap cylinder rows
   float4 *acc_s = reinterpret_cast<float4 *>(rows + kPar4Cap);  // kFwdCB x nthr
-  const int nblk = gridDim.x, blk = blockIdx.x, vl = blockIdx.y;
+  // (channel block, view) from the grid: views on x for whole-volume
+  // epilogues (EPI::kViewFastest), so that the CTAs in flight are adjacent
+  // views of one channel block, whose pixel strips nearly coincide and whose
+  // cylinder reads hit L2; channel blocks on x otherwise.
+  const bool vf = EPI::kViewFastest;
+  const int nblk = vf ? gridDim.y : gridDim.x, blk = vf ? blockIdx.y : blockIdx.x,
+            vl = vf ? blockIdx.x : blockIdx.y;
   const int c0 = blk * kFwdCB;
   const int ncb = min(kFwdCB, g.C - c0);
   const ConeFwdRec *vrec = recs + (size_t)vl * P;
@@ -1487,6 +1577,7 @@ __device__ __forceinline__ void forward_parallel_binned4_kernel_body(Geo g, int 
   const int v = v_start + vl;
   if (tid == 0) touched[(size_t)v * nblk + blk] = end > start;
   if (end == start) {
+    epi.empty_tile(v, c0, ncb);
     epi.begin(v);
     epi.end(v * nblk + blk);
     return;

@@ -363,6 +363,7 @@ __device__ __forceinline__ bool last_cta(unsigned int *counter, unsigned int tot
 // Ad * (1 / scale).
 template <typename T>
 struct LineSearchEpi {
+  static constexpr bool kViewFastest = false;  // binned grids: channel blocks on x
   const T *e;
   const float *es;
   const T *w;
@@ -495,6 +496,9 @@ struct LineSearchEpi {
       }
     }
   }
+  // A tile that no pixel reaches: A delta is zero there and is not stored
+  // (the sinogram update skips untouched tiles).
+  __device__ __forceinline__ void empty_tile(int, int, int) {}
   __device__ __forceinline__ void end(int slot) {
     if (!with_sums) return;
     block_sum2(fl, fq);
@@ -510,6 +514,7 @@ struct LineSearchEpi {
 // sinogram from y bounds the drift that in-place 16-bit updates accumulate.
 template <typename T>
 struct RefreshEpi {
+  static constexpr bool kViewFastest = true;  // binned grids: views on x
   const float *y;
   T *e;
   const float *es;
@@ -532,6 +537,26 @@ struct RefreshEpi {
     for (int j = 0; j < N; ++j)
       if (j < ncb)
         e[i0 + (size_t)j * R] = from_f32<T>(__fmul_rn(__fsub_rn(yv[j], acc[j]), inv_scale));
+  }
+  // Rows m0 .. m0 + 3 of channels c0 .. c0 + ncb - 1 (channel j's four sums
+  // in acc[j * stride]).
+  __device__ __forceinline__ void cells4(int v, int c0, int ncb, int m0,
+                                         const float4 *__restrict__ acc, int stride) {
+    for (int j = 0; j < ncb; ++j) {
+      const float4 a = acc[j * stride];
+      const float q[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (m0 + k < R) cell(v, c0 + j, m0 + k, q[k]);
+    }
+  }
+  // A tile that no pixel reaches: A x is zero, so e = y / scale there.
+  __device__ __forceinline__ void empty_tile(int v, int c0, int ncb) {
+    const float inv = 1.f / __ldg(es + v);
+    for (int i = threadIdx.x; i < ncb * R; i += blockDim.x) {
+      const size_t k = ((size_t)v * C + c0 + i / R) * R + i % R;
+      e[k] = from_f32<T>(__fmul_rn(__ldg(y + k), inv));
+    }
   }
   __device__ __forceinline__ void end(int) {}
 };

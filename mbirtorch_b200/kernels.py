@@ -57,8 +57,22 @@ def _view_params_2col(view_params, device):
     return vp.reshape(-1, 2).contiguous()
 
 
+BINNED_BYTES_PER_PIXEL_VIEW = 52  # a binned forward's record + list entry
+
+
 class DeviceProjector:
-    """Forward/back projection of one geometry on one CUDA device."""
+    """Forward/back projection of one geometry on one CUDA device.
+
+    Whole-cylinder forward projections go through the channel-sorted bins
+    (``mbir_forward_project_binned``) wherever those kernels apply (psf
+    radius 1, up to 1024 detector rows): the records of a chunk of views
+    are formed and sorted once, and each (view, channel block) CTA walks
+    only the pixels that reach it, where the scanning forward tests every
+    pixel in every block.  The workspace (up to about 1 GiB of records, from
+    torch's caching allocator) is the one transient.
+    """
+
+    binned_forward = {MBIR_PARALLEL: True, MBIR_CONE: True}
 
     def __init__(self, geom, view_params, device):
         self.geom = geom
@@ -66,6 +80,21 @@ class DeviceProjector:
         self.view_params = _view_params_2col(view_params, self.device)
         if self.view_params.shape[0] != geom.num_views:
             raise ValueError("view parameter count does not match the geometry's views")
+
+    def _binned_workspace(self, device, view_count, num_pixels):
+        """The binned forward's workspace, or None where it does not apply."""
+        if not self.binned_forward.get(self.geom.geometry, False) or num_pixels <= 0:
+            return None
+        nbytes = int(_lib.query(device, 'mbir_forward_project_binned_workspace_size', self.geom,
+                                view_count, num_pixels))
+        if nbytes <= 0:
+            return None
+        return torch.empty(nbytes, dtype=torch.uint8, device=device)
+
+    def _forward_binned(self, values, by_pixel, idx, view_start, vc, out, layout, ws):
+        _lib.call(values.device, 'mbir_forward_project_binned', self.geom,
+                  ptr(self.view_params), view_start, vc, ptr(values), by_pixel, ptr(idx),
+                  idx.shape[0], ptr(out), layout, ptr(ws), ws.numel(), stream_of(values.device))
 
     @property
     def sino_shape(self):
@@ -85,6 +114,11 @@ class DeviceProjector:
                  else (vc, g.num_det_channels, g.num_det_rows))
         if out is None:
             out = torch.empty(shape, dtype=torch.float32, device=values.device)
+        ws = (self._binned_workspace(values.device, vc, idx.shape[0])
+              if slice_start == 0 and L == g.num_slices else None)
+        if ws is not None:
+            self._forward_binned(values, 0, idx, view_start, vc, out, layout, ws)
+            return out
         _lib.call(values.device, 'mbir_forward_project', g, ptr(self.view_params), view_start,
                   vc, ptr(values), idx.shape[0], L, slice_start, ptr(idx), ptr(out), layout,
                   stream_of(values.device))
@@ -104,6 +138,10 @@ class DeviceProjector:
                  else (g.num_views, g.num_det_channels, g.num_det_rows))
         if out is None:
             out = torch.empty(shape, dtype=torch.float32, device=flat.device)
+        ws = self._binned_workspace(flat.device, g.num_views, idx.shape[0])
+        if ws is not None:
+            self._forward_binned(flat, 1, idx, 0, g.num_views, out, layout, ws)
+            return out
         _lib.call(flat.device, 'mbir_forward_project_volume', g, ptr(self.view_params), 0,
                   g.num_views, ptr(flat), ptr(idx), idx.shape[0], ptr(out), layout,
                   stream_of(flat.device))
@@ -220,7 +258,14 @@ def cone_back_view_batch(sino_batch, pixel_indices, view_params_batch, num_rows_
 for _f in (parallel_forward_view_batch, parallel_back_view_batch, cone_forward_view_batch,
            cone_back_view_batch):
     _f._mbirtorch_no_compile = True
-    # (bytes per view, nominal view chunk): the kernels hold no per-view
-    # transient, so a whole view range is one batch (projectors.py:475-516).
+    # (bytes per view, nominal view chunk): the scanning kernels hold no
+    # per-view transient, so a whole view range is one batch
+    # (projectors.py:475-516).
     _f._view_batch_cost = lambda num_pixels, band_cols, args: (1, 1 << 30)
+# The whole-cylinder forward bins its views: one record (48 bytes) and one
+# list entry (4 bytes) per (view, pixel).
+for _f in (parallel_forward_view_batch, cone_forward_view_batch):
+    _f._view_batch_cost = (
+        lambda num_pixels, band_cols, args: (BINNED_BYTES_PER_PIXEL_VIEW * max(1, int(num_pixels)),
+                                             1 << 30))
 del _f

@@ -73,8 +73,17 @@ class MemoryLedger:
         ws = int(_lib.query(getattr(model, 'torch_device', None), 'mbir_vcd_workspace_size',
                             model._geometry(), int(max_subset_pixels), prm))
         y = 4 * n_sino if code != _lib.MBIR_F32 else 0
-        resident = y + (2 if weighted else 1) * s * n_sino + ws + 8 * n_vol
-        init = 4 * 4 * n_sino + 3 * 4 * n_vol + y + (4 * n_sino if weighted else 0)
+        # the binned whole-volume forward's workspace (initialisation, and
+        # every error refresh of a 16-bit job; torch's caching allocator
+        # keeps it)
+        rs, ror = model.get_params(['recon_shape', 'use_ror_mask'])
+        n_pix = int(vcd_utils.get_2d_ror_mask(rs, use_ror_mask=ror).sum()) \
+            if ror is not False else rs[0] * rs[1]
+        bins = int(_lib.query(getattr(model, 'torch_device', None),
+                              'mbir_forward_project_binned_workspace_size', model._geometry(),
+                              V, n_pix))
+        resident = y + (2 if weighted else 1) * s * n_sino + ws + 8 * n_vol + (bins if y else 0)
+        init = 4 * 4 * n_sino + 3 * 4 * n_vol + y + (4 * n_sino if weighted else 0) + bins
         return max(init, resident), resident
 
 

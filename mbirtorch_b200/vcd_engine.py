@@ -212,9 +212,15 @@ def partition_pass_batched(engines, flats, errs, partitions, orders, accums=None
 def _refresh(engine, flat_recon, err, pixel_indices, y_vcr):
     idx = _lib.as_i64_contig(pixel_indices)
     require_cuda(flat_recon, idx, y_vcr)
-    _lib.call(engine.device, 'mbir_vcd_refresh_error', engine.geom, ptr(engine.view_params),
+    g = engine.geom
+    nbytes = int(_lib.query(engine.device, 'mbir_forward_project_binned_workspace_size', g,
+                            g.num_views, idx.shape[0]))
+    # the bins' workspace (torch's caching allocator); none: the scanning forward
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=engine.device) if nbytes > 0 else None
+    _lib.call(engine.device, 'mbir_vcd_refresh_error', g, ptr(engine.view_params),
               ptr(flat_recon), ptr(idx), idx.shape[0], ptr(y_vcr), ptr(err.data),
-              ptr(err.scale), err.storage, stream_of(engine.device))
+              ptr(err.scale), err.storage, ptr(ws), 0 if ws is None else ws.numel(),
+              stream_of(engine.device))
 
 
 VcdEngine.refresh_error = _refresh

@@ -2,7 +2,7 @@
 
 This package restates the reference algorithm (mbirtorch v0.0.2) on the CPU
 in FP64 so that the sm_100a kernels of ``mbirtorch_b200`` can be checked
-against it.  It is the checker, never the thing measured or shipped: only
+against it.  It checks results and is never the thing measured or shipped: only
 ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
 import it, and nothing in ``mbirtorch_b200`` does.
 

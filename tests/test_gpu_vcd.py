@@ -2,7 +2,7 @@
 
 * Seeded recon() against the reference's own seeded recon (golden traces):
   relative L2 <= 1e-4 on the volume after the fixed iteration count, and
-  the fm_rmse / alpha traces to 1e-4 (north_star reconstruction bar).
+  the fm_rmse / alpha traces to 1e-4 (the reconstruction parity bar).
 * The same against the FP64 oracle.
 * Mixed-precision storage (bfloat16, float16) against the FP64 oracle at
   relative L2 <= 1e-3.
@@ -520,3 +520,52 @@ def test_curved_cone_partition_pass_weighted_positivity():
     assert abs(float(acc[1]) - alpha_sum) / alpha_sum <= 1e-4
     assert rel_l2(flat.cpu().numpy(), oflat) <= 2e-5
     assert rel_l2(err.to_vrc().cpu().numpy(), oerr) <= 2e-5
+
+
+@pytest.mark.parametrize("kind", ["parallel", "cone"])
+@pytest.mark.parametrize("storage", ["float32", "float16"])
+def test_error_refresh_binned_equals_scanning(kind, storage):
+    """The error refresh e = (y - A x) / scale through the channel-sorted bins
+    (a workspace given) against the scanning forward (none given): the same
+    operator summed in another order.  e is a small difference of large
+    terms (y and A x), so the differences are measured against ||y||: FP32
+    rounding of A x (1e-6) in FP32 storage, one 16-bit rounding step of e in
+    float16."""
+    from mbirtorch_b200 import _lib
+    from mbirtorch_b200._lib import ptr, stream_of
+    from mbirtorch_b200.vcd_engine import ResidentSinogram
+    dev = torch.device('cuda', 0)
+    if kind == 'parallel':
+        m = mb.ParallelBeamModel((50, 128, 70), np.linspace(0, np.pi, 50, endpoint=False))
+        m.set_params(no_warning=True, verbose=0)
+    else:
+        m = mb.ConeBeamModel((40, 24, 56), np.linspace(0, 2 * np.pi, 40, endpoint=False),
+                             300.0, 150.0)
+        m.set_params(no_warning=True, verbose=0)
+    rs = m.get_params('recon_shape')
+    g = m._geometry()
+    idx = torch.as_tensor(mb.gen_full_indices(rs).astype(np.int64), device=dev)
+    flat = torch.rand(rs[0] * rs[1], rs[2], device=dev)
+    y = m.projector.forward_volume(flat, idx) + 0.1 * torch.randn(
+        *m.get_params('sinogram_shape'), device=dev)
+    y_vcr = y.transpose(1, 2).contiguous()
+    code = {'float32': _lib.MBIR_F32, 'float16': _lib.MBIR_F16}[storage]
+    outs = []
+    for binned in (False, True):
+        err = ResidentSinogram.from_vrc(y, code)
+        ws = None
+        if binned:
+            nb = int(_lib.query(dev, 'mbir_forward_project_binned_workspace_size', g,
+                                g.num_views, idx.shape[0]))
+            ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+        _lib.call(dev, 'mbir_vcd_refresh_error', g, ptr(m.projector.view_params), ptr(flat),
+                  ptr(idx), idx.shape[0], ptr(y_vcr), ptr(err.data), ptr(err.scale), code,
+                  ptr(ws), 0 if ws is None else ws.numel(), stream_of(dev))
+        outs.append(err.data.float() * err.scale.view(-1, 1, 1))
+    torch.cuda.synchronize()
+    ynorm = float(y.norm())
+    d = float((outs[0] - outs[1]).norm()) / ynorm
+    assert d <= (1e-6 if storage == 'float32' else 1e-3 * float(outs[0].norm()) / ynorm), d
+    ref = (y - m.projector.forward_volume(flat, idx)).transpose(1, 2)
+    d_ref = float((outs[1] - ref).norm()) / ynorm
+    assert d_ref <= (1e-6 if storage == 'float32' else 1e-3 * float(ref.norm()) / ynorm), d_ref
