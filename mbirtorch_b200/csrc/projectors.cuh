@@ -865,6 +865,9 @@ __device__ __forceinline__ void fwd_block_range(int ctr, int C, int &b_lo, int &
 // psf radius 1 with the taps unrolled; BP = 0 takes the radius bp at run
 // time.  A tap weight clamp(x, 0, lmax) is formed as min(sat(x), lmax),
 // the same value for lmax = min(w_r, 1) <= 1, with no branch on lmax.
+//
+// The shared records hold -m0 / w_r in a.x (fwd_stage_record), so that the
+// row's centre slice k_m = (m - m0) / w_r is one FMA.
 template <int BP, bool SORTED>
 __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec, int nb,
                                              const float *__restrict__ stage, int SP, float mf,
@@ -872,30 +875,36 @@ __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec,
                                              int c0, float *__restrict__ acc_s, int &cj,
                                              float &q0, float &q1, float &q2) {
   const int tid = threadIdx.x, nthr = blockDim.x;
-  // A row m reaches the band only when its centre slice (m - m0) / w_r lies
-  // within [kc_lo, kc_hi], i.e. m in [m0 + w_r kc_lo, m0 + w_r kc_hi]
-  // (widened here by a row either side).  Outside, every tap meets the zero
-  // padding and adds an exact zero, so a warp whose rows [wr0, wr0 + 31] all
-  // lie outside skips the pixel, with the same result.  Lane e tests pixel
-  // e of the batch (nb <= kFwdEB <= 32); bit e of `skip` is the answer.
-  unsigned skip;
+  // A row m reaches the band only when its centre slice k_m lies within
+  // [kc_lo, kc_hi]; outside, the clamped centre puts every tap in the zero
+  // padding and the row adds an exact zero.  So a warp whose rows
+  // [wr0, wr0 + 31], widened by a row either side, all map outside skips the
+  // pixel, with the same result.  Lane e tests pixel e of the batch
+  // (nb <= kFwdEB <= 32); bit e of `skip` is the answer, and a pixel whose
+  // lane does not run (a warp cut short by the detector's last row) is not
+  // skipped.  The warp then walks only the pixels left in `todo`, lowest
+  // first.
+  unsigned todo;
   {
     const int lane = tid & 31;
     const float wr0 = (float)(tid - lane), wr1 = wr0 + 31.f;
     bool out = false;
     if (lane < nb) {
-      const float4 ra = rec[lane].a;
-      out = fmaf(ra.y, kc_hi, ra.x) + 1.f < wr0 || fmaf(ra.y, kc_lo, ra.x) - 1.f > wr1;
+      const float nm = rec[lane].a.x, inv_wr = rec[lane].b.x;
+      out = fmaf(wr1 + 1.f, inv_wr, nm) < kc_lo || fmaf(wr0 - 1.f, inv_wr, nm) > kc_hi;
     }
-    skip = __ballot_sync(__activemask(), out);
+    const unsigned skip = __ballot_sync(__activemask(), out);
+    todo = ~skip & (nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u));
   }
 #pragma unroll 1
-  for (int e = 0; e < nb; ++e) {
+  while (todo) {  // uniform over the warp
+    const int e = __ffs(todo) - 1;
+    todo &= todo - 1u;
     const ConeFwdRec *r = rec + e;
     const float4 ra = r->a, rb = r->b;
     const int j = __float_as_int(r->c.z) - c0 + 1;  // in [0, kFwdCB + 1]
-    const float m0 = ra.x, w_r = ra.y, hw1r = ra.z, lmaxr = ra.w;
-    if (SORTED && j != cj) {  // uniform over the CTA; j > cj
+    const float nm = ra.x, w_r = ra.y, hw1r = ra.z, lmaxr = ra.w;
+    if (SORTED && j != cj) {  // uniform over the warp; j > cj
       float *a = acc_s + cj * nthr + tid;
       a[0] += q0;
       if (j == cj + 1) {
@@ -914,16 +923,19 @@ __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec,
       q2 = 0.f;
       cj = j;
     }
-    if ((skip >> e) & 1u) continue;  // uniform over the warp
-    const float k_m = (mf - m0) * rb.x;
+    const float k_m = fmaf(mf, rb.x, nm);
     const float kc = fminf(fmaxf(rintf(k_m), kc_lo), kc_hi);
     const float d = w_r * (kc - k_m);
     const float *st = stage + e * SP + kFwdVPad + ((int)kc - slice_start);
     float det;
     if (BP == 1) {
-      const float am = fminf(__saturatef(hw1r - fabsf(d - w_r)), lmaxr);
+      // |kc - k_m| <= 1/2 wherever the taps can meet the band (elsewhere they
+      // meet the zero padding), so |d| <= w_r / 2: the outer taps' distances
+      // |d -+ w_r| are w_r -+ d.
+      const float c1 = hw1r - w_r;
+      const float am = fminf(__saturatef(c1 + d), lmaxr);
       const float a0 = fminf(__saturatef(hw1r - fabsf(d)), lmaxr);
-      const float ap = fminf(__saturatef(hw1r - fabsf(d + w_r)), lmaxr);
+      const float ap = fminf(__saturatef(c1 - d), lmaxr);
       det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
     } else {
       det = 0.f;
@@ -945,6 +957,13 @@ __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec,
       a[2 * nthr] = fmaf(rb.w, det, a[2 * nthr]);
     }
   }
+}
+
+// A record as the forward CTAs keep it in shared memory: a.x = -m0 / w_r
+// (the row-to-slice offset) instead of m0; the other fields as formed.
+__device__ __forceinline__ ConeFwdRec fwd_stage_record(ConeFwdRec r) {
+  r.a.x = -r.a.x * r.b.x;
+  return r;
 }
 
 // The batches of one round: n records in shared memory, processed kFwdEB at
@@ -1081,7 +1100,7 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
       }
       if (keep)
         rec[off + __popc(bal & ((1u << lane) - 1u))] =
-            cone_fwd_record(g, ang, z_off, cc, by_pixel ? (int)pix[p] : p);
+            fwd_stage_record(cone_fwd_record(g, ang, z_off, cc, by_pixel ? (int)pix[p] : p));
       n += tot;
       pos += nthr;
       __syncthreads();
@@ -1362,7 +1381,7 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
   for (int base = start; base < end; base += cap) {
     const int n = min(cap, end - base);
     __syncthreads();
-    for (int i = tid; i < n; i += nthr) rec[i] = vrec[vlist[base + i]];
+    for (int i = tid; i < n; i += nthr) rec[i] = fwd_stage_record(vrec[vlist[base + i]]);
     __syncthreads();
     // The round's cylinders, 128-byte line by line, toward L1 ahead of the
     // batch staging.
