@@ -564,11 +564,16 @@ bool use_binned(const mbir_geometry *g) { return use_cone_binned(g) || use_par_b
 
 // by_pixel: the records name the cylinder's row of `values` as pix[p] (a
 // flat volume) instead of the subset slot p.  wide: whole-volume bins, with
-// kBinWideThreads threads per view where their counters fit shared memory.
+// kBinWideThreads threads per view where their counters fit shared memory;
+// subsets of at least kBinWidePixels pixels take them too, outside a batch
+// recording (the batched binning runs the 256-thread body).
+constexpr long long kBinWidePixels = 16384;
+
 int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count,
                const int64_t *pix, long long P, const FwdBins &b, cudaStream_t st,
                int by_pixel = 0, bool wide = false) {
   const Geo geo = make_geo(*g);
+  wide = wide || (P >= kBinWidePixels && t_batch == nullptr);
   if (wide && bin_smem(g, kBinWideThreads) <= (size_t)device_attrs().smem_optin) {
     const size_t smem_w = bin_smem(g, kBinWideThreads);
     const int rc_smem = request_smem(cone_bin_wide_kernel, smem_w, "forward binning");
