@@ -16,7 +16,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 LIB_NAME = "libmbir_b200.so"
 LIB_PATH = os.path.join(HERE, LIB_NAME)
 SOURCES = ["capi.cu"]
-HEADERS = ["mbir_common.cuh", "projectors.cuh", "vcd.cuh"]
+HEADERS = ["mbir_common.cuh", "projectors.cuh", "vcd.cuh", "batch.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
