@@ -503,6 +503,15 @@ size_t cone_rt_smem(const mbir_geometry *g, int band) {
          sizeof(float) * ((size_t)kFwdEB * (band + 2 * kFwdVPad) + (size_t)(kFwdCB + 4) * nthr);
 }
 
+// The binned cone forward with asynchronous staging: two stage buffers and
+// smaller record rounds.
+size_t cone_binned_async_smem(const mbir_geometry *g, int band) {
+  const int nthr = cone_rt_threads(g);
+  return sizeof(ConeFwdRec) * (size_t)fwd_cap_async(nthr) +
+         sizeof(float) *
+             ((size_t)2 * kFwdEB * (band + 2 * kFwdVPad) + (size_t)(kFwdCB + 4) * nthr);
+}
+
 template <typename EPI>
 int launch_cone_rt(const mbir_geometry *g, const float *vp, int v_start, int v_count,
                    const float *values, long long P, int band, int slice_start,
@@ -601,17 +610,60 @@ int launch_binned(const mbir_geometry *g, int v_start, int v_count, const float 
                   long long P, int band, const FwdBins &b, const EPI &epi, cudaStream_t st,
                   const char *what) {
   const Geo geo = make_geo(*g);
-  const size_t smem = cone_rt_smem(g, band);
-  auto k = forward_cone_binned_kernel<EPI>;
+  const dim3 grid = EPI::kViewFastest ? dim3(v_count, fwd_nblk(g)) : dim3(fwd_nblk(g), v_count);
+  // Asynchronous staging copies 16-byte chunks: whole cylinders of a
+  // multiple of 4 slices from a 16-byte aligned array, with room for two
+  // stage buffers.
+  // It is taken where it keeps as many CTAs per SM as the synchronous
+  // staging (its second stage buffer can cost one: the 256-row detector of
+  // the 256^3 cone workload runs 4 CTAs per SM synchronously, 3 with it).
+  const int nthr = cone_rt_threads(g);
+  const size_t smem_a = cone_binned_async_smem(g, band), smem_s = cone_rt_smem(g, band);
+  bool async = band >= 4 && band % 4 == 0 && (reinterpret_cast<uintptr_t>(values) & 15) == 0 &&
+               smem_a <= (size_t)device_attrs().smem_optin;
+  if (async) {
+    int rc_smem = request_smem(forward_cone_binned_kernel<EPI, true>, smem_a, "forward");
+    if (rc_smem) return rc_smem;
+    // The occupancy answer for the last (device, threads, band) seen by this
+    // thread and epilogue.
+    static thread_local int last_dev = -1, last_nthr = -1, last_band = -1;
+    static thread_local bool last_async = false;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != last_dev || nthr != last_nthr || band != last_band) {
+      rc_smem = request_smem(forward_cone_binned_kernel<EPI, false>, smem_s, "forward");
+      if (rc_smem) return rc_smem;
+      int n_a = 0, n_s = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+              &n_a, forward_cone_binned_kernel<EPI, true>, nthr, smem_a) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+              &n_s, forward_cone_binned_kernel<EPI, false>, nthr, smem_s) != cudaSuccess) {
+        cudaGetLastError();
+        n_a = 0;
+      }
+      last_dev = dev;
+      last_nthr = nthr;
+      last_band = band;
+      last_async = n_a > 0 && n_a >= n_s;
+    }
+    async = last_async;
+  }
+  if (async) {
+    tpre(st);
+    launchb<FwdConeBinnedB<EPI, true>>(grid, nthr, smem_a, st, what, geo, v_start,
+                                       values, (int)P, band, 0, (const ConeFwdRec *)b.recs,
+                                       (const int *)b.list, (const int *)b.offs, b.touched, epi);
+    MBIR_CHECK_LAUNCH(what);
+    return MBIR_OK;
+  }
   {
-    const int rc_smem = request_smem(k, smem, "forward");
+    const int rc_smem = request_smem(forward_cone_binned_kernel<EPI, false>, smem_s, "forward");
     if (rc_smem) return rc_smem;
   }
-  const dim3 grid = EPI::kViewFastest ? dim3(v_count, fwd_nblk(g)) : dim3(fwd_nblk(g), v_count);
   tpre(st);
-  launchb<FwdConeBinnedB<EPI>>(grid, cone_rt_threads(g), smem, st, what, geo, v_start, values,
-                               (int)P, band, 0, (const ConeFwdRec *)b.recs, (const int *)b.list,
-                               (const int *)b.offs, b.touched, epi);
+  launchb<FwdConeBinnedB<EPI, false>>(grid, nthr, smem_s, st, what, geo, v_start,
+                                      values, (int)P, band, 0, (const ConeFwdRec *)b.recs,
+                                      (const int *)b.list, (const int *)b.offs, b.touched, epi);
   MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
 }

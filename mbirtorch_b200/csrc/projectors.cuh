@@ -1036,6 +1036,101 @@ __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec,
   }
 }
 
+// ── asynchronous cylinder staging ─────────────────────────────────────────
+// cp.async 16-byte global -> shared copies (L2 only), grouped per batch.
+__device__ __forceinline__ void cp_async16(float *dst_smem, const float *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Records per round of the asynchronously staged forward (its two stage
+// buffers take the room of the larger record rounds).
+__host__ __device__ inline int fwd_cap_async(int nthr) { return min(fwd_cap(nthr), 256); }
+
+// fwd_rt_round<true> with the cylinders staged asynchronously (band a
+// multiple of 4, 16-byte aligned cylinder rows): two stage buffers; the raw
+// cylinders of batch b + 1 are copied global -> shared while batch b is
+// projected, and each batch is scaled by 1 / cos(phi) in place once it has
+// landed.  The staged values and every sum are the same as fwd_rt_round's.
+__device__ __forceinline__ void fwd_rt_round_async(const ConeFwdRec *__restrict__ rec, int n,
+                                                   float *__restrict__ stage2, int SP,
+                                                   const float *__restrict__ values, int band,
+                                                   int slice_start, float kc_lo, float kc_hi,
+                                                   int bp, int R, int c0,
+                                                   float *__restrict__ acc_s) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const float mf = (float)tid;
+  int cj = __float_as_int(rec[0].c.z) - c0 + 1;
+  float q0 = 0.f, q1 = 0.f, q2 = 0.f;
+  const int q4 = band >> 2;  // 16-byte chunks per cylinder (band >= 4)
+  const int nbat = (n + kFwdEB - 1) / kFwdEB;
+  // This thread's chunks i = tid, tid + nthr, ... as (pixel e, chunk q),
+  // stepped without a division per chunk.
+  const int e_step = nthr / q4, q_step = nthr - e_step * q4;
+  const int e_first = tid / q4, q_first = tid - e_first * q4;
+  auto issue = [&](int b) {
+    const int b0 = b * kFwdEB, nb = min(kFwdEB, n - b0);
+    float *buf = stage2 + (b & 1) * kFwdEB * SP + kFwdVPad;
+    int e = e_first, q = q_first;
+    while (e < nb) {
+      cp_async16(buf + e * SP + 4 * q,
+                 values + (size_t)__float_as_int(rec[b0 + e].c.w) * band + 4 * q);
+      e += e_step;
+      q += q_step;
+      if (q >= q4) {
+        q -= q4;
+        ++e;
+      }
+    }
+    cp_async_commit();
+  };
+  issue(0);
+  for (int b = 0; b < nbat; ++b) {
+    const int b0 = b * kFwdEB, nb = min(kFwdEB, n - b0);
+    if (b + 1 < nbat) {
+      issue(b + 1);
+      cp_async_wait<1>();  // this thread's copies of batch b have landed
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    float *buf = stage2 + (b & 1) * kFwdEB * SP;
+    for (int k = tid; k < band; k += nthr) {
+      const float kf = (float)(slice_start + k);
+      float *sk = buf + kFwdVPad + k;
+#pragma unroll
+      for (int e = 0; e < kFwdEB; ++e) {
+        if (e >= nb) break;
+        const float4 c = rec[b0 + e].c;
+        sk[e * SP] = sk[e * SP] * inv_cos_from_t_ftz(fmaf(c.y, kf, c.x));
+      }
+    }
+    __syncthreads();
+    if (tid < R) {
+      if (bp == 1)
+        fwd_rt_batch<1, true>(rec + b0, nb, buf, SP, mf, kc_lo, kc_hi, slice_start, bp, c0,
+                              acc_s, cj, q0, q1, q2);
+      else
+        fwd_rt_batch<0, true>(rec + b0, nb, buf, SP, mf, kc_lo, kc_hi, slice_start, bp, c0,
+                              acc_s, cj, q0, q1, q2);
+    }
+    __syncthreads();  // before the copy issued next round or batch overwrites buf
+  }
+  if (tid < R) {
+    float *a = acc_s + cj * nthr + tid;
+    a[0] += q0;
+    a[nthr] += q1;
+    a[2 * nthr] += q2;
+  }
+}
+
 template <typename EPI>
 __global__ void __launch_bounds__(1024)
 forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
@@ -1326,7 +1421,9 @@ cone_bin_wide_kernel(Geo g, const float *__restrict__ vp, int v_start,
 // epilogue sees the absolute view v_start + vl and partial slot
 // (v_start + vl) * nblk + block; touched[view * nblk + block] records
 // whether any pixel reached the tile.
-template <typename EPI>
+// ASYNC: the cylinders are staged asynchronously (fwd_rt_round_async; band a
+// multiple of 4 and 16-byte aligned cylinder rows, checked on the host).
+template <typename EPI, bool ASYNC>
 __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_start, const float *__restrict__ values, int P, int band,
                            int slice_start, const ConeFwdRec *__restrict__ recs,
                            const int *__restrict__ list, const int *__restrict__ offs,
@@ -1334,11 +1431,12 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
   MBIR_PDL_ENTRY();
   extern __shared__ float4 sm4[];
   const int nthr = blockDim.x, tid = threadIdx.x;
-  const int cap = fwd_cap(nthr);
+  const int cap = ASYNC ? fwd_cap_async(nthr) : fwd_cap(nthr);
   const int SP = band + 2 * kFwdVPad;
+  constexpr int NBUF = ASYNC ? 2 : 1;  // stage buffers
   ConeFwdRec *rec = reinterpret_cast<ConeFwdRec *>(sm4);
   float *stage = reinterpret_cast<float *>(rec + cap);
-  float *acc_s = stage + kFwdEB * SP;  // (kFwdCB + 4) x nthr
+  float *acc_s = stage + NBUF * kFwdEB * SP;  // (kFwdCB + 4) x nthr
   // (channel block, view) from the grid: views on x for whole-volume
   // epilogues (EPI::kViewFastest), so that the CTAs in flight are adjacent
   // views of one channel block, whose pixel strips nearly coincide and whose
@@ -1369,7 +1467,7 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
 
   // Zero padding either side of each staged cylinder (the interiors are
   // written by every batch before they are read).
-  for (int i = tid; i < kFwdEB * 2 * kFwdVPad; i += nthr) {
+  for (int i = tid; i < NBUF * kFwdEB * 2 * kFwdVPad; i += nthr) {
     const int e = i / (2 * kFwdVPad), o = i - e * 2 * kFwdVPad;
     stage[e * SP + (o < kFwdVPad ? o : band + o)] = 0.f;
   }
@@ -1383,6 +1481,11 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
     __syncthreads();
     for (int i = tid; i < n; i += nthr) rec[i] = fwd_stage_record(vrec[vlist[base + i]]);
     __syncthreads();
+    if (ASYNC) {
+      fwd_rt_round_async(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R,
+                         c0, acc_s);
+      continue;
+    }
     // The round's cylinders, 128-byte line by line, toward L1 ahead of the
     // batch staging.
     {
@@ -1402,14 +1505,15 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
   epi.end(v * nblk + blk);
 }
 
-template <typename EPI>
+template <typename EPI, bool ASYNC>
 __global__ void __launch_bounds__(1024)
 
 forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values, int P, int band,
                            int slice_start, const ConeFwdRec *__restrict__ recs,
                            const int *__restrict__ list, const int *__restrict__ offs,
                            unsigned char *__restrict__ touched, EPI epi) {
-  forward_cone_binned_kernel_body<EPI>(g, v_start, values, P, band, slice_start, recs, list, offs, touched, epi);
+  forward_cone_binned_kernel_body<EPI, ASYNC>(g, v_start, values, P, band, slice_start, recs, list,
+                                              offs, touched, epi);
 }
 
 // ── forward projection, parallel, binned ───────────────────────────────────
