@@ -346,12 +346,26 @@ __device__ __forceinline__ void back_cone_slices(float (&acc)[SPL], const float 
       const int mc = (int)mcf;
       const float d = m_p - mcf;
       float s = 0.f;
+      if (NT == 3) {
+        // |d| <= 1/2 (m_p is rounded to mcf; a clamped m_p is whole), so
+        // the outer taps' distances |d +- 1| are 1 +- d.
+        const float c1 = hw1r - 1.f;
+        float am = trap_w<SAT>(c1 - d, lmaxr), a0 = trap_w<SAT>(hw1r - fabsf(d), lmaxr),
+              ap = trap_w<SAT>(c1 + d, lmaxr);
+        if (CP == 2) {
+          am = am * am;
+          a0 = a0 * a0;
+          ap = ap * ap;
+        }
+        s = fmaf(ap, h[mc + 1], fmaf(a0, h[mc], am * h[mc - 1]));
+      } else {
 #pragma unroll
-      for (int t = 0; t < MT; ++t) {
-        if (MBIR_TAP_ON(NT, t, nt)) {
-          float a = trap_w<SAT>(hw1r - fabsf(d - (float)(t - RT)), lmaxr);
-          if (CP == 2) a = a * a;
-          s = fmaf(a, h[mc + t - RT], s);
+        for (int t = 0; t < MT; ++t) {
+          if (MBIR_TAP_ON(NT, t, nt)) {
+            float a = trap_w<SAT>(hw1r - fabsf(d - (float)(t - RT)), lmaxr);
+            if (CP == 2) a = a * a;
+            s = fmaf(a, h[mc + t - RT], s);
+          }
         }
       }
       const float tk = fmaf(a1, k, a0);
