@@ -506,10 +506,10 @@ def roofline_block(m, torch, y, kt, storage, hbm):
 
 
 # DRAM traffic of one forward + line-search launch of the headline workload's
-# 128-subset step (ncu dram__bytes_read.sum 559.0 MB + dram__bytes_write.sum
-# 460.3 MB, one captured launch): one read of e (439 MB), the A delta store
+# 128-subset step (ncu dram__bytes_read.sum 556.2 MB + dram__bytes_write.sum
+# 458.3 MB, one captured launch): one read of e (439 MB), the A delta store
 # (439 MB) and the records and cylinders.
-TRAFFIC_FWD_LS_FP32 = 1019375360.0
+TRAFFIC_FWD_LS_FP32 = 1014512128.0
 
 
 def projector_block(m, torch, dev):
