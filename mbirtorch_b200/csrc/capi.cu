@@ -582,15 +582,16 @@ int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count
                const int64_t *pix, long long P, const FwdBins &b, cudaStream_t st,
                int by_pixel = 0, bool wide = false) {
   const Geo geo = make_geo(*g);
+  const char *what = wide ? "forward binning" : "vcd forward binning";
   wide = wide || (P >= kBinWidePixels && t_batch == nullptr);
   if (wide && bin_smem(g, kBinWideThreads) <= (size_t)device_attrs().smem_optin) {
     const size_t smem_w = bin_smem(g, kBinWideThreads);
-    const int rc_smem = request_smem(cone_bin_wide_kernel, smem_w, "forward binning");
+    const int rc_smem = request_smem(cone_bin_wide_kernel, smem_w, what);
     if (rc_smem) return rc_smem;
     tpre(st);
     launch(cone_bin_wide_kernel, v_count, kBinWideThreads, smem_w, st, geo, vp, v_start, pix,
            (int)P, by_pixel, b.recs, b.list, b.offs);
-    MBIR_CHECK_LAUNCH("forward binning");
+    MBIR_CHECK_LAUNCH(what);
     return MBIR_OK;
   }
   const size_t smem = bin_smem(g);
@@ -599,9 +600,9 @@ int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count
     if (rc_smem) return rc_smem;
   }
   tpre(st);
-  launchb<ConeBinB>(v_count, kThreads, smem, st, "vcd forward binning", geo, vp, v_start, pix,
+  launchb<ConeBinB>(v_count, kThreads, smem, st, what, geo, vp, v_start, pix,
                     (int)P, by_pixel, b.recs, b.list, b.offs);
-  MBIR_CHECK_LAUNCH("vcd forward binning");
+  MBIR_CHECK_LAUNCH(what);
   return MBIR_OK;
 }
 
