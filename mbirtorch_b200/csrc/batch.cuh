@@ -101,11 +101,11 @@ struct ConeBinB {
   static auto kernel() { return cone_bin_kernel; }
   template <typename... A> __device__ static void run(const A &...a) { cone_bin_kernel_body(a...); }
 };
-template <typename EPI, bool ASYNC> struct FwdConeBinnedB {
+template <typename EPI, int AEB> struct FwdConeBinnedB {
   static constexpr int kMaxThreads = 1024, kMinBlocks = 1;
-  static auto kernel() { return forward_cone_binned_kernel<EPI, ASYNC>; }
+  static auto kernel() { return forward_cone_binned_kernel<EPI, AEB>; }
   template <typename... A> __device__ static void run(const A &...a) {
-    forward_cone_binned_kernel_body<EPI, ASYNC>(a...);
+    forward_cone_binned_kernel_body<EPI, AEB>(a...);
   }
 };
 template <typename EPI> struct FwdParBinnedB {

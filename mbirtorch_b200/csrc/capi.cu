@@ -503,13 +503,12 @@ size_t cone_rt_smem(const mbir_geometry *g, int band) {
          sizeof(float) * ((size_t)kFwdEB * (band + 2 * kFwdVPad) + (size_t)(kFwdCB + 4) * nthr);
 }
 
-// The binned cone forward with asynchronous staging: two stage buffers and
-// smaller record rounds.
-size_t cone_binned_async_smem(const mbir_geometry *g, int band) {
+// The binned cone forward with asynchronous staging in batches of eb
+// pixels: two stage buffers and smaller record rounds.
+size_t cone_binned_async_smem(const mbir_geometry *g, int band, int eb) {
   const int nthr = cone_rt_threads(g);
   return sizeof(ConeFwdRec) * (size_t)fwd_cap_async(nthr) +
-         sizeof(float) *
-             ((size_t)2 * kFwdEB * (band + 2 * kFwdVPad) + (size_t)(kFwdCB + 4) * nthr);
+         sizeof(float) * ((size_t)2 * eb * (band + 2 * kFwdVPad) + (size_t)(kFwdCB + 4) * nthr);
 }
 
 template <typename EPI>
@@ -606,67 +605,78 @@ int launch_bin(const mbir_geometry *g, const float *vp, int v_start, int v_count
   return MBIR_OK;
 }
 
+// Launch of the binned cone forward with staging variant AEB (see
+// forward_cone_binned_kernel_body).
+template <typename EPI, int AEB>
+int launch_binned_as(const Geo &geo, const dim3 &grid, int nthr, size_t smem, int v_start,
+                     const float *values, long long P, int band, const FwdBins &b,
+                     const EPI &epi, cudaStream_t st, const char *what) {
+  const int rc_smem = request_smem(forward_cone_binned_kernel<EPI, AEB>, smem, "forward");
+  if (rc_smem) return rc_smem;
+  tpre(st);
+  launchb<FwdConeBinnedB<EPI, AEB>>(grid, nthr, smem, st, what, geo, v_start, values, (int)P,
+                                    band, 0, (const ConeFwdRec *)b.recs, (const int *)b.list,
+                                    (const int *)b.offs, b.touched, epi);
+  MBIR_CHECK_LAUNCH(what);
+  return MBIR_OK;
+}
+
+// CTAs per SM of a variant (0 when the query fails or it does not fit).
+template <typename EPI, int AEB>
+int binned_occupancy(int nthr, size_t smem) {
+  if (smem > (size_t)device_attrs().smem_optin) return 0;
+  if (request_smem(forward_cone_binned_kernel<EPI, AEB>, smem, "forward")) return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, forward_cone_binned_kernel<EPI, AEB>,
+                                                    nthr, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
 template <typename EPI>
 int launch_binned(const mbir_geometry *g, int v_start, int v_count, const float *values,
                   long long P, int band, const FwdBins &b, const EPI &epi, cudaStream_t st,
                   const char *what) {
   const Geo geo = make_geo(*g);
   const dim3 grid = EPI::kViewFastest ? dim3(v_count, fwd_nblk(g)) : dim3(fwd_nblk(g), v_count);
-  // Asynchronous staging copies 16-byte chunks: whole cylinders of a
-  // multiple of 4 slices from a 16-byte aligned array, with room for two
-  // stage buffers.
-  // It is taken where it keeps as many CTAs per SM as the synchronous
-  // staging (its second stage buffer can cost one: the 256-row detector of
-  // the 256^3 cone workload runs 4 CTAs per SM synchronously, 3 with it).
   const int nthr = cone_rt_threads(g);
-  const size_t smem_a = cone_binned_async_smem(g, band), smem_s = cone_rt_smem(g, band);
-  bool async = band >= 4 && band % 4 == 0 && (reinterpret_cast<uintptr_t>(values) & 15) == 0 &&
-               smem_a <= (size_t)device_attrs().smem_optin;
-  if (async) {
-    int rc_smem = request_smem(forward_cone_binned_kernel<EPI, true>, smem_a, "forward");
-    if (rc_smem) return rc_smem;
-    // The occupancy answer for the last (device, threads, band) seen by this
-    // thread and epilogue.
-    static thread_local int last_dev = -1, last_nthr = -1, last_band = -1;
-    static thread_local bool last_async = false;
+  const size_t smem_s = cone_rt_smem(g, band);
+  const size_t smem_16 = cone_binned_async_smem(g, band, kFwdEB);
+  const size_t smem_8 = cone_binned_async_smem(g, band, kFwdEB / 2);
+  // Asynchronous staging copies 16-byte chunks: whole cylinders of a
+  // multiple of 4 slices from a 16-byte aligned array.  Its second stage
+  // buffer can cost a CTA per SM (the 256-row detector of the 256^3 cone
+  // workload runs 4 CTAs per SM synchronously, 3 with two 16-pixel
+  // buffers), so it is taken in 16-pixel batches where that keeps the
+  // synchronous staging's CTAs per SM, else in 8-pixel batches where those
+  // keep them, else not.  The choice for the last (device, threads, band)
+  // is kept per thread and epilogue.
+  int variant = 0;
+  if (band >= 4 && band % 4 == 0 && (reinterpret_cast<uintptr_t>(values) & 15) == 0) {
+    static thread_local int last_dev = -1, last_nthr = -1, last_band = -1, last_variant = 0;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev != last_dev || nthr != last_nthr || band != last_band) {
-      rc_smem = request_smem(forward_cone_binned_kernel<EPI, false>, smem_s, "forward");
-      if (rc_smem) return rc_smem;
-      int n_a = 0, n_s = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-              &n_a, forward_cone_binned_kernel<EPI, true>, nthr, smem_a) != cudaSuccess ||
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-              &n_s, forward_cone_binned_kernel<EPI, false>, nthr, smem_s) != cudaSuccess) {
-        cudaGetLastError();
-        n_a = 0;
-      }
+      const int n_s = binned_occupancy<EPI, 0>(nthr, smem_s);
+      const int n_16 = binned_occupancy<EPI, kFwdEB>(nthr, smem_16);
+      const int n_8 = binned_occupancy<EPI, kFwdEB / 2>(nthr, smem_8);
+      last_variant = (n_16 > 0 && n_16 >= n_s) ? kFwdEB : (n_8 > 0 && n_8 >= n_s) ? kFwdEB / 2 : 0;
       last_dev = dev;
       last_nthr = nthr;
       last_band = band;
-      last_async = n_a > 0 && n_a >= n_s;
     }
-    async = last_async;
+    variant = last_variant;
   }
-  if (async) {
-    tpre(st);
-    launchb<FwdConeBinnedB<EPI, true>>(grid, nthr, smem_a, st, what, geo, v_start,
-                                       values, (int)P, band, 0, (const ConeFwdRec *)b.recs,
-                                       (const int *)b.list, (const int *)b.offs, b.touched, epi);
-    MBIR_CHECK_LAUNCH(what);
-    return MBIR_OK;
-  }
-  {
-    const int rc_smem = request_smem(forward_cone_binned_kernel<EPI, false>, smem_s, "forward");
-    if (rc_smem) return rc_smem;
-  }
-  tpre(st);
-  launchb<FwdConeBinnedB<EPI, false>>(grid, nthr, smem_s, st, what, geo, v_start,
-                                      values, (int)P, band, 0, (const ConeFwdRec *)b.recs,
-                                      (const int *)b.list, (const int *)b.offs, b.touched, epi);
-  MBIR_CHECK_LAUNCH(what);
-  return MBIR_OK;
+  if (variant == kFwdEB)
+    return launch_binned_as<EPI, kFwdEB>(geo, grid, nthr, smem_16, v_start, values, P, band, b,
+                                         epi, st, what);
+  if (variant == kFwdEB / 2)
+    return launch_binned_as<EPI, kFwdEB / 2>(geo, grid, nthr, smem_8, v_start, values, P, band,
+                                             b, epi, st, what);
+  return launch_binned_as<EPI, 0>(geo, grid, nthr, smem_s, v_start, values, P, band, b, epi, st,
+                                  what);
 }
 
 template <typename EPI>

@@ -1069,10 +1069,13 @@ __device__ __forceinline__ void cp_async_wait() {
 __host__ __device__ inline int fwd_cap_async(int nthr) { return min(fwd_cap(nthr), 256); }
 
 // fwd_rt_round<true> with the cylinders staged asynchronously (band a
-// multiple of 4, 16-byte aligned cylinder rows): two stage buffers; the raw
+// multiple of 4, 16-byte aligned cylinder rows), in batches of EB pixels
+// (EB <= kFwdEB; a smaller batch keeps the two buffers in the shared memory
+// of one synchronous buffer): two stage buffers; the raw
 // cylinders of batch b + 1 are copied global -> shared while batch b is
 // projected, and each batch is scaled by 1 / cos(phi) in place once it has
 // landed.  The staged values and every sum are the same as fwd_rt_round's.
+template <int EB>
 __device__ __forceinline__ void fwd_rt_round_async(const ConeFwdRec *__restrict__ rec, int n,
                                                    float *__restrict__ stage2, int SP,
                                                    const float *__restrict__ values, int band,
@@ -1084,14 +1087,14 @@ __device__ __forceinline__ void fwd_rt_round_async(const ConeFwdRec *__restrict_
   int cj = __float_as_int(rec[0].c.z) - c0 + 1;
   float q0 = 0.f, q1 = 0.f, q2 = 0.f;
   const int q4 = band >> 2;  // 16-byte chunks per cylinder (band >= 4)
-  const int nbat = (n + kFwdEB - 1) / kFwdEB;
+  const int nbat = (n + EB - 1) / EB;
   // This thread's chunks i = tid, tid + nthr, ... as (pixel e, chunk q),
   // stepped without a division per chunk.
   const int e_step = nthr / q4, q_step = nthr - e_step * q4;
   const int e_first = tid / q4, q_first = tid - e_first * q4;
   auto issue = [&](int b) {
-    const int b0 = b * kFwdEB, nb = min(kFwdEB, n - b0);
-    float *buf = stage2 + (b & 1) * kFwdEB * SP + kFwdVPad;
+    const int b0 = b * EB, nb = min(EB, n - b0);
+    float *buf = stage2 + (b & 1) * EB * SP + kFwdVPad;
     int e = e_first, q = q_first;
     while (e < nb) {
       cp_async16(buf + e * SP + 4 * q,
@@ -1107,7 +1110,7 @@ __device__ __forceinline__ void fwd_rt_round_async(const ConeFwdRec *__restrict_
   };
   issue(0);
   for (int b = 0; b < nbat; ++b) {
-    const int b0 = b * kFwdEB, nb = min(kFwdEB, n - b0);
+    const int b0 = b * EB, nb = min(EB, n - b0);
     if (b + 1 < nbat) {
       issue(b + 1);
       cp_async_wait<1>();  // this thread's copies of batch b have landed
@@ -1115,12 +1118,12 @@ __device__ __forceinline__ void fwd_rt_round_async(const ConeFwdRec *__restrict_
       cp_async_wait<0>();
     }
     __syncthreads();
-    float *buf = stage2 + (b & 1) * kFwdEB * SP;
+    float *buf = stage2 + (b & 1) * EB * SP;
     for (int k = tid; k < band; k += nthr) {
       const float kf = (float)(slice_start + k);
       float *sk = buf + kFwdVPad + k;
 #pragma unroll
-      for (int e = 0; e < kFwdEB; ++e) {
+      for (int e = 0; e < EB; ++e) {
         if (e >= nb) break;
         const float4 c = rec[b0 + e].c;
         sk[e * SP] = sk[e * SP] * inv_cos_from_t_ftz(fmaf(c.y, kf, c.x));
@@ -1435,9 +1438,10 @@ cone_bin_wide_kernel(Geo g, const float *__restrict__ vp, int v_start,
 // epilogue sees the absolute view v_start + vl and partial slot
 // (v_start + vl) * nblk + block; touched[view * nblk + block] records
 // whether any pixel reached the tile.
-// ASYNC: the cylinders are staged asynchronously (fwd_rt_round_async; band a
-// multiple of 4 and 16-byte aligned cylinder rows, checked on the host).
-template <typename EPI, bool ASYNC>
+// AEB > 0: the cylinders are staged asynchronously in batches of AEB pixels
+// (fwd_rt_round_async; band a multiple of 4 and 16-byte aligned cylinder
+// rows, checked on the host); AEB = 0: synchronously, kFwdEB at a time.
+template <typename EPI, int AEB>
 __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_start, const float *__restrict__ values, int P, int band,
                            int slice_start, const ConeFwdRec *__restrict__ recs,
                            const int *__restrict__ list, const int *__restrict__ offs,
@@ -1445,12 +1449,13 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
   MBIR_PDL_ENTRY();
   extern __shared__ float4 sm4[];
   const int nthr = blockDim.x, tid = threadIdx.x;
+  constexpr bool ASYNC = AEB > 0;
   const int cap = ASYNC ? fwd_cap_async(nthr) : fwd_cap(nthr);
   const int SP = band + 2 * kFwdVPad;
-  constexpr int NBUF = ASYNC ? 2 : 1;  // stage buffers
+  constexpr int SEB = ASYNC ? 2 * AEB : kFwdEB;  // staged cylinders (both buffers)
   ConeFwdRec *rec = reinterpret_cast<ConeFwdRec *>(sm4);
   float *stage = reinterpret_cast<float *>(rec + cap);
-  float *acc_s = stage + NBUF * kFwdEB * SP;  // (kFwdCB + 4) x nthr
+  float *acc_s = stage + SEB * SP;  // (kFwdCB + 4) x nthr
   // (channel block, view) from the grid: views on x for whole-volume
   // epilogues (EPI::kViewFastest), so that the CTAs in flight are adjacent
   // views of one channel block, whose pixel strips nearly coincide and whose
@@ -1481,7 +1486,7 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
 
   // Zero padding either side of each staged cylinder (the interiors are
   // written by every batch before they are read).
-  for (int i = tid; i < NBUF * kFwdEB * 2 * kFwdVPad; i += nthr) {
+  for (int i = tid; i < SEB * 2 * kFwdVPad; i += nthr) {
     const int e = i / (2 * kFwdVPad), o = i - e * 2 * kFwdVPad;
     stage[e * SP + (o < kFwdVPad ? o : band + o)] = 0.f;
   }
@@ -1495,9 +1500,9 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
     __syncthreads();
     for (int i = tid; i < n; i += nthr) rec[i] = fwd_stage_record(vrec[vlist[base + i]]);
     __syncthreads();
-    if (ASYNC) {
-      fwd_rt_round_async(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp, g.R,
-                         c0, acc_s);
+    if constexpr (ASYNC) {
+      fwd_rt_round_async<AEB>(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp,
+                              g.R, c0, acc_s);
       continue;
     }
     // The round's cylinders, 128-byte line by line, toward L1 ahead of the
@@ -1519,14 +1524,14 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
   epi.end(v * nblk + blk);
 }
 
-template <typename EPI, bool ASYNC>
+template <typename EPI, int AEB>
 __global__ void __launch_bounds__(1024)
 
 forward_cone_binned_kernel(Geo g, int v_start, const float *__restrict__ values, int P, int band,
                            int slice_start, const ConeFwdRec *__restrict__ recs,
                            const int *__restrict__ list, const int *__restrict__ offs,
                            unsigned char *__restrict__ touched, EPI epi) {
-  forward_cone_binned_kernel_body<EPI, ASYNC>(g, v_start, values, P, band, slice_start, recs, list,
+  forward_cone_binned_kernel_body<EPI, AEB>(g, v_start, values, P, band, slice_start, recs, list,
                                               offs, touched, epi);
 }
 
