@@ -492,7 +492,22 @@ def roofline_block(m, torch, y, kt, storage, hbm):
     # DRAM bytes per launch of the dominant kernel (ncu, dram__bytes_read.sum +
     # dram__bytes_write.sum) on this workload's 128-subset step, FP32 storage.
     traffic = {("vcd forward + line search", "float32"): TRAFFIC_FWD_LS_FP32}
+    # The kernel is instruction-issue-bound, not HBM-bound: its warp
+    # instructions per launch (ncu smsp__inst_executed.sum) over the same
+    # CUDA-event launch time, against one warp instruction per cycle per SM
+    # sub-partition at the maximum SM clock.
+    issue = None
+    winst = {("vcd forward + line search", "float32"): WARP_INST_FWD_LS_FP32}.get((top, storage))
+    if winst:
+        props = torch.cuda.get_device_properties(torch.cuda.current_device())
+        peak_i = props.multi_processor_count * 4 * SM_MAX_MHZ * 1e6
+        ach_i = winst / (tms / tcnt / 1e3)
+        issue = {"warp_instructions_per_launch": winst, "achieved_warp_inst_per_s": ach_i,
+                 "peak_warp_inst_per_s": peak_i, "frac": ach_i / peak_i,
+                 "peak_rule": f"{props.multi_processor_count} SMs x 4 sub-partitions x "
+                              f"{SM_MAX_MHZ} MHz"}
     return {"kernel": top, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+            "issue": issue,
             "frac": ach / hbm, "traffic": traffic.get((top, storage)),
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
                               "(profiles/), 128-subset step of this workload",
@@ -510,6 +525,10 @@ def roofline_block(m, torch, y, kt, storage, hbm):
 # 458.3 MB, one captured launch): one read of e (439 MB), the A delta store
 # (439 MB) and the records and cylinders.
 TRAFFIC_FWD_LS_FP32 = 1014512128.0
+# Warp instructions of the same launch (ncu smsp__inst_executed.sum), and
+# the SM clock the issue peak is taken at (clocks.max.sm of this pool's B200s).
+WARP_INST_FWD_LS_FP32 = 1084691937
+SM_MAX_MHZ = 1965
 
 
 def projector_block(m, torch, dev):
