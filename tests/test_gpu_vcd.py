@@ -569,3 +569,37 @@ def test_error_refresh_binned_equals_scanning(kind, storage):
     ref = (y - m.projector.forward_volume(flat, idx)).transpose(1, 2)
     d_ref = float((outs[1] - ref).norm()) / ynorm
     assert d_ref <= (1e-6 if storage == 'float32' else 1e-3 * float(ref.norm()) / ynorm), d_ref
+
+
+def test_large_subset_step_vs_oracle():
+    """A subset of every ROR pixel (above 16 384 pixels: its records are
+    binned with 1024 threads per view, as in the first pass of a large
+    recon) against the FP64 oracle's SubsetUpdater from the same state."""
+    from oracle import vcd as ovcd
+    m = mb.ConeBeamModel((40, 20, 330), np.linspace(0, 2 * np.pi, 40, endpoint=False),
+                         300.0, 150.0)
+    m.set_params(no_warning=True, verbose=0, recon_shape=(160, 160, 8))
+    rs = m.get_params('recon_shape')
+    rng = np.random.default_rng(9)
+    x_true = rng.random(rs).astype(np.float32)
+    sino = m.forward_project(x_true)
+    m.auto_set_regularization_params(sino)
+    x0 = (0.1 * rng.random(rs)).astype(np.float32)
+    e0 = sino - m.forward_project(x0)
+    H = m.compute_hessian_diagonal()
+    upd = m.create_vcd_subset_updater(H, weights=1)
+    idx = mb.gen_full_indices(rs).astype(np.int64)
+    assert idx.size >= 16384
+    flat = torch.as_tensor(x0.reshape(-1, rs[2]), device='cuda').clone()
+    err = torch.as_tensor(e0, device='cuda').clone()
+    flat, err, ell1, alpha, sumsq = upd(flat, err, torch.as_tensor(idx, device='cuda'))
+    prob = _oracle_problem(m)
+    sy, sx = m.get_params(['sigma_y', 'sigma_x'])
+    ou = ovcd.SubsetUpdater(prob, np.asarray(H).reshape(-1, rs[2]), None, sy, sx,
+                            dc_profile=ovcd.dc_damping_profile(prob))
+    oflat = x0.reshape(-1, rs[2]).astype(np.float64)
+    oerr = e0.astype(np.float64)
+    oell1, oalpha, osumsq = ou(oflat, oerr, idx)
+    assert abs(float(alpha) - oalpha) / oalpha <= 1e-4
+    assert rel_l2(flat.cpu().numpy(), oflat) <= 1e-5
+    assert rel_l2(err.cpu().numpy(), oerr) <= 1e-5
