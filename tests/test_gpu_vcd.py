@@ -571,14 +571,17 @@ def test_error_refresh_binned_equals_scanning(kind, storage):
     assert d_ref <= (1e-6 if storage == 'float32' else 1e-3 * float(ref.norm()) / ynorm), d_ref
 
 
-def test_large_subset_step_vs_oracle():
-    """A subset of every ROR pixel (above 16 384 pixels: its records are
+@pytest.mark.parametrize("slices,subset", [(8, None), (7, 300)])
+def test_large_subset_step_vs_oracle(slices, subset):
+    """Subset steps against the FP64 oracle's SubsetUpdater from the same
+    state: a subset of every ROR pixel (above 16 384 pixels: its records are
     binned with 1024 threads per view, as in the first pass of a large
-    recon) against the FP64 oracle's SubsetUpdater from the same state."""
+    recon), and a 7-slice volume (cylinders that are not a multiple of 4
+    slices: the forward stages them synchronously)."""
     from oracle import vcd as ovcd
     m = mb.ConeBeamModel((40, 20, 330), np.linspace(0, 2 * np.pi, 40, endpoint=False),
                          300.0, 150.0)
-    m.set_params(no_warning=True, verbose=0, recon_shape=(160, 160, 8))
+    m.set_params(no_warning=True, verbose=0, recon_shape=(160, 160, slices))
     rs = m.get_params('recon_shape')
     rng = np.random.default_rng(9)
     x_true = rng.random(rs).astype(np.float32)
@@ -590,6 +593,8 @@ def test_large_subset_step_vs_oracle():
     upd = m.create_vcd_subset_updater(H, weights=1)
     idx = mb.gen_full_indices(rs).astype(np.int64)
     assert idx.size >= 16384
+    if subset is not None:
+        idx = np.sort(rng.choice(idx, size=subset, replace=False)).astype(np.int64)
     flat = torch.as_tensor(x0.reshape(-1, rs[2]), device='cuda').clone()
     err = torch.as_tensor(e0, device='cuda').clone()
     flat, err, ell1, alpha, sumsq = upd(flat, err, torch.as_tensor(idx, device='cuda'))
