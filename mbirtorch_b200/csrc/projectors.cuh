@@ -821,7 +821,9 @@ forward_kernel(Geo g, const float *__restrict__ vp, int v_start, const float *__
 }
 
 // ── forward projection, cone, row-tiled ────────────────────────────────────
-// The cone forward for psf radius 1 and up to 1024 detector rows.  A CTA
+// The cone forward for psf radius 1 and up to 1024 detector rows (the
+// scanning form of a slice band here; the binned form below shares the row
+// loop and, where it applies, stages asynchronously).  A CTA
 // owns one view and kFwdCB channels; thread m owns detector row m and its
 // kFwdCB channel sums, held in a thread-private column of shared memory
 // (kFwdCB + 4 rows so that the three taps of any reaching pixel land
@@ -1231,8 +1233,9 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
 
 // ── forward projection, cone, binned ───────────────────────────────────────
 // For a pixel subset that several launches use (the VCD gradient, forward
-// and positivity re-projection), the (view, pixel) records are formed once by
-// cone_bin_kernel and sorted by centre channel, so that each forward CTA
+// and positivity re-projection), and for whole volumes a chunk of views at a
+// time, the (view, pixel) records are formed once by cone_bin_kernel (or its
+// 1024-thread form) and sorted by centre channel, so that each forward CTA
 // reads exactly its pixels, in channel order, instead of scanning the subset
 // and re-forming every pixel's geometry (atan2, sin/cos, divisions) in each
 // of the C / kFwdCB blocks of a view.
