@@ -1148,6 +1148,45 @@ def triton_reference_extra(mb, torch):
     return out
 
 
+def reference_gpu_recon_extra(mb, torch, names=("cone256_flat", HEAD)):
+    """Whole reconstructions by the reference's own GPU path (mbirtorch 0.0.2
+    from baseline/_ref on this GPU: its Triton projector bodies, its eager
+    torch VCD updater and loop, compile_mode='off') against this package on
+    the same numpy sinogram with the same seed (so the same partitions):
+    seconds per recon through each package's `recon` (host sinogram in, host
+    volume out), and the relative L2 between the two volumes."""
+    ref = import_reference()
+    if ref is None:
+        return {"unavailable": "reference not installed under baseline/_ref"}
+    dev = torch.device("cuda", 0)
+    out = {"reference": f"mbirtorch {ref.__version__} (baseline/_ref), compile_mode='off'"}
+    for name in names:
+        res = {}
+        try:
+            mm = cone_model(mb, name)
+            rm = cone_model(ref, name, compile_mode='off')
+            rm.configure_devices(devices=['cuda:0'])
+            y = make_data(mm, torch, dev, 5).cpu().numpy()
+            for who, model in (("mbirtorch_b200", mm), ("reference", rm)):
+                recon(model, y, iters=2)  # warm-up (Triton compiles on first use)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                r, rd = recon(model, y)
+                torch.cuda.synchronize()
+                res[who] = {"seconds": time.perf_counter() - t0,
+                            "fm_rmse_final": float(rd["recon_params"]["fm_rmse"][-1])}
+                res[who + "_volume"] = np.asarray(r, dtype=np.float64)
+            a, b = res.pop("mbirtorch_b200_volume"), res.pop("reference_volume")
+            res["rel_l2_mine_vs_reference"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+            res["ratio"] = res["reference"]["seconds"] / res["mbirtorch_b200"]["seconds"]
+            res["workload"] = workload(name)
+        except Exception as exc:
+            res = {"error": repr(exc)[:400]}
+        torch.cuda.empty_cache()
+        out[name] = res
+    return out
+
+
 # ── main ────────────────────────────────────────────────────────────────────
 def main():
     args = parse()
@@ -1244,7 +1283,8 @@ def main():
 
 
 EXTRAS = ("roofline", "cpu_baseline", "projectors", "mixed_precision", "cone256_flat",
-          "parallel_subset", "serving_mix", "serving_batching", "autograd", "triton_reference")
+          "parallel_subset", "serving_mix", "serving_batching", "autograd", "triton_reference",
+          "reference_gpu_recon")
 
 
 def extras(args, m, mb, torch, dev, y, rec_ref, full=True):
@@ -1288,6 +1328,7 @@ def extras(args, m, mb, torch, dev, y, rec_ref, full=True):
     run("serving_batching", lambda: serving_batching_extra(mb, torch))
     run("autograd", lambda: autograd_extra(mb, torch))
     run("triton_reference", lambda: triton_reference_extra(mb, torch))
+    run("reference_gpu_recon", lambda: reference_gpu_recon_extra(mb, torch))
     return res
 
 
