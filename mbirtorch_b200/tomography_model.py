@@ -544,11 +544,18 @@ class TomographyModel(ParameterHandler):
         if torch.is_tensor(sinogram):
             if sinogram.is_complex():
                 raise TypeError("sinogram must be real-valued; got complex dtype.")
+            if on_device and not sinogram.is_cuda:
+                # A host tensor (pinned or not) goes to the device before the
+                # checks, which then run there instead of on the host cores.
+                sinogram = self._sino_device(sinogram)
             if not bool(torch.isfinite(sinogram).all()):
                 raise ValueError("sinogram contains NaN and/or Inf values.")
         if weights is not None:
             if not torch.is_tensor(weights) and on_device and np.ndim(weights) > 0:
                 weights = self._sino_device(np.asarray(weights))
+            elif (torch.is_tensor(weights) and on_device and not weights.is_cuda
+                  and weights.ndim > 0):
+                weights = self._sino_device(weights)
             if torch.is_tensor(weights):
                 if not bool(torch.isfinite(weights).all()):
                     raise ValueError("weights contains NaN and/or Inf values.")
