@@ -75,6 +75,24 @@ inline Geo make_geo(const mbir_geometry &g) {
   return o;
 }
 
+// ── shared-memory loads at 32-bit addresses ────────────────────────────────
+// The forward's row loop forms its record and stage addresses as 32-bit
+// shared-window offsets (__cvta_generic_to_shared of the CTA's buffers plus
+// a byte offset) and loads with ld.shared, which measured fewer integer
+// instructions per iteration than indexing the generic pointers.
+__device__ __forceinline__ float lds_f32(unsigned a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ float4 lds_f32x4(unsigned a) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(a));
+  return v;
+}
+
 // ── storage types ──────────────────────────────────────────────────────────
 __device__ __forceinline__ float to_f32(float v) { return v; }
 __device__ __forceinline__ float to_f32(__nv_bfloat16 v) { return __bfloat162float(v); }

@@ -336,11 +336,14 @@ __device__ __forceinline__ void back_cone_slices(float (&acc)[SPL], const float 
                                                  float a1, float mlo_clamp, float mhi_clamp,
                                                  int RT, int nt) {
   constexpr int MT = MBIR_TAPS(NT);
+  // k = slice_start + l as a float, formed by adding whole numbers below
+  // 2^24 to one conversion (exact, the same value as converting each).
+  const float kb = (float)(slice_start + l1);
 #pragma unroll
   for (int j = 0; j < SPL; ++j) {
     const int l = l1 + 32 * j;
     if (l < band) {
-      const float k = (float)(slice_start + l);
+      const float k = kb + (float)(32 * j);
       const float m_p = fminf(fmaxf(fmaf(w_r, k, m0), mlo_clamp), mhi_clamp);
       const float mcf = rintf(m_p);
       const int mc = (int)mcf;
@@ -882,8 +885,13 @@ __device__ __forceinline__ void fwd_block_range(int ctr, int C, int &b_lo, int &
 // time.  A tap weight clamp(x, 0, lmax) is formed as min(sat(x), lmax),
 // the same value for lmax = min(w_r, 1) <= 1, with no branch on lmax.
 //
-// The shared records hold -m0 / w_r in a.x (fwd_stage_record), so that the
-// row's centre slice k_m = (m - m0) / w_r is one FMA.
+// The shared records hold -m0 / w_r in a.x and the centre's accumulator
+// slot j = ctr - c0 + 1 in c.z (fwd_stage_record), so that the row's centre
+// slice k_m = (m - m0) / w_r is one FMA and the slot needs no arithmetic.
+// For BP = 1 with sorted records the warp takes the pixels left to walk four
+// (or two) at a time: it forms the fans of all of them first, then adds
+// them in pixel order, so every sum is the same sequence of FMAs as one
+// pixel at a time, with the loads of four pixels in flight together.
 template <int BP, bool SORTED>
 __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec, int nb,
                                              const float *__restrict__ stage, int SP, float mf,
@@ -912,13 +920,103 @@ __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec,
     const unsigned skip = __ballot_sync(__activemask(), out);
     todo = ~skip & (nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u));
   }
+  const unsigned rec_s = (unsigned)__cvta_generic_to_shared(rec);
+  const unsigned st_s =
+      (unsigned)__cvta_generic_to_shared(stage) + 4u * (unsigned)(kFwdVPad - slice_start);
+  if (BP == 1 && SORTED) {
+    // Pixel e's fan on this row: its slot j, its channel tap weights (rb.y ..
+    // rb.w) and the three staged values around the clamped centre slice
+    // with their vertical weights.  |kc - k_m| <= 1/2 wherever the taps can
+    // meet the band (elsewhere they meet the zero padding), so |d| <= w_r / 2:
+    // the outer taps' distances |d -+ w_r| are w_r -+ d.
+    auto fan = [&](int e, float4 &rb, int &j) -> float {
+      const unsigned ra_s = rec_s + (unsigned)e * (unsigned)sizeof(ConeFwdRec);
+      const float4 ra = lds_f32x4(ra_s);
+      rb = lds_f32x4(ra_s + 16u);
+      j = __float_as_int(lds_f32(ra_s + 40u));  // c.z, in [0, kFwdCB + 1]
+      const float nm = ra.x, w_r = ra.y, hw1r = ra.z, lmaxr = ra.w;
+      const float k_m = fmaf(mf, rb.x, nm);
+      const float kc = fminf(fmaxf(rintf(k_m), kc_lo), kc_hi);
+      const float d = w_r * (kc - k_m);
+      const unsigned st_a = st_s + 4u * (unsigned)(e * SP + (int)kc);
+      const float c1 = hw1r - w_r;
+      const float am = fminf(__saturatef(c1 + d), lmaxr);
+      const float a0 = fminf(__saturatef(hw1r - fabsf(d)), lmaxr);
+      const float ap = fminf(__saturatef(c1 - d), lmaxr);
+      return fmaf(ap, lds_f32(st_a + 4u), fmaf(a0, lds_f32(st_a), am * lds_f32(st_a - 4u)));
+    };
+    // Its three taps into rows j .. j + 2 of the accumulator column, kept in
+    // q0..q2 while the slot stays (fwd_rt_round).
+    auto add = [&](int j, const float4 &rb, float det) {
+      if (j != cj) {  // uniform over the warp; j > cj
+        float *a = acc_s + cj * nthr + tid;
+        a[0] += q0;
+        if (j == cj + 1) {
+          q0 = q1;
+          q1 = q2;
+        } else {
+          a[nthr] += q1;
+          if (j == cj + 2) {
+            q0 = q2;
+          } else {
+            a[2 * nthr] += q2;
+            q0 = 0.f;
+          }
+          q1 = 0.f;
+        }
+        q2 = 0.f;
+        cj = j;
+      }
+      q0 = fmaf(rb.y, det, q0);
+      q1 = fmaf(rb.z, det, q1);
+      q2 = fmaf(rb.w, det, q2);
+    };
+#pragma unroll 1
+    while (todo) {  // uniform over the warp
+      const int e0 = __ffs(todo) - 1;
+      todo &= todo - 1u;
+      if (__popc(todo) >= 3) {
+        const int e1 = __ffs(todo) - 1;
+        todo &= todo - 1u;
+        const int e2 = __ffs(todo) - 1;
+        todo &= todo - 1u;
+        const int e3 = __ffs(todo) - 1;
+        todo &= todo - 1u;
+        float4 rb0, rb1, rb2, rb3;
+        int j0, j1, j2, j3;
+        const float det0 = fan(e0, rb0, j0);
+        const float det1 = fan(e1, rb1, j1);
+        const float det2 = fan(e2, rb2, j2);
+        const float det3 = fan(e3, rb3, j3);
+        add(j0, rb0, det0);
+        add(j1, rb1, det1);
+        add(j2, rb2, det2);
+        add(j3, rb3, det3);
+      } else if (todo) {
+        const int e1 = __ffs(todo) - 1;
+        todo &= todo - 1u;
+        float4 rb0, rb1;
+        int j0, j1;
+        const float det0 = fan(e0, rb0, j0);
+        const float det1 = fan(e1, rb1, j1);
+        add(j0, rb0, det0);
+        add(j1, rb1, det1);
+      } else {
+        float4 rb0;
+        int j0;
+        const float det0 = fan(e0, rb0, j0);
+        add(j0, rb0, det0);
+      }
+    }
+    return;
+  }
 #pragma unroll 1
   while (todo) {  // uniform over the warp
     const int e = __ffs(todo) - 1;
     todo &= todo - 1u;
-    const ConeFwdRec *r = rec + e;
-    const float4 ra = r->a, rb = r->b;
-    const int j = __float_as_int(r->c.z) - c0 + 1;  // in [0, kFwdCB + 1]
+    const unsigned ra_s = rec_s + (unsigned)e * (unsigned)sizeof(ConeFwdRec);
+    const float4 ra = lds_f32x4(ra_s), rb = lds_f32x4(ra_s + 16u);
+    const int j = __float_as_int(lds_f32(ra_s + 40u));  // c.z, in [0, kFwdCB + 1]
     const float nm = ra.x, w_r = ra.y, hw1r = ra.z, lmaxr = ra.w;
     if (SORTED && j != cj) {  // uniform over the warp; j > cj
       float *a = acc_s + cj * nthr + tid;
@@ -942,6 +1040,7 @@ __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec,
     const float k_m = fmaf(mf, rb.x, nm);
     const float kc = fminf(fmaxf(rintf(k_m), kc_lo), kc_hi);
     const float d = w_r * (kc - k_m);
+    const unsigned st_a = st_s + 4u * (unsigned)(e * SP + (int)kc);
     const float *st = stage + e * SP + kFwdVPad + ((int)kc - slice_start);
     float det;
     if (BP == 1) {
@@ -952,7 +1051,7 @@ __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec,
       const float am = fminf(__saturatef(c1 + d), lmaxr);
       const float a0 = fminf(__saturatef(hw1r - fabsf(d)), lmaxr);
       const float ap = fminf(__saturatef(c1 - d), lmaxr);
-      det = fmaf(ap, st[1], fmaf(a0, st[0], am * st[-1]));
+      det = fmaf(ap, lds_f32(st_a + 4u), fmaf(a0, lds_f32(st_a), am * lds_f32(st_a - 4u)));
     } else {
       det = 0.f;
       for (int ko = -bp; ko <= bp; ++ko) {
@@ -975,10 +1074,13 @@ __device__ __forceinline__ void fwd_rt_batch(const ConeFwdRec *__restrict__ rec,
   }
 }
 
-// A record as the forward CTAs keep it in shared memory: a.x = -m0 / w_r
-// (the row-to-slice offset) instead of m0; the other fields as formed.
-__device__ __forceinline__ ConeFwdRec fwd_stage_record(ConeFwdRec r) {
+// A record as the forward CTA of channel block c0 keeps it in shared
+// memory: a.x = -m0 / w_r (the row-to-slice offset) instead of m0, and c.z
+// = the centre's accumulator slot ctr - c0 + 1 (int bits) instead of the
+// centre channel; the other fields as formed.
+__device__ __forceinline__ ConeFwdRec fwd_stage_record(ConeFwdRec r, int c0) {
   r.a.x = -r.a.x * r.b.x;
+  r.c.z = __int_as_float(__float_as_int(r.c.z) - c0 + 1);
   return r;
 }
 
@@ -999,7 +1101,7 @@ __device__ __forceinline__ void fwd_rt_round(const ConeFwdRec *__restrict__ rec,
                                              int R, int c0, float *__restrict__ acc_s) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   const float mf = (float)tid;
-  int cj = SORTED ? __float_as_int(rec[0].c.z) - c0 + 1 : 0;
+  int cj = SORTED ? __float_as_int(rec[0].c.z) : 0;
   float q0 = 0.f, q1 = 0.f, q2 = 0.f;
   for (int b0 = 0; b0 < n; b0 += kFwdEB) {
     const int nb = min(kFwdEB, n - b0);
@@ -1086,7 +1188,7 @@ __device__ __forceinline__ void fwd_rt_round_async(const ConeFwdRec *__restrict_
                                                    float *__restrict__ acc_s) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   const float mf = (float)tid;
-  int cj = __float_as_int(rec[0].c.z) - c0 + 1;
+  int cj = __float_as_int(rec[0].c.z);
   float q0 = 0.f, q1 = 0.f, q2 = 0.f;
   const int q4 = band >> 2;  // 16-byte chunks per cylinder (band >= 4)
   const int nbat = (n + EB - 1) / EB;
@@ -1214,7 +1316,7 @@ forward_cone_rt_kernel(Geo g, const float *__restrict__ vp, int v_start,
       }
       if (keep)
         rec[off + __popc(bal & ((1u << lane) - 1u))] =
-            fwd_stage_record(cone_fwd_record(g, ang, z_off, cc, by_pixel ? (int)pix[p] : p));
+            fwd_stage_record(cone_fwd_record(g, ang, z_off, cc, by_pixel ? (int)pix[p] : p), c0);
       n += tot;
       pos += nthr;
       __syncthreads();
@@ -1501,7 +1603,7 @@ __device__ __forceinline__ void forward_cone_binned_kernel_body(Geo g, int v_sta
   for (int base = start; base < end; base += cap) {
     const int n = min(cap, end - base);
     __syncthreads();
-    for (int i = tid; i < n; i += nthr) rec[i] = fwd_stage_record(vrec[vlist[base + i]]);
+    for (int i = tid; i < n; i += nthr) rec[i] = fwd_stage_record(vrec[vlist[base + i]], c0);
     __syncthreads();
     if constexpr (ASYNC) {
       fwd_rt_round_async<AEB>(rec, n, stage, SP, values, band, slice_start, kc_lo, kc_hi, bp,
