@@ -521,13 +521,13 @@ def roofline_block(m, torch, y, kt, storage, hbm):
 
 
 # DRAM traffic of one forward + line-search launch of the headline workload's
-# 128-subset step (ncu dram__bytes_read.sum 556.2 MB + dram__bytes_write.sum
-# 458.3 MB, one captured launch): one read of e (439 MB), the A delta store
+# 128-subset step (ncu dram__bytes_read.sum 555.4 MB + dram__bytes_write.sum
+# 455.4 MB, one captured launch): one read of e (439 MB), the A delta store
 # (439 MB) and the records and cylinders.
-TRAFFIC_FWD_LS_FP32 = 1014512128.0
+TRAFFIC_FWD_LS_FP32 = 1010784512.0
 # Warp instructions of the same launch (ncu smsp__inst_executed.sum), and
 # the SM clock the issue peak is taken at (clocks.max.sm of this pool's B200s).
-WARP_INST_FWD_LS_FP32 = 1084691937
+WARP_INST_FWD_LS_FP32 = 1028039755
 SM_MAX_MHZ = 1965
 
 
