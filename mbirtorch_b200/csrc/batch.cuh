@@ -89,11 +89,11 @@ template <int CP, int T, typename RD> struct BackParallel4B {
     back_parallel4_kernel_body<CP, T, RD>(a...);
   }
 };
-template <int CP, int SPL, int NT, typename RD> struct BackConeB {
+template <int CP, int SPL, int NT, typename RD, int HBL = 8> struct BackConeB {
   static constexpr int kMaxThreads = kThreads, kMinBlocks = 1;
-  static auto kernel() { return back_cone_kernel<CP, SPL, NT, RD>; }
+  static auto kernel() { return back_cone_kernel<CP, SPL, NT, RD, HBL>; }
   template <typename... A> __device__ static void run(const A &...a) {
-    back_cone_kernel_body<CP, SPL, NT, RD>(a...);
+    back_cone_kernel_body<CP, SPL, NT, RD, HBL>(a...);
   }
 };
 struct ConeBinB {

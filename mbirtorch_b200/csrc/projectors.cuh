@@ -409,7 +409,10 @@ __device__ __forceinline__ void column_batch(const RD &rd, const size_t (&base)[
 
 // One warp per (pixel, chunk of 32*SPL slices).  Dynamic shared memory:
 // 8 warps x (R + 2 kPad) floats of column buffer, then 8 x 32 ConeRec.
-template <int CP, int SPL, int NT, typename RD>
+// HBL: rows per lane of a column batch for bands of more than 64 slices
+// (8, or 6 where the host's back_long_batch finds 192-row batches leave
+// fewer idle row slots on the detector's column than 256-row ones).
+template <int CP, int SPL, int NT, typename RD, int HBL = 8>
 __device__ __forceinline__ void back_cone_kernel_body(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc, RD rd,
                  const int64_t *__restrict__ pix, int P, int slice_start, int band,
                  int slice_chunks, float *__restrict__ out,
@@ -504,8 +507,10 @@ __device__ __forceinline__ void back_cone_kernel_body(Geo g, const float *__rest
         // Column rows in batches of HB per lane, every load of a batch in
         // flight before the first use.  A short band (SPL <= 2, at most 64
         // slices) spans about 64 w_r rows, so its batches are 4 rows deep:
-        // fewer predicated-off loads than 8.
-        constexpr int HB = NT == 3 ? (SPL <= 2 ? 4 : 8) : 2;
+        // fewer predicated-off loads than 8.  A batch's rows past the
+        // column's end are predicated off but still issue, so longer bands
+        // take the depth HBL that fits the detector's rows (back_long_batch).
+        constexpr int HB = NT == 3 ? (SPL <= 2 ? 4 : HBL) : 2;
         const int m_lo = (int)lo, m_hi = (int)hi;
         if constexpr (SPL <= 2) {
           // Short bands: whole batches (every lane's HB rows exist, no row
@@ -559,14 +564,14 @@ __device__ __forceinline__ void back_cone_kernel_body(Geo g, const float *__rest
   }
 }
 
-template <int CP, int SPL, int NT, typename RD>
+template <int CP, int SPL, int NT, typename RD, int HBL = 8>
 __global__ void __launch_bounds__(kThreads)
 
 back_cone_kernel(Geo g, const float *__restrict__ vp, int v_start, int v_count, int vpc, RD rd,
                  const int64_t *__restrict__ pix, int P, int slice_start, int band,
                  int slice_chunks, float *__restrict__ out,
                  const ConeFwdRec *__restrict__ recs) {
-  back_cone_kernel_body<CP, SPL, NT, RD>(g, vp, v_start, v_count, vpc, rd, pix, P, slice_start, band, slice_chunks, out, recs);
+  back_cone_kernel_body<CP, SPL, NT, RD, HBL>(g, vp, v_start, v_count, vpc, rd, pix, P, slice_start, band, slice_chunks, out, recs);
 }
 
 // out[i] = sum over chunks of part[chunk * n + i], in chunk order.

@@ -608,3 +608,48 @@ def test_large_subset_step_vs_oracle(slices, subset):
     assert abs(float(alpha) - oalpha) / oalpha <= 1e-4
     assert rel_l2(flat.cpu().numpy(), oflat) <= 1e-5
     assert rel_l2(err.cpu().numpy(), oerr) <= 1e-5
+
+
+@pytest.mark.parametrize("rows", [256, 300])
+def test_long_band_back_projection_and_step_vs_oracle(rows):
+    """Cone bands of more than 128 slices (8 slices per lane) on detectors of
+    256 rows (column batches 8 rows deep per lane) and 300 rows (6 rows deep,
+    the depth that covers 257..384 rows in fewer row slots): the sparse back
+    projection and a VCD subset step against the FP64 oracle."""
+    import oracle
+    from oracle import vcd as ovcd
+    m = mb.ConeBeamModel((12, rows, 40), np.linspace(0, 2 * np.pi, 12, endpoint=False),
+                         300.0, 150.0)
+    m.set_params(no_warning=True, verbose=0, recon_shape=(24, 24, 200))
+    rs = m.get_params('recon_shape')
+    g = m._geometry()
+    assert g.num_det_rows == rows and rs[2] == 200
+    rng = np.random.default_rng(21)
+    idx = mb.gen_full_indices(rs).astype(np.int64)
+    y = rng.standard_normal(m.get_params('sinogram_shape')).astype(np.float32)
+    sub = np.sort(rng.choice(idx, size=40, replace=False))
+    b = m.sparse_back_project(torch.as_tensor(y, device='cuda'),
+                              torch.as_tensor(sub, device='cuda')).cpu().numpy()
+    prob = _oracle_problem(m)
+    vp = m._view_params_array().astype(np.float64)
+    assert rel_l2(b, oracle.cone_back(prob.geom, vp, y, sub)) <= 1e-5
+
+    x_true = rng.random(rs).astype(np.float32)
+    sino = m.forward_project(x_true)
+    m.auto_set_regularization_params(sino)
+    x0 = (0.1 * rng.random(rs)).astype(np.float32)
+    e0 = sino - m.forward_project(x0)
+    H = m.compute_hessian_diagonal()
+    upd = m.create_vcd_subset_updater(H, weights=1)
+    flat = torch.as_tensor(x0.reshape(-1, rs[2]), device='cuda').clone()
+    err = torch.as_tensor(e0, device='cuda').clone()
+    flat, err, ell1, alpha, sumsq = upd(flat, err, torch.as_tensor(sub, device='cuda'))
+    sy, sx = m.get_params(['sigma_y', 'sigma_x'])
+    ou = ovcd.SubsetUpdater(prob, np.asarray(H).reshape(-1, rs[2]), None, sy, sx,
+                            dc_profile=ovcd.dc_damping_profile(prob))
+    oflat = x0.reshape(-1, rs[2]).astype(np.float64)
+    oerr = e0.astype(np.float64)
+    oell1, oalpha, osumsq = ou(oflat, oerr, sub)
+    assert abs(float(alpha) - oalpha) / oalpha <= 1e-4
+    assert rel_l2(flat.cpu().numpy(), oflat) <= 1e-5
+    assert rel_l2(err.cpu().numpy(), oerr) <= 1e-5
